@@ -1,0 +1,176 @@
+/*
+ * gsplat_b200.h -- C ABI of the B200 (sm_100a) palette-weight Gaussian
+ * rasterizer.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (cudaStream_t passed as void*; NULL is the legacy default stream), enqueues
+ * its kernels on that stream and returns a status code (GSB_OK == 0).  No
+ * entry point allocates device memory: callers pass every output buffer and
+ * every scratch buffer, sized with the *_workspace_bytes() queries.  On error
+ * gsb_last_error() returns a message for the calling thread.
+ *
+ * The functions under "reference operators" are the kernels behind the 13
+ * Python ops of the reference extension `gsplatcu` (ReparamGS-Palette,
+ * gsplatcu/ext.cpp:125-139); each comment names the reference host function
+ * (gsplatcu/gausplat.cu) it replaces.  Unless stated, outputs have the shapes
+ * and layouts of the reference's output tensors, FP32 row-major.
+ */
+#ifndef GSPLAT_B200_H_
+#define GSPLAT_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------- status codes */
+#define GSB_OK 0
+#define GSB_ERR_INVALID_ARGUMENT 1 /* bad size, pointer or mode            */
+#define GSB_ERR_CUDA 2             /* a CUDA runtime call or launch failed */
+#define GSB_ERR_UNSUPPORTED 3      /* valid but unsupported configuration  */
+#define GSB_ERR_CAPACITY 4         /* patch count exceeded a capacity      */
+#define GSB_ERR_DEVICE_TIMEOUT 5   /* a bounded device-side wait expired   */
+
+/* Storage type of per-Gaussian colour parameters (SH weights, factors). */
+#define GSB_DTYPE_F32 0
+#define GSB_DTYPE_BF16 1
+
+/* Maximum channels composited per pixel (MAX_SPLAT_DIM, gsplatcu/kernel.cu:12). */
+#define GSB_MAX_CHANNELS 8
+
+/* Message describing the last error on this thread ("" if none). */
+const char* gsb_last_error(void);
+/* Library ABI version, major * 100 + minor. */
+int gsb_version(void);
+
+/* ===================================================== reference operators */
+
+/* project (gsplatcu/gausplat.cu:381-419).  pc = Rcw pw + tcw; depth = -1 and
+ * zero us/pcs when z < 0.2; u = (fx x/z + cx, fy y/z + cy).  du_dpcs [n,2,3]
+ * may be NULL (calc_J false).  Rcw [3,3] and tcw [3] are device pointers. */
+int gsb_project(int64_t n, const float* pws, const float* Rcw, const float* tcw, float fx,
+                float fy, float cx, float cy, float* us, float* pcs, float* depths,
+                float* du_dpcs, void* stream);
+
+/* computeCov3D (gsplatcu/gausplat.cu:298-331).  Sigma = (R(q) S)(R(q) S)^T as
+ * 6 upper entries; zero where depth < 0.2.  Jacobians [n,6,4] and [n,6,3] may
+ * both be NULL. */
+int gsb_compute_cov3d(int64_t n, const float* rots, const float* scales, const float* depths,
+                      float* cov3ds, float* dcov3d_drots, float* dcov3d_dscales, void* stream);
+
+/* computeCov2D (gsplatcu/gausplat.cu:333-379).  width/height are used only to
+ * form tan_fov = width/(2 fx), height/(2 fy) as the reference does.
+ * Jacobians [n,3,6] and [n,3,3] may both be NULL. */
+int gsb_compute_cov2d(int64_t n, const float* cov3ds, const float* pcs, const float* Rcw,
+                      const float* depths, float fx, float fy, float width, float height,
+                      float* cov2ds, float* dcov2d_dcov3ds, float* dcov2d_dpcs, void* stream);
+
+/* inverseCov2D (gsplatcu/gausplat.cu:590-617).  conic = adj/det with no
+ * epsilon; a NaN 1/det sets depth := -1 IN PLACE.  areas (int32 [n,2]) =
+ * ceil(3 sqrt|diag|).  dcinv2d_dcov2ds [n,3,3] may be NULL. */
+int gsb_inverse_cov2d(int64_t n, const float* cov2ds, float* depths, float* cinv2ds,
+                      int32_t* areas, float* dcinv2d_dcov2ds, void* stream);
+
+/* sh2Weight (gsplatcu/gausplat.cu:425-462).  shs [n, sh_dim*K] band-major in
+ * FP32 or BF16 (shs_dtype), sh_dim in {1,4,9,16}, 1 <= K <= 8.  weights [n,K];
+ * dweight_dshs [n,1,sh_dim] and dweight_dpws [n,K,3] may both be NULL. */
+int gsb_sh2weight(int64_t n, const void* shs, int shs_dtype, int sh_dim, int K, const float* pws,
+                  const float* twc, float* weights, float* dweight_dshs, float* dweight_dpws,
+                  void* stream);
+
+/* sh2Weight_fast (gsplatcu/gausplat.cu:469-509), generalised to rank r.
+ * shs_dc [n,K]; shs_A [n,P,r]; shs_B [n,r,Q] (rank 1 is the reference's 2-D
+ * [n,P], [n,Q]); L = P*Q/K must be 0, 3, 8 or 15.  dweight_ddc [n,K] and
+ * ylm [n,L] may both be NULL (calc_J false). */
+int gsb_sh2weight_fast(int64_t n, const void* shs_dc, const void* shs_A, const void* shs_B,
+                       int dtype, int K, int P, int Q, int rank, const float* pws,
+                       const float* twc, float* weights, float* dweight_ddc, float* ylm,
+                       void* stream);
+
+/* sh2Weight_fast_B (gsplatcu/gausplat.cu:512-541), rank r.  dA [n,P,r] and
+ * dB [n,r,Q] are overwritten (no atomics; one thread owns one Gaussian). */
+int gsb_sh2weight_fast_backward(int64_t n, const void* shs_A, const void* shs_B, int dtype,
+                                const float* ylm, const float* dloss_dw, int K, int P, int Q,
+                                int rank, float* dA, float* dB, void* stream);
+
+/* sh2Color (gsplatcu/gausplat.cu:551-584).  shs [n, sh_dim*3]; colors [n,3];
+ * dcolor_dshs [n,1,sh_dim] and dcolor_dpws [n,3,3] may both be NULL. */
+int gsb_sh2color(int64_t n, const void* shs, int shs_dtype, int sh_dim, const float* pws,
+                 const float* twc, float* colors, float* dcolor_dshs, float* dcolor_dpws,
+                 void* stream);
+
+/* lab2rgb (gsplatcu/gausplat.cu:623-641).  lab, rgb: [3,H,W]. */
+int gsb_lab2rgb(int height, int width, const float* lab, float* rgb, void* stream);
+
+/* ------------------------------------------------------ splatting pipeline
+ * splat_weight / splat_color (gsplatcu/gausplat.cu:161-249, 25-109) run as
+ * three calls so that the caller owns every allocation:
+ *
+ *   1. gsb_splat_pack      -- per-Gaussian tile rectangles and patch counts
+ *                             (getRects, gsplatcu/kernel.cu:127-162, updating
+ *                             depths/areas in place like the reference), the
+ *                             packed compositing records, and the patch-count
+ *                             prefix sum.  Needs `state` of
+ *                             gsb_splat_state_bytes(n, channels) bytes.
+ *   2. gsb_splat_counts    -- copies {patch count M, max depth key} to host
+ *                             memory (synchronises `stream`).
+ *   3. gsb_splat_sort      -- key emission, radix sort and per-tile ranges
+ *                             (createKeys / sort_by_key / getRanges).  Needs
+ *                             `sort_ws` of gsb_splat_sort_bytes(...) bytes.
+ *   4. gsb_splat_draw      -- front-to-back compositing (draw_weight /
+ *                             draw_color, gsplatcu/kernel.cu:194-372).
+ *
+ * Tile lists and ranges are bit-identical to the reference's given identical
+ * us/areas/depths: keys are (tile, uint32(depth*1000)) sorted stably in
+ * Gaussian order.  `channels` is K for weights, 3 for colours. */
+size_t gsb_splat_state_bytes(int64_t n, int channels);
+
+int gsb_splat_pack(int64_t n, int height, int width, int channels, const float* us,
+                   const float* cinv2ds, const float* alphas, const void* feats, int feat_dtype,
+                   float* depths, int32_t* areas, void* state, void* stream);
+
+/* host_out[0] = M (patches), host_out[1] = max uint32(depth*1000) over
+ * binned Gaussians.  Blocks until `stream` has finished step 1. */
+int gsb_splat_counts(int64_t n, const void* state, uint32_t* host_out, void* stream);
+
+size_t gsb_splat_sort_bytes(int64_t n, int height, int width, int64_t patches,
+                            uint32_t max_depth_key);
+
+/* gsid_out [patches] (int32) receives the sorted Gaussian ids; ranges_out
+ * [tiles,2] (int32) the per-tile [start,end) -- (0,0) for empty tiles and,
+ * as in the reference's getRanges, (0,0) for the single tile when M == 1. */
+int gsb_splat_sort(int64_t n, int height, int width, int64_t patches, uint32_t max_depth_key,
+                   const void* state, void* sort_ws, int32_t* gsid_out, int32_t* ranges_out,
+                   void* stream);
+
+/* out [channels,H,W], contrib [H,W] (1-based index of the last blended
+ * Gaussian in the tile list), final_tau [H,W].  Pixels of tiles without
+ * patches are set to 0 / 0 / tau_init (0 for weights, 1 for colours, as
+ * gsplatcu/gausplat.cu:178 and :39 initialise them). */
+int gsb_splat_draw(int64_t n, int height, int width, int channels, const int32_t* ranges,
+                   const int32_t* gsid, const void* state, float tau_init, float* out,
+                   int32_t* contrib, float* final_tau, void* stream);
+
+/* splat_weight_B / splat_color_B (gsplatcu/gausplat.cu:252-292, 111-155):
+ * reverse-order adjoint of the compositing.  Re-packs the records into
+ * `state` (gsb_splat_state_bytes) from the forward's inputs.  Outputs are
+ * ACCUMULATED (+=) and may be NULL:
+ *   dfeats [n,channels]  -- dL/dweights (splat_weight_B) / dL/dcolors
+ *   dalphas [n], dus [n,2], dcinv2ds [n,3]  -- the geometry/opacity adjoint of
+ *   draw_color_B (gsplatcu/kernel.cu:1176-1284), here for any channel count.
+ * dloss_dtau [H,W] (may be NULL) adds the final-transmittance term of
+ * vanilla_3dgs/gsplatcu/kernel.cu:912-919. */
+int gsb_splat_backward(int64_t n, int height, int width, int channels, const float* us,
+                       const float* cinv2ds, const float* alphas, const void* feats,
+                       int feat_dtype, const int32_t* ranges, const int32_t* gsid,
+                       const int32_t* contrib, const float* final_tau, const float* dloss_dout,
+                       const float* dloss_dtau, void* state, float* dfeats, float* dalphas,
+                       float* dus, float* dcinv2ds, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSPLAT_B200_H_ */

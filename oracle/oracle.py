@@ -1,0 +1,306 @@
+"""numpy front-end of the CPU oracle (gsplat_oracle.cpp) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, as the checker or the timed CPU baseline; the product never does.
+Each function mirrors one reference ``gsplatcu`` op (ReparamGS-Palette
+``gsplatcu/ext.cpp:125-139``) on numpy arrays, in FP32 (``np.float32``) or in
+FP64 (``np.float64``), chosen by the dtype argument.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+TILE = 16
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or (
+                os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "gsplat_oracle.cpp"))):
+            build()
+        _lib = C.CDLL(LIB_PATH)
+        _lib.oracle_bin_count.restype = C.c_int64
+        _lib.oracle_get_threads.restype = C.c_int
+    return _lib
+
+
+def set_threads(n):
+    lib().oracle_set_threads(int(n))
+
+
+def get_threads():
+    return int(lib().oracle_get_threads())
+
+
+def _p(a):
+    """Raw pointer of a contiguous numpy array (or NULL for None)."""
+    if a is None:
+        return C.c_void_p(0)
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be contiguous"
+    return C.c_void_p(a.ctypes.data)
+
+
+def _sfx(dt):
+    dt = np.dtype(dt)
+    if dt == np.float32:
+        return "f32", C.c_float
+    if dt == np.float64:
+        return "f64", C.c_double
+    raise TypeError(f"oracle supports float32/float64, got {dt}")
+
+
+def _arr(x, dt):
+    return np.ascontiguousarray(np.asarray(x, dtype=dt))
+
+
+def grid_dims(H, W):
+    return (W + TILE - 1) // TILE, (H + TILE - 1) // TILE
+
+
+# ------------------------------------------------------------------ geometry
+def project(pws, Rcw, tcw, fx, fy, cx, cy, calc_J=False, dtype=np.float32):
+    s, cf = _sfx(dtype)
+    pws, Rcw, tcw = _arr(pws, dtype), _arr(Rcw, dtype), _arr(tcw, dtype)
+    n = pws.shape[0]
+    us = np.zeros((n, 2), dtype)
+    pcs = np.zeros((n, 3), dtype)
+    depths = np.zeros((n,), dtype)
+    du = np.zeros((n, 2, 3), dtype) if calc_J else None
+    getattr(lib(), f"oracle_project_{s}")(C.c_int64(n), _p(pws), _p(Rcw), _p(tcw), cf(fx), cf(fy),
+                                           cf(cx), cf(cy), _p(us), _p(pcs), _p(depths), _p(du))
+    return [us, pcs, depths] + ([du] if calc_J else [])
+
+
+def cov3d(rots, scales, depths, calc_J=False, dtype=np.float32):
+    s, _ = _sfx(dtype)
+    rots, scales, depths = _arr(rots, dtype), _arr(scales, dtype), _arr(depths, dtype)
+    n = rots.shape[0]
+    out = np.zeros((n, 6), dtype)
+    dr = np.zeros((n, 6, 4), dtype) if calc_J else None
+    ds = np.zeros((n, 6, 3), dtype) if calc_J else None
+    getattr(lib(), f"oracle_cov3d_{s}")(C.c_int64(n), _p(rots), _p(scales), _p(depths), _p(out),
+                                         _p(dr), _p(ds))
+    return [out] + ([dr, ds] if calc_J else [])
+
+
+def tan_fov(width, height, fx, fy, dtype=np.float32):
+    """tan of the half field of view as the reference host code computes it
+    (gsplatcu/gausplat.cu:357-358): W / (2 fx) in the working precision."""
+    dt = np.dtype(dtype).type
+    return dt(width) / (dt(2) * dt(fx)), dt(height) / (dt(2) * dt(fy))
+
+
+def cov2d(cov3ds, pcs, Rcw, depths, fx, fy, width, height, calc_J=False, dtype=np.float32):
+    s, cf = _sfx(dtype)
+    cov3ds, pcs, Rcw, depths = (_arr(x, dtype) for x in (cov3ds, pcs, Rcw, depths))
+    n = pcs.shape[0]
+    tx, ty = tan_fov(width, height, fx, fy, dtype)
+    out = np.zeros((n, 3), dtype)
+    d3 = np.zeros((n, 3, 6), dtype) if calc_J else None
+    dp = np.zeros((n, 3, 3), dtype) if calc_J else None
+    getattr(lib(), f"oracle_cov2d_{s}")(C.c_int64(n), _p(cov3ds), _p(pcs), _p(Rcw), _p(depths),
+                                         cf(fx), cf(fy), cf(tx), cf(ty), _p(out), _p(d3), _p(dp))
+    return [out] + ([d3, dp] if calc_J else [])
+
+
+def inverse_cov2d(cov2ds, depths, calc_J=False, dtype=np.float32):
+    """Returns [cinv, areas, (dcinv)]; `depths` (a numpy array of `dtype`) is
+    updated in place, as the reference does."""
+    s, _ = _sfx(dtype)
+    cov2ds = _arr(cov2ds, dtype)
+    assert depths.dtype == np.dtype(dtype) and depths.flags["C_CONTIGUOUS"]
+    n = cov2ds.shape[0]
+    cinv = np.zeros((n, 3), dtype)
+    areas = np.zeros((n, 2), np.int32)
+    dc = np.zeros((n, 3, 3), dtype) if calc_J else None
+    getattr(lib(), f"oracle_inverse_cov2d_{s}")(C.c_int64(n), _p(cov2ds), _p(depths), _p(cinv),
+                                                 _p(areas), _p(dc))
+    return [cinv, areas] + ([dc] if calc_J else [])
+
+
+# -------------------------------------------------------- spherical harmonics
+def sh2feat(shs, pws, twc, K, calc_J=False, dtype=np.float32, ref_quirk=True):
+    """sh2Weight (K palette weights) / sh2Color (K = 3).  shs [N, nb*K] band-major."""
+    s, _ = _sfx(dtype)
+    shs, pws, twc = _arr(shs, dtype), _arr(pws, dtype), _arr(twc, dtype).reshape(3)
+    n = pws.shape[0]
+    nb = shs.shape[1] // K
+    assert nb in (1, 4, 9, 16)
+    feat = np.zeros((n, K), dtype)
+    dshs = np.zeros((n, 1, nb), dtype) if calc_J else None
+    dpws = np.zeros((n, K, 3), dtype) if calc_J else None
+    getattr(lib(), f"oracle_sh2feat_{s}")(C.c_int64(n), _p(shs), _p(pws), _p(twc), C.c_int(nb),
+                                           C.c_int(K), _p(feat), _p(dshs), _p(dpws),
+                                           C.c_int(1 if ref_quirk else 0))
+    return [feat] + ([dshs, dpws] if calc_J else [])
+
+
+def _lowrank_dims(A, B, K, Q):
+    if A.ndim == 2:
+        P, rank = A.shape[1], 1
+        assert B.ndim == 2 and B.shape[1] == Q
+    else:
+        P, rank = A.shape[1], A.shape[2]
+        assert B.shape[1] == rank and B.shape[2] == Q
+    L = P * Q // K
+    return P, rank, L
+
+
+def sh2weight_fast(dc, A, B, pws, twc, K, Q, calc_J=True, dtype=np.float32):
+    s, _ = _sfx(dtype)
+    dc, A, B, pws = (_arr(x, dtype) for x in (dc, A, B, pws))
+    twc = _arr(twc, dtype).reshape(3)
+    n = pws.shape[0]
+    P, rank, L = _lowrank_dims(A, B, K, Q)
+    w = np.zeros((n, K), dtype)
+    ddc = np.zeros((n, K), dtype)
+    ylm = np.zeros((n, L), dtype)
+    getattr(lib(), f"oracle_sh2weight_lowrank_{s}")(
+        C.c_int64(n), _p(dc), _p(A), _p(B), _p(pws), _p(twc), C.c_int(K), C.c_int(P), C.c_int(Q),
+        C.c_int(rank), C.c_int(L), _p(w), _p(ddc), _p(ylm))
+    return [w, ddc, ylm] if calc_J else [w]
+
+
+def sh2weight_fast_b(A, B, ylm, dw, K, Q, dtype=np.float32):
+    s, _ = _sfx(dtype)
+    A, B, ylm, dw = (_arr(x, dtype) for x in (A, B, ylm, dw))
+    n = A.shape[0]
+    P, rank, L = _lowrank_dims(A, B, K, Q)
+    dA = np.zeros(A.shape, dtype)
+    dB = np.zeros(B.shape, dtype)
+    getattr(lib(), f"oracle_sh2weight_lowrank_b_{s}")(
+        C.c_int64(n), _p(A), _p(B), _p(ylm), _p(dw), C.c_int(K), C.c_int(P), C.c_int(Q),
+        C.c_int(rank), C.c_int(L), _p(dA), _p(dB))
+    return [dA, dB]
+
+
+# ------------------------------------------------------------------- binning
+def bin_gaussians(us, areas, depths, H, W):
+    """Rects, counts, scan, key emission, stable sort and ranges (FP32, bit-exact
+    restatement).  `areas` (int32) and `depths` (float32) are updated in place.
+    Returns dict(gsid, ranges, keys, M, counts, rects)."""
+    us = _arr(us, np.float32)
+    assert areas.dtype == np.int32 and depths.dtype == np.float32
+    n = us.shape[0]
+    gx, gy = grid_dims(H, W)
+    rects = np.zeros((n, 4), np.uint32)
+    counts = np.zeros((n,), np.uint32)
+    offsets = np.zeros((n,), np.uint32)
+    M = int(lib().oracle_bin_count(C.c_int64(n), _p(us), _p(areas), _p(depths), C.c_int(H),
+                                   C.c_int(W), _p(rects), _p(counts), _p(offsets)))
+    gsid = np.zeros((M,), np.int32)
+    keys = np.zeros((M,), np.uint64)
+    ranges = np.zeros((gx * gy, 2), np.int32)
+    lib().oracle_bin_sort(C.c_int64(n), _p(depths), _p(rects), _p(offsets), C.c_int(H), C.c_int(W),
+                          C.c_int64(M), _p(gsid), _p(ranges), _p(keys))
+    return dict(gsid=gsid, ranges=ranges, keys=keys, M=M, counts=counts, rects=rects)
+
+
+# -------------------------------------------------------------- compositing
+def draw(H, W, K, ranges, gsid, us, cinv, alphas, feat, tau_init, dtype=np.float32):
+    """Forward compositing; returns [out [K,H,W], contrib [H,W], final_tau [H,W]].
+    `tau_init` is 0 for splat_weight and 1 for splat_color (the reference's
+    initial value kept by empty tiles)."""
+    s, _ = _sfx(dtype)
+    us, cinv, feat = _arr(us, dtype), _arr(cinv, dtype), _arr(feat, dtype)
+    alphas = _arr(alphas, dtype).reshape(-1)
+    ranges, gsid = _arr(ranges, np.int32), _arr(gsid, np.int32)
+    out = np.zeros((K, H, W), dtype)
+    contrib = np.zeros((H, W), np.int32)
+    ft = np.full((H, W), tau_init, dtype)
+    getattr(lib(), f"oracle_draw_{s}")(C.c_int(H), C.c_int(W), C.c_int(K), _p(ranges), _p(gsid),
+                                        _p(us), _p(cinv), _p(alphas), _p(feat), _p(out),
+                                        _p(contrib), _p(ft))
+    return [out, contrib, ft]
+
+
+def draw_backward(H, W, K, ranges, gsid, us, cinv, alphas, feat, final_tau, contrib, dout,
+                  dT=None, dtype=np.float32):
+    """Adjoint of draw(); returns dict(dfeat [N,K], dalpha [N], du [N,2], dconic [N,3])."""
+    s, _ = _sfx(dtype)
+    us, cinv, feat = _arr(us, dtype), _arr(cinv, dtype), _arr(feat, dtype)
+    alphas = _arr(alphas, dtype).reshape(-1)
+    final_tau, dout = _arr(final_tau, dtype), _arr(dout, dtype)
+    dT = None if dT is None else _arr(dT, dtype)
+    ranges, gsid, contrib = _arr(ranges, np.int32), _arr(gsid, np.int32), _arr(contrib, np.int32)
+    n = us.shape[0]
+    dfeat = np.zeros((n, K), dtype)
+    dalpha = np.zeros((n,), dtype)
+    du = np.zeros((n, 2), dtype)
+    dq = np.zeros((n, 3), dtype)
+    getattr(lib(), f"oracle_draw_backward_{s}")(
+        C.c_int(H), C.c_int(W), C.c_int(K), _p(ranges), _p(gsid), _p(us), _p(cinv), _p(alphas),
+        _p(feat), _p(final_tau), _p(contrib), _p(dout), _p(dT), _p(dfeat), _p(dalpha), _p(du), _p(dq))
+    return dict(dfeat=dfeat, dalpha=dalpha, du=du, dconic=dq)
+
+
+def lab2rgb(lab):
+    lab = _arr(lab, np.float32)
+    _, H, W = lab.shape
+    out = np.zeros_like(lab)
+    lib().oracle_lab2rgb(C.c_int(H), C.c_int(W), _p(lab), _p(out))
+    return out
+
+
+# ---------------------------------------------------- composite pipelines
+def splat(H, W, K, us, cinv, alphas, depths, feat, areas, tau_init):
+    """The reference's splat_weight / splat_color host sequence
+    (gsplatcu/gausplat.cu:161-249): binning then compositing, FP32.  depths and
+    areas are updated in place.  Returns [out, contrib, final_tau, ranges, gsid]."""
+    b = bin_gaussians(us, areas, depths, H, W)
+    out, contrib, ft = draw(H, W, K, b["ranges"], b["gsid"], us, cinv, alphas, feat, tau_init)
+    return [out, contrib, ft, b["ranges"], b["gsid"]]
+
+
+def camera_arrays(cam, dtype):
+    """(Rcw [3,3], tcw [3], twc [3]) of a camera-like object as numpy arrays."""
+    def npy(x):
+        if hasattr(x, "detach"):
+            x = x.detach().cpu().numpy()
+        return np.asarray(x, dtype=np.float64)
+    Rcw, tcw = npy(cam.Rcw), npy(cam.tcw).reshape(3)
+    twc = -np.linalg.inv(Rcw) @ tcw
+    return Rcw.astype(dtype), tcw.astype(dtype), twc.astype(dtype)
+
+
+def preprocess(pws, rots, scales, cam, dtype=np.float32):
+    """project -> cov3D -> cov2D -> inverse, as WeightGSFunctionTest does
+    (gsplat/gsmodel.py:107-115).  Returns dict of per-Gaussian arrays."""
+    Rcw, tcw, twc = camera_arrays(cam, dtype)
+    us, pcs, depths = project(pws, Rcw, tcw, cam.fx, cam.fy, cam.cx, cam.cy, False, dtype)
+    c3, = cov3d(rots, scales, depths, False, dtype)
+    c2, = cov2d(c3, pcs, Rcw, depths, cam.fx, cam.fy, cam.width, cam.height, False, dtype)
+    cinv, areas = inverse_cov2d(c2, depths, False, dtype)
+    return dict(us=us, pcs=pcs, depths=depths, cov3d=c3, cov2d=c2, cinv=cinv, areas=areas,
+                twc=twc, Rcw=Rcw, tcw=tcw)
+
+
+def render_weights(pws, rots, scales, alphas, weights, cam, dtype=np.float32, lists=None):
+    """Full forward of the palette-weight path.  Geometry and compositing run in
+    `dtype`; binning always runs on the FP32 image of the projected values (it
+    is integer work defined on FP32 inputs), unless `lists` = (ranges, gsid)
+    supplies the tile lists to use.  Returns dict(layer, contrib, final_tau,
+    ranges, gsid, pre)."""
+    pre = preprocess(pws, rots, scales, cam, dtype)
+    K = weights.shape[1]
+    H, W = int(cam.height), int(cam.width)
+    if lists is None:
+        d32 = pre["depths"].astype(np.float32)
+        a32 = pre["areas"].copy()
+        b = bin_gaussians(pre["us"].astype(np.float32), a32, d32, H, W)
+        ranges, gsid = b["ranges"], b["gsid"]
+    else:
+        ranges, gsid = lists
+    out, contrib, ft = draw(H, W, K, ranges, gsid, pre["us"], pre["cinv"], alphas, weights, 0.0, dtype)
+    return dict(layer=out, contrib=contrib, final_tau=ft, ranges=ranges, gsid=gsid, pre=pre)

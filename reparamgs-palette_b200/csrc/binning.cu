@@ -1,0 +1,550 @@
+// Tile binning: per-Gaussian rectangles and patch counts, packed compositing
+// records, patch-count scan, key emission, an LSD radix sort over only the
+// key bits in use, and per-tile ranges.
+//
+// Ordering contract (gsplatcu/kernel.cu:96-187, gsplatcu/gausplat.cu:185-226):
+// patches are emitted Gaussian by Gaussian (tiles of one Gaussian row-major)
+// and sorted STABLY by (tile, uint32(depth*1000)), so each tile's list is
+// ordered by quantised depth, then Gaussian id -- the same total order the
+// reference's stable 64-bit thrust::sort_by_key produces.  Keys here hold
+// only ceil(log2 T) tile bits above the depth-key bits actually used, so the
+// sort runs ceil(bits/8) passes instead of eight.
+#include "gsb_geometry.cuh"
+#include "gsb_internal.h"
+
+namespace gsb {
+
+// ----------------------------------------------------------------- state
+int record_vec4(int channels) { return ((11 + channels) + 3) / 4; }
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Layout: channel-independent arrays first (so that callers that do not know
+// the channel count can locate them), packed records last.
+size_t splat_state_bytes(int64_t n, int channels) {
+  const int64_t nb = (n + kBinBlock - 1) / kBinBlock;
+  size_t b = 0;
+  b += align256((size_t)n * 8);                       // rects
+  b += align256((size_t)n * 4);                       // dkeys
+  b += align256((size_t)n * 4);                       // counts
+  b += align256((size_t)(nb > 0 ? nb : 1) * 4);       // block sums
+  b += align256(16 * 4);                              // stats
+  b += align256((size_t)n * record_vec4(channels) * 16);  // records
+  return b;
+}
+
+SplatState carve_state(void* base, int64_t n, int channels) {
+  SplatState s;
+  char* p = (char*)base;
+  s.rec_vec4 = record_vec4(channels);
+  s.n_blocks = (n + kBinBlock - 1) / kBinBlock;
+  s.rects = (uint2*)p;
+  p += align256((size_t)n * 8);
+  s.dkeys = (uint32_t*)p;
+  p += align256((size_t)n * 4);
+  s.counts = (uint32_t*)p;
+  p += align256((size_t)n * 4);
+  s.block_sums = (uint32_t*)p;
+  p += align256((size_t)(s.n_blocks > 0 ? s.n_blocks : 1) * 4);
+  s.stats = (uint32_t*)p;
+  p += align256(16 * 4);
+  s.records = (float4*)p;
+  return s;
+}
+
+// --------------------------------------------------------- block helpers
+// Exclusive scan of one value per thread over a 256-thread block.
+__device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t* warp_tot,
+                                                       uint32_t* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  uint32_t base = 0, tot = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t t = warp_tot[k];
+    base += (k < w) ? t : 0u;
+    tot += t;
+  }
+  __syncthreads();
+  if (total) *total = tot;
+  return base + incl - v;
+}
+
+// ------------------------------------------------------------------ pack
+// One thread per Gaussian: tile rectangle and patch count (getRects,
+// gsplatcu/kernel.cu:127-162, including its in-place depth/areas updates),
+// the quantised depth key, and the packed compositing record.
+//
+// The record carries a conservative support box: pixels outside it satisfy
+// d^T Q d > cut, where cut = 2 ln(alpha/0.002) + margin guarantees
+// alpha' < 0.002 in the reference's evaluation.  The box is widened for the
+// rounding error of the FP32 quadratic form (proportional to the conic's
+// condition number) and disabled for degenerate or non-finite conics.
+template <typename T>
+__global__ void __launch_bounds__(kBinBlock)
+    k_pack(int64_t n, uint32_t gx, uint32_t gy, int C, int V, const float* __restrict__ us,
+           const float* __restrict__ cinv, const float* __restrict__ alphas,
+           const T* __restrict__ feats, float* __restrict__ depths, int32_t* __restrict__ areas,
+           bool bin, float4* __restrict__ records, uint2* __restrict__ rects,
+           uint32_t* __restrict__ dkeys, uint32_t* __restrict__ counts,
+           uint32_t* __restrict__ block_sums, uint32_t* __restrict__ stats) {
+  __shared__ uint32_t warp_tot[8];
+  const int64_t i = (int64_t)blockIdx.x * kBinBlock + threadIdx.x;
+  uint32_t cnt = 0, dk = 0;
+  if (i < n) {
+    const float ux = us[2 * i], uy = us[2 * i + 1];
+    if (bin) {
+      const float depth = depths[i];
+      if (!(depth < kMinDepth)) {
+        const float xs = (float)areas[2 * i], ys = (float)areas[2 * i + 1];
+        const TileRect r = tile_rect(ux, uy, xs, ys, gx, gy);
+        cnt = (r.y1 - r.y0) * (r.x1 - r.x0);
+        if (cnt == 0) {
+          depths[i] = kBadDepth;
+          areas[2 * i] = 0;
+          areas[2 * i + 1] = 0;
+        } else {
+          rects[i] = make_uint2(r.x0 | (r.y0 << 16), r.x1 | (r.y1 << 16));
+          dk = __float2uint_rz(depth * 1000);
+        }
+      }
+      counts[i] = cnt;
+      dkeys[i] = dk;
+    }
+    const float qa = cinv[3 * i], qb = cinv[3 * i + 1], qc = cinv[3 * i + 2];
+    const float a = alphas[i];
+    const float cut = 2.f * logf(a / kAlphaMin) + kCutMargin;
+    float xmin = -INFINITY, xmax = INFINITY, ymin = -INFINITY, ymax = INFINITY;
+    if (cut < 0.f) {  // alpha < 0.002: never blends, empty box
+      xmin = ymin = INFINITY;
+      xmax = ymax = -INFINITY;
+    } else if (isfinite(cut) && isfinite(ux) && isfinite(uy)) {
+      const float det = qa * qc - qb * qb;
+      const float kappa = (qa + qc) * (qa + qc) / det;
+      if (det > 0.f && qa > 0.f && qc > 0.f && kappa < 1e5f) {
+        const float c2 = cut * (1.f + 4e-6f * kappa) + 1e-3f;
+        const float hx = sqrtf(c2 * qc / det) * 1.0001f + 0.02f;
+        const float hy = sqrtf(c2 * qa / det) * 1.0001f + 0.02f;
+        if (isfinite(hx) && isfinite(hy)) {
+          xmin = ux - hx;
+          xmax = ux + hx;
+          ymin = uy - hy;
+          ymax = uy + hy;
+        }
+      }
+    }
+    float4* rec = records + i * V;
+    float f[4 * 5];
+#pragma unroll
+    for (int k = 0; k < 20; ++k) f[k] = 0.f;
+    f[0] = xmin; f[1] = xmax; f[2] = ymin; f[3] = ymax;
+    f[4] = ux; f[5] = uy; f[6] = qa; f[7] = qb;
+    f[8] = qc; f[9] = cut; f[10] = a;
+#pragma unroll
+    for (int k = 0; k < kMaxChannels; ++k)
+      if (k < C) f[11 + k] = ld(feats, i * C + k);
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+      if (v < V) rec[v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
+  }
+  if (!bin) return;
+  uint32_t tot;
+  block_excl_scan256(cnt, warp_tot, &tot);
+  // block max of the depth keys of binned Gaussians
+  uint32_t m = dk;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(stats + 1, m);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+}
+
+// Single-block exclusive scan of the per-block patch counts; writes the
+// total M (low/high words) into stats[0] / stats[3].
+__global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__ sums, int64_t nb,
+                                                          uint32_t* __restrict__ stats) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ unsigned long long carry;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0ull;
+  __syncthreads();
+  for (int64_t base = 0; base < nb; base += 1024 * 4) {
+    uint32_t v[4], s = 0;
+    const int64_t j0 = base + (int64_t)threadIdx.x * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = (j0 + k < nb) ? sums[j0 + k] : 0u;
+      s += v[k];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    uint32_t wbase = 0, btot = 0;
+    for (int k = 0; k < 32; ++k) {
+      const uint32_t t = warp_tot[k];
+      wbase += (k < w) ? t : 0u;
+      btot += t;
+    }
+    uint32_t run = (uint32_t)carry + wbase + incl - s;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (j0 + k < nb) sums[j0 + k] = run;
+      run += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) carry += btot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    stats[0] = (uint32_t)carry;
+    stats[3] = (uint32_t)(carry >> 32);
+  }
+}
+
+// Tile index of a sort key (the depth key occupies the low `dkey_bits`).
+template <typename KT>
+__device__ __forceinline__ uint32_t key_tile(KT k, int dkey_bits) {
+  return dkey_bits >= (int)(8 * sizeof(KT)) ? 0u : (uint32_t)(k >> dkey_bits);
+}
+template <typename KT>
+__device__ __forceinline__ KT make_key(uint32_t tile, uint32_t dk, int dkey_bits) {
+  return dkey_bits >= (int)(8 * sizeof(KT)) ? (KT)dk : (((KT)tile << dkey_bits) | (KT)dk);
+}
+
+// ------------------------------------------------------------------ emit
+// Key emission (createKeys, gsplatcu/kernel.cu:96-124) done cooperatively by
+// each warp: the warp's 32 Gaussians own one contiguous run of patch slots,
+// and the lanes fill it slot by slot (coalesced), each slot locating its
+// Gaussian by binary search over the warp's inclusive counts.
+template <typename KT>
+__global__ void __launch_bounds__(kBinBlock)
+    k_emit(int64_t n, uint32_t gx, int dkey_bits, const uint2* __restrict__ rects,
+           const uint32_t* __restrict__ dkeys, const uint32_t* __restrict__ counts,
+           const uint32_t* __restrict__ block_offs, KT* __restrict__ keys,
+           int32_t* __restrict__ vals) {
+  __shared__ uint32_t warp_tot[8];
+  __shared__ uint32_t s_incl[8][32];
+  __shared__ uint2 s_rect[8][32];
+  __shared__ uint32_t s_dk[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t i = (int64_t)blockIdx.x * kBinBlock + threadIdx.x;
+  const uint32_t c = (i < n) ? counts[i] : 0u;
+  const uint32_t excl = block_excl_scan256(c, warp_tot, nullptr);
+  // inclusive count within the warp
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t warp_total = __shfl_sync(0xffffffffu, incl, 31);
+  const uint32_t warp_start = block_offs[blockIdx.x] + __shfl_sync(0xffffffffu, excl, 0);
+  s_incl[w][lane] = incl;
+  s_rect[w][lane] = (c > 0) ? rects[i] : make_uint2(0u, 0u);
+  s_dk[w][lane] = (c > 0) ? dkeys[i] : 0u;
+  __syncwarp();
+  const int64_t first = (int64_t)blockIdx.x * kBinBlock + w * 32;
+  for (uint32_t p = lane; p < warp_total; p += 32) {
+    int L = 0;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1)
+      if (s_incl[w][L + s - 1] <= p) L += s;
+    const uint32_t local = p - (L ? s_incl[w][L - 1] : 0u);
+    const uint2 r = s_rect[w][L];
+    const uint32_t x0 = r.x & 0xffffu, y0 = r.x >> 16, x1 = r.y & 0xffffu;
+    const uint32_t wdt = x1 - x0;
+    const uint32_t ty = local / wdt, tx = local - ty * wdt;
+    const uint32_t tile = (y0 + ty) * gx + (x0 + tx);
+    const uint32_t slot = warp_start + p;
+    keys[slot] = make_key<KT>(tile, s_dk[w][L], dkey_bits);
+    vals[slot] = (int32_t)(first + L);
+  }
+}
+
+// ------------------------------------------------------------ radix sort
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per block
+
+template <typename KT>
+__global__ void __launch_bounds__(kSortThreads)
+    k_radix_upsweep(const KT* __restrict__ keys, int64_t M, int shift, uint32_t mask,
+                    uint32_t* __restrict__ hist, int64_t nblocks) {
+  __shared__ uint32_t h[8][256];
+  const int w = threadIdx.x >> 5;
+  for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) (&h[0][0])[k] = 0u;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int r = 0; r < kSortItems; ++r) {
+    const int64_t idx = base + r * kSortThreads + threadIdx.x;
+    if (idx < M) atomicAdd(&h[w][(uint32_t)(keys[idx] >> shift) & mask], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x <= mask) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += h[k][threadIdx.x];
+    hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = s;
+  }
+}
+
+// One block per digit: exclusive scan of that digit's per-block counts.
+__global__ void __launch_bounds__(256)
+    k_radix_scan(uint32_t* __restrict__ hist, int64_t nblocks, uint32_t* __restrict__ digit_tot) {
+  __shared__ uint32_t warp_tot[8];
+  uint32_t* row = hist + (int64_t)blockIdx.x * nblocks;
+  uint32_t carry = 0;
+  for (int64_t base = 0; base < nblocks; base += 256) {
+    const int64_t j = base + threadIdx.x;
+    const uint32_t v = (j < nblocks) ? row[j] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan256(v, warp_tot, &tot);
+    if (j < nblocks) row[j] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) digit_tot[blockIdx.x] = carry;
+}
+
+// Stable scatter of one digit pass.  Items of a block are ranked in their
+// original order (warp w owns items [512w, 512w+512), lane-minor), staged in
+// shared memory in digit order and written out in digit-contiguous runs.
+template <typename KT>
+__global__ void __launch_bounds__(kSortThreads)
+    k_radix_downsweep(const KT* __restrict__ kin, const int32_t* __restrict__ vin,
+                      KT* __restrict__ kout, int32_t* __restrict__ vout, int64_t M, int shift,
+                      uint32_t mask, const uint32_t* __restrict__ hist,
+                      const uint32_t* __restrict__ digit_tot, int64_t nblocks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  KT* sk = (KT*)smem_raw;
+  int32_t* sv = (int32_t*)(sk + kSortTile);
+  uint32_t* wcnt = (uint32_t*)(sv + kSortTile);  // [8][256]
+  uint32_t* lstart = wcnt + 8 * 256;            // [256]
+  uint32_t* gstart = lstart + 256;              // [256]
+  uint32_t* warp_tot = gstart + 256;            // [8]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) wcnt[k] = 0u;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kSortTile + w * (32 * kSortItems);
+  KT key[kSortItems];
+  int32_t val[kSortItems];
+  uint32_t dig[kSortItems], rnk[kSortItems];
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int64_t idx = base + r * 32 + lane;
+    const bool ok = idx < M;
+    key[r] = ok ? kin[idx] : (KT)0;
+    val[r] = ok ? vin[idx] : 0;
+    dig[r] = ok ? ((uint32_t)(key[r] >> shift) & mask) : 0xffffu;
+  }
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint32_t d = dig[r];
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t before = (d < 256u) ? wcnt[w * 256 + d] : 0u;
+    rnk[r] = before + __popc(peers & lt);
+    __syncwarp();
+    if (d < 256u && lane == __ffs(peers) - 1) wcnt[w * 256 + d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: exclusive offsets across warps, block-local start, global start
+  const uint32_t d = threadIdx.x;
+  uint32_t tot = 0;
+  if (d <= mask) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t c = wcnt[k * 256 + d];
+      wcnt[k * 256 + d] = tot;
+      tot += c;
+    }
+  }
+  const uint32_t dt = (d <= mask) ? digit_tot[d] : 0u;
+  const uint32_t ls = block_excl_scan256(tot, warp_tot, nullptr);
+  const uint32_t gd = block_excl_scan256(dt, warp_tot, nullptr);
+  if (d <= mask) {
+    lstart[d] = ls;
+    gstart[d] = gd + hist[(int64_t)d * nblocks + blockIdx.x];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint32_t dd = dig[r];
+    if (dd < 256u) {
+      const uint32_t pos = lstart[dd] + wcnt[w * 256 + dd] + rnk[r];
+      sk[pos] = key[r];
+      sv[pos] = val[r];
+    }
+  }
+  __syncthreads();
+  const int64_t rem = M - (int64_t)blockIdx.x * kSortTile;
+  const int cnt = rem < kSortTile ? (int)rem : kSortTile;
+  for (int j = threadIdx.x; j < cnt; j += kSortThreads) {
+    const KT k = sk[j];
+    const uint32_t dd = (uint32_t)(k >> shift) & mask;
+    const uint32_t g = gstart[dd] + (uint32_t)j - lstart[dd];
+    kout[g] = k;
+    vout[g] = sv[j];
+  }
+}
+
+// getRanges (gsplatcu/kernel.cu:165-187) on the sorted keys, with the same
+// writes -- including that the end of the only tile is left unset when
+// M == 1.  `ranges` is cleared beforehand.
+template <typename KT>
+__global__ void k_ranges(const KT* __restrict__ keys, int64_t M, int dkey_bits,
+                         int2* __restrict__ ranges) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  const uint32_t cur = key_tile(keys[p], dkey_bits);
+  const uint32_t prv = key_tile(keys[p == 0 ? 0 : p - 1], dkey_bits);
+  if (p == 0)
+    ranges[cur].x = 0;
+  else if (p == M - 1)
+    ranges[cur].y = (int)M;
+  if (prv != cur) {
+    ranges[prv].y = (int)p;
+    ranges[cur].x = (int)p;
+  }
+}
+
+// ------------------------------------------------------------ launchers
+template <typename T>
+static void pack_t(int64_t n, uint32_t gx, uint32_t gy, int C, const float* us, const float* cinv,
+                   const float* alphas, const void* feats, float* depths, int32_t* areas, bool bin,
+                   const SplatState& s, cudaStream_t st) {
+  k_pack<T><<<(int)s.n_blocks, kBinBlock, 0, st>>>(n, gx, gy, C, s.rec_vec4, us, cinv, alphas,
+                                                   (const T*)feats, depths, areas, bin, s.records,
+                                                   s.rects, s.dkeys, s.counts, s.block_sums,
+                                                   s.stats);
+}
+
+int launch_pack(int64_t n, int H, int W, int channels, const float* us, const float* cinv,
+                const float* alphas, const void* feats, int feat_dtype, float* depths,
+                int32_t* areas, bool bin, const SplatState& s, cudaStream_t st) {
+  if (bin && cudaMemsetAsync(s.stats, 0, 16 * sizeof(uint32_t), st) != cudaSuccess)
+    return check_launch("splat_pack (memset)");
+  if (n == 0) return GSB_OK;
+  const uint32_t gx = (uint32_t)div_up(W, kTile), gy = (uint32_t)div_up(H, kTile);
+  if (feat_dtype == GSB_DTYPE_BF16)
+    pack_t<__nv_bfloat16>(n, gx, gy, channels, us, cinv, alphas, feats, depths, areas, bin, s, st);
+  else
+    pack_t<float>(n, gx, gy, channels, us, cinv, alphas, feats, depths, areas, bin, s, st);
+  return check_launch("splat_pack");
+}
+
+int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  k_scan_block_sums<<<1, 1024, 0, st>>>(s.block_sums, s.n_blocks, s.stats);
+  return check_launch("splat_scan");
+}
+
+static int bit_length(uint64_t v) {
+  int b = 0;
+  while (v) {
+    ++b;
+    v >>= 1;
+  }
+  return b;
+}
+
+SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey) {
+  SortPlan p;
+  const int64_t gx = div_up(W, kTile), gy = div_up(H, kTile);
+  p.n_tiles = gx * gy;
+  p.M = M;
+  p.tile_bits = bit_length((uint64_t)(p.n_tiles - 1));
+  p.dkey_bits = bit_length(max_dkey);
+  p.key_bits = p.tile_bits + p.dkey_bits;
+  p.wide = p.key_bits > 32;
+  p.passes = (p.key_bits + 7) / 8;
+  p.n_sort_blocks = (M + kSortTile - 1) / kSortTile;
+  p.key_bytes = p.wide ? 8 : 4;
+  size_t off = 0;
+  p.off_keys_a = off;
+  off += align256((size_t)M * p.key_bytes);
+  p.off_keys_b = off;
+  off += align256((size_t)M * p.key_bytes);
+  p.off_vals_a = off;
+  off += align256((size_t)M * 4);
+  p.off_vals_b = off;
+  off += align256((size_t)M * 4);
+  p.off_hist = off;
+  off += align256((size_t)256 * (p.n_sort_blocks > 0 ? p.n_sort_blocks : 1) * 4);
+  p.off_digit_tot = off;
+  off += align256(256 * 4);
+  p.bytes_total = off;
+  (void)n;
+  return p;
+}
+
+template <typename KT>
+static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void* ws,
+                  int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st) {
+  char* b = (char*)ws;
+  KT* ka = (KT*)(b + p.off_keys_a);
+  KT* kb = (KT*)(b + p.off_keys_b);
+  int32_t* va = (int32_t*)(b + p.off_vals_a);
+  int32_t* vb = (int32_t*)(b + p.off_vals_b);
+  uint32_t* hist = (uint32_t*)(b + p.off_hist);
+  uint32_t* dtot = (uint32_t*)(b + p.off_digit_tot);
+  const uint32_t gx = (uint32_t)div_up(W, kTile);
+  k_emit<KT><<<(int)s.n_blocks, kBinBlock, 0, st>>>(n, gx, p.dkey_bits, s.rects, s.dkeys, s.counts,
+                                                    s.block_sums, ka,
+                                                    p.passes == 0 ? gsid_out : va);
+  int rc = check_launch("splat_sort (emit)");
+  if (rc) return rc;
+  const size_t smem = (size_t)kSortTile * (sizeof(KT) + 4) + (8 * 256 + 256 + 256 + 8) * 4;
+  if (cudaFuncSetAttribute(k_radix_downsweep<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return check_launch("splat_sort (smem attribute)");
+  KT* ks = ka;
+  KT* kd = kb;
+  int32_t* vs = va;
+  int32_t* vd = vb;
+  const int nbk = (int)p.n_sort_blocks;
+  for (int pass = 0; pass < p.passes; ++pass) {
+    const int shift = 8 * pass;
+    const int bits = (p.key_bits - shift) < 8 ? (p.key_bits - shift) : 8;
+    const uint32_t mask = (1u << bits) - 1u;
+    int32_t* vdst = (pass == p.passes - 1) ? gsid_out : vd;
+    k_radix_upsweep<KT><<<nbk, kSortThreads, 0, st>>>(ks, p.M, shift, mask, hist, p.n_sort_blocks);
+    k_radix_scan<<<(int)mask + 1, 256, 0, st>>>(hist, p.n_sort_blocks, dtot);
+    k_radix_downsweep<KT><<<nbk, kSortThreads, smem, st>>>(ks, vs, kd, vdst, p.M, shift, mask,
+                                                           hist, dtot, p.n_sort_blocks);
+    rc = check_launch("splat_sort (radix pass)");
+    if (rc) return rc;
+    KT* kt = ks;
+    ks = kd;
+    kd = kt;
+    int32_t* vt = vs;
+    vs = vd;
+    vd = vt;
+  }
+  k_ranges<KT><<<div_up(p.M, 256), 256, 0, st>>>(ks, p.M, p.dkey_bits, (int2*)ranges_out);
+  return check_launch("splat_sort (ranges)");
+}
+
+int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s, void* ws,
+                int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st) {
+  (void)H;
+  if (cudaMemsetAsync(ranges_out, 0, (size_t)p.n_tiles * 2 * sizeof(int32_t), st) != cudaSuccess)
+    return check_launch("splat_sort (memset)");
+  if (p.M == 0) return GSB_OK;
+  return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, st)
+                : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, st);
+}
+
+}  // namespace gsb

@@ -1,0 +1,281 @@
+// extern "C" entry points of libgsplat_b200.so (declared in gsplat_b200.h):
+// argument validation, workspace carving and kernel launches.  No entry point
+// allocates device memory or synchronises, except gsb_splat_counts, which
+// must return the patch count to the host.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "gsb_common.cuh"
+#include "gsb_internal.h"
+
+namespace gsb {
+
+static thread_local char g_err[512] = {0};
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return GSB_ERR_CUDA;
+  }
+  return GSB_OK;
+}
+
+// lab2rgb -- gsplatcu/kernel.cu:1385-1428: CIE L*a*b* (L in [0,1]) -> sRGB.
+__device__ __forceinline__ float lab_finv(float t) {
+  const float delta = 6.0f / 29.0f;
+  return (t > delta) ? t * t * t : 3.f * delta * delta * (t - 4.f / 29.f);
+}
+__device__ __forceinline__ float srgb_gamma(float c) {
+  return (c <= 0.0031308f) ? 12.92f * c : 1.055f * powf(c, 1.f / 2.4f) - 0.055f;
+}
+__global__ void k_lab2rgb(int H, int W, const float* __restrict__ lab, float* __restrict__ rgb) {
+  const int px = blockIdx.x * blockDim.x + threadIdx.x;
+  const int py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= W || py >= H) return;
+  const int64_t p = (int64_t)py * W + px, P = (int64_t)H * W;
+  const float L = lab[p] * 100.f, a = lab[P + p], b = lab[2 * P + p];
+  const float fy = (L + 16.f) / 116.f, fx = a / 500.f + fy, fz = fy - b / 200.f;
+  const float X = 0.95047f * lab_finv(fx), Y = 1.00000f * lab_finv(fy), Z = 1.08883f * lab_finv(fz);
+  const float r = fmaxf(0.f, fminf(1.f, 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z));
+  const float g = fmaxf(0.f, fminf(1.f, -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z));
+  const float bl = fmaxf(0.f, fminf(1.f, 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z));
+  rgb[p] = srgb_gamma(r);
+  rgb[P + p] = srgb_gamma(g);
+  rgb[2 * P + p] = srgb_gamma(bl);
+}
+
+int launch_lab2rgb(int H, int W, const float* lab, float* rgb, cudaStream_t st) {
+  if (H == 0 || W == 0) return GSB_OK;
+  dim3 block(16, 16), grid(div_up(W, 16), div_up(H, 16));
+  k_lab2rgb<<<grid, block, 0, st>>>(H, W, lab, rgb);
+  return check_launch("lab2rgb");
+}
+
+static bool valid_sh_dim(int nb) { return nb == 1 || nb == 4 || nb == 9 || nb == 16; }
+static bool valid_dtype(int d) { return d == GSB_DTYPE_F32 || d == GSB_DTYPE_BF16; }
+
+}  // namespace gsb
+
+using namespace gsb;
+
+#define ST(s) ((cudaStream_t)(s))
+#define GSB_API extern "C" __attribute__((visibility("default")))
+
+GSB_API const char* gsb_last_error(void) { return g_err; }
+GSB_API int gsb_version(void) { return 100; }
+
+GSB_API int gsb_project(int64_t n, const float* pws, const float* Rcw, const float* tcw, float fx,
+                        float fy, float cx, float cy, float* us, float* pcs, float* depths,
+                        float* du_dpcs, void* stream) {
+  GSB_CHECK_ARG(n >= 0, "project: n < 0");
+  GSB_CHECK_ARG(n == 0 || (pws && Rcw && tcw && us && pcs && depths), "project: null pointer");
+  return launch_project(n, pws, Rcw, tcw, fx, fy, cx, cy, us, pcs, depths, du_dpcs, ST(stream));
+}
+
+GSB_API int gsb_compute_cov3d(int64_t n, const float* rots, const float* scales,
+                              const float* depths, float* cov3ds, float* dq, float* ds,
+                              void* stream) {
+  GSB_CHECK_ARG(n >= 0, "computeCov3D: n < 0");
+  GSB_CHECK_ARG(n == 0 || (rots && scales && depths && cov3ds), "computeCov3D: null pointer");
+  GSB_CHECK_ARG((dq == nullptr) == (ds == nullptr), "computeCov3D: pass both Jacobians or none");
+  GSB_CHECK_ARG(((uintptr_t)rots & 15) == 0, "computeCov3D: rots must be 16-byte aligned");
+  return launch_cov3d(n, rots, scales, depths, cov3ds, dq, ds, ST(stream));
+}
+
+GSB_API int gsb_compute_cov2d(int64_t n, const float* cov3ds, const float* pcs, const float* Rcw,
+                              const float* depths, float fx, float fy, float width, float height,
+                              float* cov2ds, float* d3, float* dp, void* stream) {
+  GSB_CHECK_ARG(n >= 0, "computeCov2D: n < 0");
+  GSB_CHECK_ARG(n == 0 || (cov3ds && pcs && Rcw && depths && cov2ds), "computeCov2D: null pointer");
+  GSB_CHECK_ARG((d3 == nullptr) == (dp == nullptr), "computeCov2D: pass both Jacobians or none");
+  // tan of the half field of view, formed in FP32 as gsplatcu/gausplat.cu:357-358
+  const float tanx = width / (2 * fx);
+  const float tany = height / (2 * fy);
+  return launch_cov2d(n, cov3ds, pcs, Rcw, depths, fx, fy, tanx, tany, cov2ds, d3, dp, ST(stream));
+}
+
+GSB_API int gsb_inverse_cov2d(int64_t n, const float* cov2ds, float* depths, float* cinv2ds,
+                              int32_t* areas, float* dcinv, void* stream) {
+  GSB_CHECK_ARG(n >= 0, "inverseCov2D: n < 0");
+  GSB_CHECK_ARG(n == 0 || (cov2ds && depths && cinv2ds && areas), "inverseCov2D: null pointer");
+  return launch_inverse_cov2d(n, cov2ds, depths, cinv2ds, areas, dcinv, ST(stream));
+}
+
+GSB_API int gsb_sh2weight(int64_t n, const void* shs, int shs_dtype, int sh_dim, int K,
+                          const float* pws, const float* twc, float* weights, float* dshs,
+                          float* dpws, void* stream) {
+  GSB_CHECK_ARG(n >= 0, "sh2Weight: n < 0");
+  GSB_CHECK_ARG(K >= 1 && K <= GSB_MAX_CHANNELS, "sh2Weight: num_palette must be in [1, %d], got %d",
+                GSB_MAX_CHANNELS, K);
+  GSB_CHECK_ARG(valid_sh_dim(sh_dim), "sh2Weight: SH bands per channel must be 1, 4, 9 or 16, got %d",
+                sh_dim);
+  GSB_CHECK_ARG(valid_dtype(shs_dtype), "sh2Weight: unsupported shs dtype %d", shs_dtype);
+  GSB_CHECK_ARG(n == 0 || (shs && pws && twc && weights), "sh2Weight: null pointer");
+  GSB_CHECK_ARG((dshs == nullptr) == (dpws == nullptr), "sh2Weight: pass both Jacobians or none");
+  return launch_sh2feat(n, shs, shs_dtype, sh_dim, K, pws, twc, weights, dshs, dpws, ST(stream));
+}
+
+GSB_API int gsb_sh2color(int64_t n, const void* shs, int shs_dtype, int sh_dim, const float* pws,
+                         const float* twc, float* colors, float* dshs, float* dpws, void* stream) {
+  GSB_CHECK_ARG(n >= 0, "sh2Color: n < 0");
+  GSB_CHECK_ARG(valid_sh_dim(sh_dim), "sh2Color: SH bands must be 1, 4, 9 or 16, got %d", sh_dim);
+  GSB_CHECK_ARG(valid_dtype(shs_dtype), "sh2Color: unsupported shs dtype %d", shs_dtype);
+  GSB_CHECK_ARG(n == 0 || (shs && pws && twc && colors), "sh2Color: null pointer");
+  GSB_CHECK_ARG((dshs == nullptr) == (dpws == nullptr), "sh2Color: pass both Jacobians or none");
+  return launch_sh2feat(n, shs, shs_dtype, sh_dim, 3, pws, twc, colors, dshs, dpws, ST(stream));
+}
+
+static int check_lowrank(const char* op, int K, int P, int Q, int rank, int dtype, int* L) {
+  GSB_CHECK_ARG(K >= 1 && K <= GSB_MAX_CHANNELS, "%s: num_palette must be in [1, %d], got %d", op,
+                GSB_MAX_CHANNELS, K);
+  GSB_CHECK_ARG(P >= 1 && Q >= 1 && rank >= 1, "%s: P, Q and rank must be positive", op);
+  GSB_CHECK_ARG((P * Q) % K == 0, "%s: P*Q (%d) must be a multiple of num_palette (%d)", op, P * Q, K);
+  *L = P * Q / K;
+  GSB_CHECK_ARG(*L == 0 || *L == 3 || *L == 8 || *L == 15,
+                "%s: P*Q/K = %d higher-order SH coefficients; must be 3, 8 or 15", op, *L);
+  GSB_CHECK_ARG(valid_dtype(dtype), "%s: unsupported dtype %d", op, dtype);
+  return GSB_OK;
+}
+
+GSB_API int gsb_sh2weight_fast(int64_t n, const void* dc, const void* A, const void* B, int dtype,
+                               int K, int P, int Q, int rank, const float* pws, const float* twc,
+                               float* weights, float* ddc, float* ylm, void* stream) {
+  int L = 0;
+  int rc = check_lowrank("sh2Weight_fast", K, P, Q, rank, dtype, &L);
+  if (rc) return rc;
+  GSB_CHECK_ARG(n >= 0, "sh2Weight_fast: n < 0");
+  GSB_CHECK_ARG(n == 0 || (dc && A && B && pws && twc && weights), "sh2Weight_fast: null pointer");
+  return launch_sh2weight_lowrank(n, dc, A, B, dtype, K, P, Q, rank, L, pws, twc, weights, ddc,
+                                  L > 0 ? ylm : nullptr, ST(stream));
+}
+
+GSB_API int gsb_sh2weight_fast_backward(int64_t n, const void* A, const void* B, int dtype,
+                                        const float* ylm, const float* dw, int K, int P, int Q,
+                                        int rank, float* dA, float* dB, void* stream) {
+  int L = 0;
+  int rc = check_lowrank("sh2Weight_fast_B", K, P, Q, rank, dtype, &L);
+  if (rc) return rc;
+  GSB_CHECK_ARG(n >= 0, "sh2Weight_fast_B: n < 0");
+  GSB_CHECK_ARG(n == 0 || (A && B && dw && dA && dB && (L == 0 || ylm)),
+                "sh2Weight_fast_B: null pointer");
+  return launch_sh2weight_lowrank_b(n, A, B, dtype, ylm, dw, K, P, Q, rank, L, dA, dB, ST(stream));
+}
+
+GSB_API int gsb_lab2rgb(int height, int width, const float* lab, float* rgb, void* stream) {
+  GSB_CHECK_ARG(height >= 0 && width >= 0, "lab2rgb: negative size");
+  GSB_CHECK_ARG((height == 0 || width == 0) || (lab && rgb), "lab2rgb: null pointer");
+  return launch_lab2rgb(height, width, lab, rgb, ST(stream));
+}
+
+// ----------------------------------------------------------------- splat
+static int check_image(const char* op, int64_t n, int H, int W, int C) {
+  GSB_CHECK_ARG(n >= 0 && n < (int64_t)INT32_MAX, "%s: Gaussian count %lld out of range", op,
+                (long long)n);
+  GSB_CHECK_ARG(H >= 0 && W >= 0, "%s: negative image size", op);
+  GSB_CHECK_ARG((int64_t)div_up(W, kTile) < 65536 && (int64_t)div_up(H, kTile) < 65536,
+                "%s: image too large (%d x %d)", op, W, H);
+  GSB_CHECK_ARG(C >= 1 && C <= GSB_MAX_CHANNELS, "%s: channels must be in [1, %d], got %d", op,
+                GSB_MAX_CHANNELS, C);
+  return GSB_OK;
+}
+
+GSB_API size_t gsb_splat_state_bytes(int64_t n, int channels) {
+  if (n < 0 || channels < 1 || channels > GSB_MAX_CHANNELS) return 0;
+  return splat_state_bytes(n, channels);
+}
+
+GSB_API int gsb_splat_pack(int64_t n, int height, int width, int channels, const float* us,
+                           const float* cinv2ds, const float* alphas, const void* feats,
+                           int feat_dtype, float* depths, int32_t* areas, void* state,
+                           void* stream) {
+  int rc = check_image("splat_pack", n, height, width, channels);
+  if (rc) return rc;
+  GSB_CHECK_ARG(valid_dtype(feat_dtype), "splat_pack: unsupported feature dtype %d", feat_dtype);
+  GSB_CHECK_ARG(state && ((uintptr_t)state & 255) == 0, "splat_pack: state must be 256-byte aligned");
+  GSB_CHECK_ARG(n == 0 || (us && cinv2ds && alphas && feats && depths && areas),
+                "splat_pack: null pointer");
+  const SplatState s = carve_state(state, n, channels);
+  rc = launch_pack(n, height, width, channels, us, cinv2ds, alphas, feats, feat_dtype, depths,
+                   areas, true, s, ST(stream));
+  if (rc) return rc;
+  return launch_count_scan(n, s, ST(stream));
+}
+
+GSB_API int gsb_splat_counts(int64_t n, const void* state, uint32_t* host_out, void* stream) {
+  GSB_CHECK_ARG(n >= 0 && state && host_out, "splat_counts: bad argument");
+  const SplatState s = carve_state((void*)state, n, 1);
+  uint32_t v[4];
+  if (cudaMemcpyAsync(v, s.stats, sizeof(v), cudaMemcpyDeviceToHost, ST(stream)) != cudaSuccess ||
+      cudaStreamSynchronize(ST(stream)) != cudaSuccess)
+    return check_launch("splat_counts");
+  GSB_CHECK_ARG(v[3] == 0 && v[0] < (uint32_t)INT32_MAX,
+                "splat_counts: patch count exceeds the int32 index range");
+  host_out[0] = v[0];
+  host_out[1] = v[1];
+  return GSB_OK;
+}
+
+GSB_API size_t gsb_splat_sort_bytes(int64_t n, int height, int width, int64_t patches,
+                                    uint32_t max_depth_key) {
+  if (n < 0 || height < 0 || width < 0 || patches < 0) return 0;
+  return make_sort_plan(n, height, width, patches, max_depth_key).bytes_total;
+}
+
+GSB_API int gsb_splat_sort(int64_t n, int height, int width, int64_t patches,
+                           uint32_t max_depth_key, const void* state, void* sort_ws,
+                           int32_t* gsid_out, int32_t* ranges_out, void* stream) {
+  int rc = check_image("splat_sort", n, height, width, 1);
+  if (rc) return rc;
+  GSB_CHECK_ARG(patches >= 0 && patches < (int64_t)INT32_MAX, "splat_sort: bad patch count");
+  GSB_CHECK_ARG(state && ranges_out, "splat_sort: null pointer");
+  GSB_CHECK_ARG(patches == 0 || (sort_ws && gsid_out), "splat_sort: null workspace/output");
+  const SortPlan p = make_sort_plan(n, height, width, patches, max_depth_key);
+  const SplatState s = carve_state((void*)state, n, 1);
+  return launch_sort(p, n, height, width, s, sort_ws, gsid_out, ranges_out, ST(stream));
+}
+
+GSB_API int gsb_splat_draw(int64_t n, int height, int width, int channels, const int32_t* ranges,
+                           const int32_t* gsid, const void* state, float tau_init, float* out,
+                           int32_t* contrib, float* final_tau, void* stream) {
+  int rc = check_image("splat_draw", n, height, width, channels);
+  if (rc) return rc;
+  GSB_CHECK_ARG(ranges && state && out && contrib && final_tau, "splat_draw: null pointer");
+  const SplatState s = carve_state((void*)state, n, channels);
+  return launch_draw(n, height, width, channels, ranges, gsid, s, tau_init, out, contrib,
+                     final_tau, ST(stream));
+}
+
+GSB_API int gsb_splat_backward(int64_t n, int height, int width, int channels, const float* us,
+                               const float* cinv2ds, const float* alphas, const void* feats,
+                               int feat_dtype, const int32_t* ranges, const int32_t* gsid,
+                               const int32_t* contrib, const float* final_tau,
+                               const float* dloss_dout, const float* dloss_dtau, void* state,
+                               float* dfeats, float* dalphas, float* dus, float* dcinv2ds,
+                               void* stream) {
+  int rc = check_image("splat_backward", n, height, width, channels);
+  if (rc) return rc;
+  GSB_CHECK_ARG(valid_dtype(feat_dtype), "splat_backward: unsupported feature dtype %d", feat_dtype);
+  GSB_CHECK_ARG(state && ((uintptr_t)state & 255) == 0,
+                "splat_backward: state must be 256-byte aligned");
+  GSB_CHECK_ARG(ranges && contrib && final_tau && dloss_dout && dfeats, "splat_backward: null pointer");
+  const bool geom = dalphas || dus || dcinv2ds;
+  GSB_CHECK_ARG(!geom || (dalphas && dus && dcinv2ds),
+                "splat_backward: pass all of dalphas/dus/dcinv2ds or none");
+  GSB_CHECK_ARG(!dloss_dtau || geom, "splat_backward: dloss_dtau needs the geometry outputs");
+  GSB_CHECK_ARG(n == 0 || (us && cinv2ds && alphas && feats), "splat_backward: null input");
+  const SplatState s = carve_state(state, n, channels);
+  rc = launch_pack(n, height, width, channels, us, cinv2ds, alphas, feats, feat_dtype, nullptr,
+                   nullptr, false, s, ST(stream));
+  if (rc) return rc;
+  return launch_draw_backward(n, height, width, channels, ranges, gsid, s, contrib, final_tau,
+                              dloss_dout, dloss_dtau, dfeats, dalphas, dus, dcinv2ds, ST(stream));
+}

@@ -1,0 +1,85 @@
+// Shared definitions of the B200 palette-weight rasterizer (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "gsplat_b200.h"
+
+namespace gsb {
+
+// ---------------------------------------------------------------- constants
+// Tile edge and thresholds of the reference rasterizer
+// (gsplatcu/common.cuh:13-14, gsplatcu/kernel.cu:10-12, 258-265).
+constexpr int kTile = 16;
+constexpr int kTilePixels = kTile * kTile;
+constexpr float kMinDepth = 0.2f;
+constexpr float kBadDepth = -1.f;
+constexpr float kAlphaMax = 0.99f;
+constexpr float kAlphaMin = 0.002f;
+constexpr float kTransMin = 0.0001f;
+constexpr int kMaxChannels = 8;  // MAX_SPLAT_DIM of the reference
+
+// Real spherical-harmonic basis constants for l <= 3, stored in FP32: the
+// B200 path evaluates the basis in FP32 only (gsplatcu/common.cuh:29-44 holds
+// the same values as double literals).
+constexpr float SH_C0 = 0.28209479177387814f;
+constexpr float SH_C1 = 0.4886025119029199f;
+constexpr float SH_C2_0 = 1.0925484305920792f;
+constexpr float SH_C2_2 = 0.31539156525252005f;
+constexpr float SH_C2_4 = 0.5462742152960396f;
+constexpr float SH_C3_0 = 0.5900435899266435f;
+constexpr float SH_C3_1 = 2.890611442640554f;
+constexpr float SH_C3_2 = 0.4570457994644658f;
+constexpr float SH_C3_3 = 0.3731763325901154f;
+constexpr float SH_C3_5 = 1.445305721320277f;
+
+// Margin (in Mahalanobis units) added to the exact skip threshold
+// 2 ln(alpha / 0.002): a pixel farther than the cut is guaranteed to give
+// alpha' < 0.002 in the reference's own FP32 evaluation, so skipping it never
+// changes a result; pixels inside it are evaluated exactly as the reference.
+constexpr float kCutMargin = 1e-3f;
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// ------------------------------------------------------------ element loads
+// Per-Gaussian colour parameters may be stored in FP32 or BF16 (selected at
+// run time by GSB_DTYPE_*); all arithmetic is FP32.
+__device__ __forceinline__ float ld(const float* p, int64_t i) { return __ldg(p + i); }
+__device__ __forceinline__ float ld(const __nv_bfloat16* p, int64_t i) {
+  return __bfloat162float(p[i]);
+}
+
+// Reference Mahalanobis form (gsplatcu/common.cuh:89-92).  The operand order
+// is kept as written there so that the FP32 result, after the compiler's FMA
+// contraction, is the same value the reference computes: the per-pixel skip
+// (alpha' < 0.002) and stop (T < 1e-4) decisions then agree with it exactly.
+__device__ __forceinline__ float maha_sq(float qa, float qb, float qc, float dx, float dy) {
+  return qa * dx * dx + qc * dy * dy + 2 * qb * dx * dy;
+}
+
+// Packed per-Gaussian record read by the compositing kernels.  Vector 0 holds
+// the conservative screen-space support box (pixels outside it give
+// alpha' < 0.002), vector 1 the centre and conic, vector 2 the skip cut,
+// opacity and the first feature, then the remaining features.
+//   v0: xmin xmax ymin ymax | v1: ux uy qa qb | v2: qc cut alpha f0 | v3..: f1..
+template <int K>
+struct RecordLayout {
+  static constexpr int kFloats = ((11 + K) + 3) / 4 * 4;
+  static constexpr int kVec4 = kFloats / 4;
+};
+
+// ----------------------------------------------------------- error plumbing
+void set_error(const char* fmt, ...);
+int check_launch(const char* what);
+
+}  // namespace gsb
+
+#define GSB_CHECK_ARG(cond, ...)        \
+  do {                                  \
+    if (!(cond)) {                      \
+      gsb::set_error(__VA_ARGS__);      \
+      return GSB_ERR_INVALID_ARGUMENT;  \
+    }                                   \
+  } while (0)

@@ -1,0 +1,278 @@
+// Per-Gaussian geometry and spherical-harmonic evaluation (device functions).
+//
+// The FP32 operation order of every value the rasterizer consumes (projected
+// centre, depth, 3D/2D covariance, conic, 3-sigma extents) is kept as the
+// reference computes it (gsplatcu/kernel.cu:379-663), including small matrix
+// products accumulated from zero in (row, column, inner) order.  Compiled with
+// the same FMA contraction rules, the results are then bit-identical, so tile
+// rectangles, sort keys and the per-pixel skip/stop decisions downstream agree
+// with the reference exactly.  Jacobians are written in closed form.
+#pragma once
+
+#include "gsb_common.cuh"
+
+namespace gsb {
+
+// C[R x Cc] = A[R x In] * B[In x Cc], accumulated from zero in k order.
+template <int Rr, int In, int Cc>
+__device__ __forceinline__ void mat_mul(const float* A, const float* B, float* Cm) {
+#pragma unroll
+  for (int i = 0; i < Rr; ++i)
+#pragma unroll
+    for (int j = 0; j < Cc; ++j) {
+      float acc = 0.f;
+#pragma unroll
+      for (int k = 0; k < In; ++k) acc += A[i * In + k] * B[k * Cc + j];
+      Cm[i * Cc + j] = acc;
+    }
+}
+
+// ---------------------------------------------------------------- project
+struct Projected {
+  float x, y, z;  // camera-space centre
+  float ux, uy;   // pixel centre
+  bool valid;     // z >= 0.2
+};
+
+__device__ __forceinline__ Projected project_point(float3 pw, const float* Rcw, float3 t, float fx,
+                                                   float fy, float cx, float cy) {
+  float p[3] = {pw.x, pw.y, pw.z};
+  float pc[3];
+  mat_mul<3, 3, 1>(Rcw, p, pc);
+  Projected r;
+  r.x = pc[0] + t.x;
+  r.y = pc[1] + t.y;
+  r.z = pc[2] + t.z;
+  r.valid = !(r.z < kMinDepth);
+  if (r.valid) {
+    const float z_inv = 1.f / r.z;
+    const float x_fx = r.x * fx;
+    const float y_fy = r.y * fy;
+    r.ux = x_fx * z_inv + cx;
+    r.uy = y_fy * z_inv + cy;
+  } else {
+    r.ux = r.uy = 0.f;
+  }
+  return r;
+}
+
+// ------------------------------------------------------------ covariance
+// Rotation of an unnormalised quaternion (w, x, y, z), row-major.
+__device__ __forceinline__ void quat_rotation(float4 q, float* R) {
+  const float w = q.x, x = q.y, y = q.z, z = q.w;
+  const float xx = x * x, yy = y * y, zz = z * z;
+  const float xy = x * y, xz = x * z, yz = y * z;
+  const float xw = x * w, yw = y * w, zw = z * w;
+  R[0] = 1.f - 2.f * (yy + zz);
+  R[1] = 2.f * (xy - zw);
+  R[2] = 2.f * (xz + yw);
+  R[3] = 2.f * (xy + zw);
+  R[4] = 1.f - 2.f * (xx + zz);
+  R[5] = 2.f * (yz - xw);
+  R[6] = 2.f * (xz - yw);
+  R[7] = 2.f * (yz + xw);
+  R[8] = 1.f - 2.f * (xx + yy);
+}
+
+// Sigma = M M^T, M = R(q) diag(s); out = 6 upper entries (00,01,02,11,12,22).
+// Also returns M (row-major) for the Jacobians.
+__device__ __forceinline__ void covariance_3d(float4 q, float3 s, float* cov, float* Mout,
+                                              float* Rout) {
+  float R[9], M[9], Mt[9], S[9];
+  quat_rotation(q, R);
+  const float sv[3] = {s.x, s.y, s.z};
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) M[3 * r + c] = R[3 * r + c] * sv[c];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Mt[3 * c + r] = M[3 * r + c];
+  mat_mul<3, 3, 3>(M, Mt, S);
+  cov[0] = S[0];
+  cov[1] = S[1];
+  cov[2] = S[2];
+  cov[3] = S[4];
+  cov[4] = S[5];
+  cov[5] = S[8];
+  if (Mout)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Mout[k] = M[k];
+  if (Rout)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Rout[k] = R[k];
+}
+
+// 2D screen covariance of a camera-space Gaussian.  The point is clamped to
+// 1.3x the half field of view before forming the perspective Jacobian J;
+// Sigma' = (J Rcw) Sigma (J Rcw)^T; +0.3 dilation on the diagonal.
+// Mout receives J Rcw (row-major 2x3), xy the clamped x, y.
+__device__ __forceinline__ void covariance_2d(const float* cov3, float px, float py, float pz,
+                                              const float* Rcw, float fx, float fy, float tanx,
+                                              float tany, float* cov2, float* Mout, float* xy) {
+  float x = px, y = py;
+  const float z = pz;
+  const float limx = 1.3f * tanx;
+  const float limy = 1.3f * tany;
+  x = fminf(limx, fmaxf(-limx, x / z)) * z;
+  y = fminf(limy, fmaxf(-limy, y / z)) * z;
+  const float z2 = z * z;
+  const float J[6] = {fx / z, 0.0f, -(fx * x) / z2, 0.0f, fy / z, -(fy * y) / z2};
+  const float a = cov3[0], b = cov3[1], c = cov3[2], d = cov3[3], e = cov3[4], f = cov3[5];
+  const float Sg[9] = {a, b, c, b, d, e, c, e, f};
+  float M[6], MS[6], Mt[6], Sp[4];
+  mat_mul<2, 3, 3>(J, Rcw, M);
+  mat_mul<2, 3, 3>(M, Sg, MS);
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c2 = 0; c2 < 3; ++c2) Mt[2 * c2 + r] = M[3 * r + c2];
+  mat_mul<2, 3, 2>(MS, Mt, Sp);
+  cov2[0] = Sp[0] + 0.3f;
+  cov2[1] = Sp[1];
+  cov2[2] = Sp[3] + 0.3f;
+  if (Mout)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) Mout[k] = M[k];
+  if (xy) {
+    xy[0] = x;
+    xy[1] = y;
+  }
+}
+
+// Conic (inverse 2D covariance) and integer 3-sigma extents.  Returns false
+// when 1/det is NaN (the Gaussian is then dropped).
+__device__ __forceinline__ bool conic_and_extent(float a, float b, float c, float* conic,
+                                                 int* ext, float* det_inv_out) {
+  const float det_inv = 1.f / (a * c - b * b);
+  if (isnan(det_inv)) return false;
+  conic[0] = det_inv * c;
+  conic[1] = -det_inv * b;
+  conic[2] = det_inv * a;
+  ext[0] = (int)ceilf(3 * sqrtf(fabsf(a)));
+  ext[1] = (int)ceilf(3 * sqrtf(fabsf(c)));
+  if (det_inv_out) *det_inv_out = det_inv;
+  return true;
+}
+
+// ------------------------------------------------------------ tile rects
+// Tile rectangle [x0,x1) x [y0,y1) covered by centre u and extents (xs, ys),
+// clamped to the tile grid; integer conversions truncate toward zero.  The
+// upper bound rounds up as ((v + 16) - 1) / 16 in FP32.
+struct TileRect {
+  uint32_t x0, y0, x1, y1;
+};
+
+__device__ __forceinline__ TileRect tile_rect(float ux, float uy, float xs, float ys,
+                                              uint32_t gx, uint32_t gy) {
+  TileRect r;
+  r.x0 = min(gx, (uint32_t)max(0, (int)((ux - xs) / kTile)));
+  r.y0 = min(gy, (uint32_t)max(0, (int)((uy - ys) / kTile)));
+  r.x1 = min(gx, (uint32_t)max(0, (int)(((ux + xs) + kTile - 1) / kTile)));
+  r.y1 = min(gy, (uint32_t)max(0, (int)(((uy + ys) + kTile - 1) / kTile)));
+  return r;
+}
+
+// ------------------------------------------------------ spherical harmonics
+// Unit view direction and (optionally) its Jacobian w.r.t. the centre.
+__device__ __forceinline__ void view_direction(float3 pw, float3 cam, float* dir, float* nd,
+                                               float* inv_norm) {
+  const float d0 = pw.x - cam.x, d1 = pw.y - cam.y, d2 = pw.z - cam.z;
+  const float ninv = 1.f / sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+  dir[0] = d0 * ninv;
+  dir[1] = d1 * ninv;
+  dir[2] = d2 * ninv;
+  if (nd) {
+    nd[0] = d0;
+    nd[1] = d1;
+    nd[2] = d2;
+  }
+  if (inv_norm) *inv_norm = ninv;
+}
+
+// Real SH basis Y_0 .. Y_{nb-1} (nb in {1,4,9,16}) in band-major order.
+__device__ __forceinline__ void sh_basis(const float* dir, int nb, float* Y) {
+  const float x = dir[0], y = dir[1], z = dir[2];
+  Y[0] = SH_C0;
+  if (nb > 1) {
+    Y[1] = -SH_C1 * y;
+    Y[2] = SH_C1 * z;
+    Y[3] = -SH_C1 * x;
+    if (nb > 4) {
+      const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+      Y[4] = SH_C2_0 * xy;
+      Y[5] = -SH_C2_0 * yz;
+      Y[6] = SH_C2_2 * (2.f * zz - xx - yy);
+      Y[7] = -SH_C2_0 * xz;
+      Y[8] = SH_C2_4 * (xx - yy);
+      if (nb > 9) {
+        Y[9] = -SH_C3_0 * y * (3.f * xx - yy);
+        Y[10] = SH_C3_1 * xy * z;
+        Y[11] = -SH_C3_2 * y * (4.f * zz - xx - yy);
+        Y[12] = SH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy);
+        Y[13] = -SH_C3_2 * x * (4.f * zz - xx - yy);
+        Y[14] = SH_C3_5 * z * (xx - yy);
+        Y[15] = -SH_C3_0 * x * (xx - 3.f * yy);
+      }
+    }
+  }
+}
+
+// dY_l / d dir for l in [1, nb): G[3*l + r].  `ref_quirk` reproduces the
+// reference's d Y_9 / d y = C (3x^2 - 2y^2) (gsplatcu/kernel.cu:840) that the
+// compatibility Jacobian outputs return; the adjoint uses the true
+// derivative C (3x^2 - 3y^2).
+__device__ __forceinline__ void sh_basis_grad(const float* dir, int nb, bool ref_quirk, float* G) {
+  const float x = dir[0], y = dir[1], z = dir[2];
+#pragma unroll
+  for (int k = 0; k < 48; ++k) G[k] = 0.f;
+  if (nb <= 1) return;
+  G[3 * 1 + 1] = -SH_C1;
+  G[3 * 2 + 2] = SH_C1;
+  G[3 * 3 + 0] = -SH_C1;
+  if (nb <= 4) return;
+  const float xx = x * x, yy = y * y, zz = z * z;
+  G[3 * 4 + 0] = SH_C2_0 * y;
+  G[3 * 4 + 1] = SH_C2_0 * x;
+  G[3 * 5 + 1] = -SH_C2_0 * z;
+  G[3 * 5 + 2] = -SH_C2_0 * y;
+  G[3 * 6 + 0] = -2.f * SH_C2_2 * x;
+  G[3 * 6 + 1] = -2.f * SH_C2_2 * y;
+  G[3 * 6 + 2] = 4.f * SH_C2_2 * z;
+  G[3 * 7 + 0] = -SH_C2_0 * z;
+  G[3 * 7 + 2] = -SH_C2_0 * x;
+  G[3 * 8 + 0] = 2.f * SH_C2_4 * x;
+  G[3 * 8 + 1] = -2.f * SH_C2_4 * y;
+  if (nb <= 9) return;
+  G[3 * 9 + 0] = -6.f * SH_C3_0 * x * y;
+  G[3 * 9 + 1] = -SH_C3_0 * (3.f * xx - (ref_quirk ? 2.f : 3.f) * yy);
+  G[3 * 10 + 0] = SH_C3_1 * y * z;
+  G[3 * 10 + 1] = SH_C3_1 * x * z;
+  G[3 * 10 + 2] = SH_C3_1 * x * y;
+  G[3 * 11 + 0] = 2.f * SH_C3_2 * x * y;
+  G[3 * 11 + 1] = -SH_C3_2 * (4.f * zz - xx - 3.f * yy);
+  G[3 * 11 + 2] = -8.f * SH_C3_2 * y * z;
+  G[3 * 12 + 0] = -6.f * SH_C3_3 * x * z;
+  G[3 * 12 + 1] = -6.f * SH_C3_3 * y * z;
+  G[3 * 12 + 2] = SH_C3_3 * (6.f * zz - 3.f * xx - 3.f * yy);
+  G[3 * 13 + 0] = -SH_C3_2 * (4.f * zz - 3.f * xx - yy);
+  G[3 * 13 + 1] = 2.f * SH_C3_2 * x * y;
+  G[3 * 13 + 2] = -8.f * SH_C3_2 * x * z;
+  G[3 * 14 + 0] = 2.f * SH_C3_5 * x * z;
+  G[3 * 14 + 1] = -2.f * SH_C3_5 * y * z;
+  G[3 * 14 + 2] = SH_C3_5 * (xx - yy);
+  G[3 * 15 + 0] = -SH_C3_0 * (3.f * xx - 3.f * yy);
+  G[3 * 15 + 1] = 6.f * SH_C3_0 * x * y;
+}
+
+// d dir / d pw = I/|d| - d d^T/|d|^3 (symmetric 3x3).
+__device__ __forceinline__ void dir_jacobian(const float* nd, float ninv, float* J) {
+  const float n3 = ninv * ninv * ninv;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) J[3 * r + c] = -nd[r] * nd[c] * n3 + (r == c ? ninv : 0.f);
+}
+
+}  // namespace gsb

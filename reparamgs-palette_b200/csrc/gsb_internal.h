@@ -1,0 +1,72 @@
+// Internal launcher declarations shared by the .cu files of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace gsb {
+
+// preprocess.cu
+int launch_project(int64_t n, const float* pws, const float* Rcw, const float* tcw, float fx,
+                   float fy, float cx, float cy, float* us, float* pcs, float* depths, float* du,
+                   cudaStream_t st);
+int launch_cov3d(int64_t n, const float* rots, const float* scales, const float* depths,
+                 float* cov3ds, float* dq, float* ds, cudaStream_t st);
+int launch_cov2d(int64_t n, const float* cov3ds, const float* pcs, const float* Rcw,
+                 const float* depths, float fx, float fy, float tanx, float tany, float* cov2ds,
+                 float* d3, float* dp, cudaStream_t st);
+int launch_inverse_cov2d(int64_t n, const float* cov2ds, float* depths, float* cinv, int* areas,
+                         float* dcinv, cudaStream_t st);
+int launch_sh2feat(int64_t n, const void* shs, int dtype, int nb, int K, const float* pws,
+                   const float* twc, float* feat, float* dshs, float* dpws, cudaStream_t st);
+int launch_sh2weight_lowrank(int64_t n, const void* dc, const void* A, const void* B, int dtype,
+                             int K, int P, int Q, int rank, int L, const float* pws,
+                             const float* twc, float* w, float* ddc, float* ylm, cudaStream_t st);
+int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtype,
+                               const float* ylm, const float* dw, int K, int P, int Q, int rank,
+                               int L, float* dA, float* dB, cudaStream_t st);
+int launch_lab2rgb(int H, int W, const float* lab, float* rgb, cudaStream_t st);
+
+// binning.cu -- per-Gaussian binning state carved out of one caller buffer.
+struct SplatState {
+  float4* records;       // [n * rec_vec4]
+  uint2* rects;          // [n] packed 16-bit x0 | y0 << 16, x1 | y1 << 16
+  uint32_t* dkeys;       // [n] uint32(depth * 1000)
+  uint32_t* counts;      // [n] patches per Gaussian
+  uint32_t* block_sums;  // [n_blocks] -> exclusive block offsets after the scan
+  uint32_t* stats;       // [16]: 0 = M, 1 = max depth key, 2 = device error flags
+  int rec_vec4;          // float4 vectors per record
+  int64_t n_blocks;
+};
+constexpr int kBinBlock = 256;  // Gaussians per binning block
+int record_vec4(int channels);
+size_t splat_state_bytes(int64_t n, int channels);
+SplatState carve_state(void* base, int64_t n, int channels);
+
+int launch_pack(int64_t n, int H, int W, int channels, const float* us, const float* cinv,
+                const float* alphas, const void* feats, int feat_dtype, float* depths,
+                int32_t* areas, bool bin, const SplatState& s, cudaStream_t st);
+int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st);
+
+struct SortPlan {
+  int tile_bits, dkey_bits, key_bits, passes;
+  bool wide;  // 64-bit keys
+  int64_t M, n_tiles, n_sort_blocks;
+  size_t key_bytes, bytes_total;
+  size_t off_keys_a, off_keys_b, off_vals_a, off_vals_b, off_hist, off_digit_tot;
+};
+SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey);
+int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s, void* ws,
+                int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st);
+
+// raster.cu
+int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, const int32_t* gsid,
+                const SplatState& s, float tau_init, float* out, int32_t* contrib,
+                float* final_tau, cudaStream_t st);
+int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* ranges,
+                         const int32_t* gsid, const SplatState& s, const int32_t* contrib,
+                         const float* final_tau, const float* dout, const float* dtau,
+                         float* dfeat, float* dalpha, float* du, float* dconic, cudaStream_t st);
+
+}  // namespace gsb

@@ -1,0 +1,483 @@
+// Per-Gaussian preprocess kernels behind the reference's geometry and SH
+// operators (project, computeCov3D, computeCov2D, inverseCov2D, sh2Weight,
+// sh2Weight_fast(_B), sh2Color).  One thread per Gaussian; every output
+// element is written (culled Gaussians get the reference's zero values), so
+// callers need not pre-clear outputs.
+#include "gsb_geometry.cuh"
+#include "gsb_internal.h"
+
+namespace gsb {
+
+constexpr int kThreads = 256;
+
+// project -- gsplatcu/kernel.cu:618-663.
+__global__ void __launch_bounds__(kThreads)
+    k_project(int64_t n, const float* __restrict__ pws, const float* __restrict__ Rcw,
+              const float* __restrict__ tcw, float fx, float fy, float cx, float cy,
+              float* __restrict__ us, float* __restrict__ pcs, float* __restrict__ depths,
+              float* __restrict__ du) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float R[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) R[k] = __ldg(Rcw + k);
+  const float3 t = make_float3(__ldg(tcw), __ldg(tcw + 1), __ldg(tcw + 2));
+  const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
+  const Projected p = project_point(pw, R, t, fx, fy, cx, cy);
+  if (!p.valid) {
+    depths[i] = kBadDepth;
+    us[2 * i] = us[2 * i + 1] = 0.f;
+    pcs[3 * i] = pcs[3 * i + 1] = pcs[3 * i + 2] = 0.f;
+    if (du)
+#pragma unroll
+      for (int k = 0; k < 6; ++k) du[6 * i + k] = 0.f;
+    return;
+  }
+  us[2 * i] = p.ux;
+  us[2 * i + 1] = p.uy;
+  pcs[3 * i] = p.x;
+  pcs[3 * i + 1] = p.y;
+  pcs[3 * i + 2] = p.z;
+  depths[i] = p.z;
+  if (du) {
+    const float z_inv = 1.f / p.z;
+    const float z2_inv = z_inv * z_inv;
+    du[6 * i + 0] = fx * z_inv;
+    du[6 * i + 1] = 0.f;
+    du[6 * i + 2] = -(p.x * fx) * z2_inv;
+    du[6 * i + 3] = 0.f;
+    du[6 * i + 4] = fy * z_inv;
+    du[6 * i + 5] = -(p.y * fy) * z2_inv;
+  }
+}
+
+// d Sigma_(rc) / d q_j and / d s_j for Sigma = M M^T, M = R(q) diag(s).
+__device__ __forceinline__ void cov3d_jacobians(float4 q, float3 s, const float* M,
+                                                const float* R, float* dq /*6x4*/,
+                                                float* ds /*6x3*/) {
+  const float w = q.x, x = q.y, y = q.z, z = q.w;
+  // dR_ab / dq_j (rows a*3+b)
+  const float dR[9][4] = {{0.f, 0.f, -4.f * y, -4.f * z},
+                          {-2.f * z, 2.f * y, 2.f * x, -2.f * w},
+                          {2.f * y, 2.f * z, 2.f * w, 2.f * x},
+                          {2.f * z, 2.f * y, 2.f * x, 2.f * w},
+                          {0.f, -4.f * x, 0.f, -4.f * z},
+                          {-2.f * x, -2.f * w, 2.f * z, 2.f * y},
+                          {-2.f * y, 2.f * z, -2.f * w, 2.f * x},
+                          {2.f * x, 2.f * w, 2.f * z, 2.f * y},
+                          {0.f, -4.f * x, -4.f * y, 0.f}};
+  const float sv[3] = {s.x, s.y, s.z};
+  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+  for (int u = 0; u < 6; ++u) {
+    const int r = sym[u][0], c = sym[u][1];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float acc = 0.f;
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        acc += (M[3 * c + b] * dR[3 * r + b][j] + M[3 * r + b] * dR[3 * c + b][j]) * sv[b];
+      dq[4 * u + j] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) ds[3 * u + j] = M[3 * c + j] * R[3 * r + j] + M[3 * r + j] * R[3 * c + j];
+  }
+}
+
+// computeCov3D -- gsplatcu/kernel.cu:422-501.
+__global__ void __launch_bounds__(kThreads)
+    k_cov3d(int64_t n, const float4* __restrict__ rots, const float* __restrict__ scales,
+            const float* __restrict__ depths, float* __restrict__ cov3ds,
+            float* __restrict__ dq, float* __restrict__ ds) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (depths[i] < kMinDepth) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cov3ds[6 * i + k] = 0.f;
+    if (dq) {
+      for (int k = 0; k < 24; ++k) dq[24 * i + k] = 0.f;
+      for (int k = 0; k < 18; ++k) ds[18 * i + k] = 0.f;
+    }
+    return;
+  }
+  const float4 q = rots[i];
+  const float3 s = make_float3(scales[3 * i], scales[3 * i + 1], scales[3 * i + 2]);
+  float cov[6], M[9], R[9];
+  covariance_3d(q, s, cov, M, R);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) cov3ds[6 * i + k] = cov[k];
+  if (dq) {
+    float jq[24], js[18];
+    cov3d_jacobians(q, s, M, R, jq, js);
+#pragma unroll
+    for (int k = 0; k < 24; ++k) dq[24 * i + k] = jq[k];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) ds[18 * i + k] = js[k];
+  }
+}
+
+// Jacobians of cov2d = (Sigma'_00 + .3, Sigma'_01, Sigma'_11 + .3) w.r.t. the 6
+// unique entries of Sigma and the camera-space centre (clamp not
+// differentiated, as in the reference).  M = J Rcw.
+__device__ __forceinline__ void cov2d_jacobians(const float* cov3, const float* M, const float* Rcw,
+                                                float x, float y, float z, float fx, float fy,
+                                                float* d3 /*3x6*/, float* dp /*3x3*/) {
+  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  const int out[3][2] = {{0, 0}, {0, 1}, {1, 1}};
+#pragma unroll
+  for (int o = 0; o < 3; ++o)
+#pragma unroll
+    for (int u = 0; u < 6; ++u) {
+      const int a = out[o][0], b = out[o][1], k = sym[u][0], l = sym[u][1];
+      float v = M[3 * a + k] * M[3 * b + l];
+      if (k != l) v += M[3 * a + l] * M[3 * b + k];
+      d3[6 * o + u] = v;
+    }
+  const float S[9] = {cov3[0], cov3[1], cov3[2], cov3[1], cov3[3], cov3[4], cov3[2], cov3[4], cov3[5]};
+  float dm[3][6];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float sm0 = S[3 * c] * M[0] + S[3 * c + 1] * M[1] + S[3 * c + 2] * M[2];
+    const float sm1 = S[3 * c] * M[3] + S[3 * c + 1] * M[4] + S[3 * c + 2] * M[5];
+    dm[0][c] = 2.f * sm0;
+    dm[0][3 + c] = 0.f;
+    dm[1][c] = sm1;
+    dm[1][3 + c] = sm0;
+    dm[2][c] = 0.f;
+    dm[2][3 + c] = 2.f * sm1;
+  }
+  const float zi2 = 1.f / (z * z), zi3 = zi2 / z;
+  float dmp[6][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    dmp[c][0] = -fx * Rcw[6 + c] * zi2;
+    dmp[c][1] = 0.f;
+    dmp[c][2] = -fx * Rcw[c] * zi2 + 2.f * fx * Rcw[6 + c] * x * zi3;
+    dmp[3 + c][0] = 0.f;
+    dmp[3 + c][1] = -fy * Rcw[6 + c] * zi2;
+    dmp[3 + c][2] = -fy * Rcw[3 + c] * zi2 + 2.f * fy * Rcw[6 + c] * y * zi3;
+  }
+#pragma unroll
+  for (int o = 0; o < 3; ++o)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float acc = 0.f;
+#pragma unroll
+      for (int m = 0; m < 6; ++m) acc += dm[o][m] * dmp[m][j];
+      dp[3 * o + j] = acc;
+    }
+}
+
+// computeCov2D -- gsplatcu/kernel.cu:508-611.
+__global__ void __launch_bounds__(kThreads)
+    k_cov2d(int64_t n, const float* __restrict__ cov3ds, const float* __restrict__ pcs,
+            const float* __restrict__ Rcw, const float* __restrict__ depths, float fx, float fy,
+            float tanx, float tany, float* __restrict__ cov2ds, float* __restrict__ d3,
+            float* __restrict__ dp) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (depths[i] < kMinDepth) {
+    cov2ds[3 * i] = cov2ds[3 * i + 1] = cov2ds[3 * i + 2] = 0.f;
+    if (d3) {
+      for (int k = 0; k < 18; ++k) d3[18 * i + k] = 0.f;
+      for (int k = 0; k < 9; ++k) dp[9 * i + k] = 0.f;
+    }
+    return;
+  }
+  float R[9], c3[6], c2[3], M[6], xy[2];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) R[k] = __ldg(Rcw + k);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) c3[k] = cov3ds[6 * i + k];
+  const float z = pcs[3 * i + 2];
+  covariance_2d(c3, pcs[3 * i], pcs[3 * i + 1], z, R, fx, fy, tanx, tany, c2, M, xy);
+  cov2ds[3 * i] = c2[0];
+  cov2ds[3 * i + 1] = c2[1];
+  cov2ds[3 * i + 2] = c2[2];
+  if (d3) {
+    float j3[18], jp[9];
+    cov2d_jacobians(c3, M, R, xy[0], xy[1], z, fx, fy, j3, jp);
+#pragma unroll
+    for (int k = 0; k < 18; ++k) d3[18 * i + k] = j3[k];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dp[9 * i + k] = jp[k];
+  }
+}
+
+// inverseCov2D -- gsplatcu/kernel.cu:379-415.  Updates depths in place.
+__global__ void __launch_bounds__(kThreads)
+    k_inverse_cov2d(int64_t n, const float* __restrict__ cov2ds, float* __restrict__ depths,
+                    float* __restrict__ cinv, int* __restrict__ areas, float* __restrict__ dcinv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float conic[3] = {0.f, 0.f, 0.f};
+  int ext[2] = {0, 0};
+  float det_inv = 0.f;
+  bool ok = false;
+  const float a = cov2ds[3 * i], b = cov2ds[3 * i + 1], c = cov2ds[3 * i + 2];
+  if (!(depths[i] < kMinDepth)) {
+    ok = conic_and_extent(a, b, c, conic, ext, &det_inv);
+    if (!ok) depths[i] = kBadDepth;
+  }
+  cinv[3 * i] = conic[0];
+  cinv[3 * i + 1] = conic[1];
+  cinv[3 * i + 2] = conic[2];
+  areas[2 * i] = ext[0];
+  areas[2 * i + 1] = ext[1];
+  if (dcinv) {
+    float J[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (ok) {
+      const float d2 = det_inv * det_inv;
+      J[0] = -c * c * d2;
+      J[1] = 2 * b * c * d2;
+      J[2] = -a * c * d2 + det_inv;
+      J[3] = b * c * d2;
+      J[4] = -2 * b * b * d2 - det_inv;
+      J[5] = a * b * d2;
+      J[6] = -a * c * d2 + det_inv;
+      J[7] = 2 * a * b * d2;
+      J[8] = -a * a * d2;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dcinv[9 * i + k] = J[k];
+  }
+}
+
+// sh2Weight / sh2Color -- gsplatcu/kernel.cu:670-870, 1040-1169.  Both are the
+// same map feat_k = sum_l Y_l(dir) c[l*K + k] (band-major); colours are K = 3.
+// All Gaussians are evaluated (no depth test), as in the reference.
+template <int K, typename T>
+__global__ void __launch_bounds__(kThreads)
+    k_sh2feat(int64_t n, const T* __restrict__ shs, int nb, const float* __restrict__ pws,
+              const float* __restrict__ twc, float* __restrict__ feat, float* __restrict__ dshs,
+              float* __restrict__ dpws) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T* c = shs + i * (int64_t)nb * K;
+  float dir[3] = {0.f, 0.f, 0.f}, nd[3] = {0.f, 0.f, 0.f}, ninv = 0.f;
+  float Y[16];
+  if (nb > 1) {
+    const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
+    const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
+    view_direction(pw, cam, dir, nd, &ninv);
+  }
+  sh_basis(dir, nb, Y);
+  float acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = Y[0] * ld(c, k);
+  // band-by-band accumulation, as the reference groups its sums
+  if (nb > 1) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      acc[k] += Y[1] * ld(c, K + k) + Y[2] * ld(c, 2 * K + k) + Y[3] * ld(c, 3 * K + k);
+    if (nb > 4) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        acc[k] += Y[4] * ld(c, 4 * K + k) + Y[5] * ld(c, 5 * K + k) + Y[6] * ld(c, 6 * K + k) +
+                  Y[7] * ld(c, 7 * K + k) + Y[8] * ld(c, 8 * K + k);
+      if (nb > 9) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          acc[k] += Y[9] * ld(c, 9 * K + k) + Y[10] * ld(c, 10 * K + k) +
+                    Y[11] * ld(c, 11 * K + k) + Y[12] * ld(c, 12 * K + k) +
+                    Y[13] * ld(c, 13 * K + k) + Y[14] * ld(c, 14 * K + k) +
+                    Y[15] * ld(c, 15 * K + k);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) feat[i * K + k] = acc[k];
+  if (dshs) {
+    for (int l = 0; l < nb; ++l) dshs[i * nb + l] = Y[l];
+    float G[48], J[9];
+    sh_basis_grad(dir, nb, /*ref_quirk=*/true, G);
+    if (nb > 1) dir_jacobian(nd, ninv, J);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float dd[3] = {0.f, 0.f, 0.f};
+      for (int l = 1; l < nb; ++l) {
+        const float cv = ld(c, l * K + k);
+        dd[0] += G[3 * l] * cv;
+        dd[1] += G[3 * l + 1] * cv;
+        dd[2] += G[3 * l + 2] * cv;
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        dpws[(i * K + k) * 3 + j] =
+            nb > 1 ? dd[0] * J[j] + dd[1] * J[3 + j] + dd[2] * J[6 + j] : 0.f;
+    }
+  }
+}
+
+// sh2Weight_fast -- gsplatcu/kernel.cu:884-987, generalised to rank r:
+// coefficient (l, k) of the L*K block (g = l*K + k) is C[g / Q][g % Q] with
+// C = A B, A [P,r], B [r,Q].
+template <int K, typename T>
+__global__ void __launch_bounds__(kThreads)
+    k_sh2weight_lowrank(int64_t n, const T* __restrict__ dc, const T* __restrict__ A,
+                        const T* __restrict__ B, int P, int Q, int rank, int L,
+                        const float* __restrict__ pws, const float* __restrict__ twc,
+                        float* __restrict__ w, float* __restrict__ ddc, float* __restrict__ ylm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float wk[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    wk[k] = SH_C0 * ld(dc, i * K + k);
+    if (ddc) ddc[i * K + k] = SH_C0;
+  }
+  if (L > 0) {
+    float dir[3], Y[16];
+    const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
+    const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
+    view_direction(pw, cam, dir, nullptr, nullptr);
+    sh_basis(dir, L + 1, Y);
+    if (ylm)
+      for (int l = 0; l < L; ++l) ylm[i * L + l] = Y[l + 1];
+    const T* a = A + i * (int64_t)P * rank;
+    const T* b = B + i * (int64_t)rank * Q;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float acc = 0.f;
+      for (int l = 0; l < L; ++l) {
+        const int g = l * K + k, row = g / Q, col = g % Q;
+        float coef = ld(a, row * rank) * ld(b, col);
+        for (int r = 1; r < rank; ++r) coef += ld(a, row * rank + r) * ld(b, r * Q + col);
+        acc += coef * Y[l + 1];
+      }
+      wk[k] += acc;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) w[i * K + k] = wk[k];
+}
+
+// sh2Weight_fast_B -- gsplatcu/kernel.cu:994-1032, rank r.  One thread owns
+// one Gaussian's rows of dA / dB, so the sums are accumulated sequentially in
+// the reference's (k, l) order without atomics.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    k_sh2weight_lowrank_b(int64_t n, const T* __restrict__ A, const T* __restrict__ B,
+                          const float* __restrict__ ylm, const float* __restrict__ dw, int K,
+                          int P, int Q, int rank, int L, float* __restrict__ dA,
+                          float* __restrict__ dB) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T* a = A + i * (int64_t)P * rank;
+  const T* b = B + i * (int64_t)rank * Q;
+  float* da = dA + i * (int64_t)P * rank;
+  float* db = dB + i * (int64_t)rank * Q;
+  for (int k = 0; k < P * rank; ++k) da[k] = 0.f;
+  for (int k = 0; k < rank * Q; ++k) db[k] = 0.f;
+  for (int k = 0; k < K; ++k) {
+    const float g0 = dw[i * K + k];
+    for (int l = 0; l < L; ++l) {
+      const int g = l * K + k, row = g / Q, col = g % Q;
+      const float y = ylm[i * L + l];
+      for (int r = 0; r < rank; ++r) {
+        da[row * rank + r] = __fadd_rn(da[row * rank + r], g0 * ld(b, r * Q + col) * y);
+        db[r * Q + col] = __fadd_rn(db[r * Q + col], g0 * ld(a, row * rank + r) * y);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ launchers
+static int grid_for(int64_t n) { return div_up(n > 0 ? n : 1, kThreads); }
+
+int launch_project(int64_t n, const float* pws, const float* Rcw, const float* tcw, float fx,
+                   float fy, float cx, float cy, float* us, float* pcs, float* depths, float* du,
+                   cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  k_project<<<grid_for(n), kThreads, 0, st>>>(n, pws, Rcw, tcw, fx, fy, cx, cy, us, pcs, depths, du);
+  return check_launch("project");
+}
+
+int launch_cov3d(int64_t n, const float* rots, const float* scales, const float* depths,
+                 float* cov3ds, float* dq, float* ds, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  k_cov3d<<<grid_for(n), kThreads, 0, st>>>(n, (const float4*)rots, scales, depths, cov3ds, dq, ds);
+  return check_launch("computeCov3D");
+}
+
+int launch_cov2d(int64_t n, const float* cov3ds, const float* pcs, const float* Rcw,
+                 const float* depths, float fx, float fy, float tanx, float tany, float* cov2ds,
+                 float* d3, float* dp, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  k_cov2d<<<grid_for(n), kThreads, 0, st>>>(n, cov3ds, pcs, Rcw, depths, fx, fy, tanx, tany, cov2ds, d3, dp);
+  return check_launch("computeCov2D");
+}
+
+int launch_inverse_cov2d(int64_t n, const float* cov2ds, float* depths, float* cinv, int* areas,
+                         float* dcinv, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  k_inverse_cov2d<<<grid_for(n), kThreads, 0, st>>>(n, cov2ds, depths, cinv, areas, dcinv);
+  return check_launch("inverseCov2D");
+}
+
+template <typename T>
+static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws, const float* twc,
+                     float* feat, float* dshs, float* dpws, cudaStream_t st) {
+  const T* s = (const T*)shs;
+  const int g = grid_for(n);
+  switch (K) {
+#define GSB_K(KK) \
+  case KK: k_sh2feat<KK, T><<<g, kThreads, 0, st>>>(n, s, nb, pws, twc, feat, dshs, dpws); break;
+    GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
+#undef GSB_K
+    default: return GSB_ERR_INVALID_ARGUMENT;
+  }
+  return check_launch("sh2Weight");
+}
+
+int launch_sh2feat(int64_t n, const void* shs, int dtype, int nb, int K, const float* pws,
+                   const float* twc, float* feat, float* dshs, float* dpws, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  return dtype == GSB_DTYPE_BF16
+             ? sh2feat_t<__nv_bfloat16>(n, shs, nb, K, pws, twc, feat, dshs, dpws, st)
+             : sh2feat_t<float>(n, shs, nb, K, pws, twc, feat, dshs, dpws, st);
+}
+
+template <typename T>
+static int lowrank_t(int64_t n, const void* dc, const void* A, const void* B, int K, int P, int Q,
+                     int rank, int L, const float* pws, const float* twc, float* w, float* ddc,
+                     float* ylm, cudaStream_t st) {
+  const int g = grid_for(n);
+  const T *d = (const T*)dc, *a = (const T*)A, *b = (const T*)B;
+  switch (K) {
+#define GSB_K(KK)                                                                             \
+  case KK:                                                                                    \
+    k_sh2weight_lowrank<KK, T><<<g, kThreads, 0, st>>>(n, d, a, b, P, Q, rank, L, pws, twc, w, \
+                                                       ddc, ylm);                             \
+    break;
+    GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
+#undef GSB_K
+    default: return GSB_ERR_INVALID_ARGUMENT;
+  }
+  return check_launch("sh2Weight_fast");
+}
+
+int launch_sh2weight_lowrank(int64_t n, const void* dc, const void* A, const void* B, int dtype,
+                             int K, int P, int Q, int rank, int L, const float* pws,
+                             const float* twc, float* w, float* ddc, float* ylm, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  return dtype == GSB_DTYPE_BF16
+             ? lowrank_t<__nv_bfloat16>(n, dc, A, B, K, P, Q, rank, L, pws, twc, w, ddc, ylm, st)
+             : lowrank_t<float>(n, dc, A, B, K, P, Q, rank, L, pws, twc, w, ddc, ylm, st);
+}
+
+int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtype,
+                               const float* ylm, const float* dw, int K, int P, int Q, int rank,
+                               int L, float* dA, float* dB, cudaStream_t st) {
+  if (n == 0) return GSB_OK;
+  const int g = grid_for(n);
+  if (dtype == GSB_DTYPE_BF16)
+    k_sh2weight_lowrank_b<__nv_bfloat16><<<g, kThreads, 0, st>>>(
+        n, (const __nv_bfloat16*)A, (const __nv_bfloat16*)B, ylm, dw, K, P, Q, rank, L, dA, dB);
+  else
+    k_sh2weight_lowrank_b<float><<<g, kThreads, 0, st>>>(n, (const float*)A, (const float*)B, ylm,
+                                                         dw, K, P, Q, rank, L, dA, dB);
+  return check_launch("sh2Weight_fast_B");
+}
+
+}  // namespace gsb

@@ -1,0 +1,339 @@
+// Tile compositing: forward (draw_weight / draw_color, gsplatcu/kernel.cu:
+// 194-372) and its reverse-order adjoint (draw_weight_B / draw_color_B,
+// gsplatcu/kernel.cu:1176-1379).
+//
+// One 256-thread CTA per 16x16 tile.  Each warp owns an 8x4 block of pixels.
+// The tile's Gaussian list is staged through shared memory in batches of 256
+// packed records; within a batch every warp first tests 32 records at a time
+// against its pixel block (one record per lane, ballot) using the record's
+// conservative support box, then walks only the overlapping records in list
+// order.  Per pixel, a record whose Mahalanobis distance exceeds its cut is
+// skipped without evaluating exp() -- the reference would skip it too
+// (alpha' < 0.002) -- and every other record is evaluated with the
+// reference's own FP32 expressions, so skip/stop decisions, contributor
+// indices and blended values agree with it.
+#include "gsb_geometry.cuh"
+#include "gsb_internal.h"
+
+namespace gsb {
+
+constexpr int kBatch = 256;
+constexpr int kDrawThreads = 256;
+
+__device__ __forceinline__ void pixel_of(int tile, int gx, int& wx, int& wy, int& px, int& py) {
+  const int tx = tile % gx, ty = tile / gx;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  wx = tx * kTile + (w & 1) * 8;
+  wy = ty * kTile + (w >> 1) * 4;
+  px = wx + (lane & 7);
+  py = wy + (lane >> 3);
+}
+
+// Stage records [first, first+cnt) of the tile list into shared memory,
+// vector-major (srec[v * kBatch + slot]) so that per-slot broadcasts and the
+// lane-per-slot box test are both conflict-free.
+template <int V>
+__device__ __forceinline__ void stage_batch(const int32_t* __restrict__ gsid, int first, int cnt,
+                                            const float4* __restrict__ records, float4* srec,
+                                            int32_t* sgid) {
+  if ((int)threadIdx.x < cnt) {
+    const int g = gsid[first + threadIdx.x];
+    const float4* src = records + (int64_t)g * V;
+#pragma unroll
+    for (int v = 0; v < V; ++v) srec[v * kBatch + threadIdx.x] = __ldg(src + v);
+    if (sgid) sgid[threadIdx.x] = g;
+  }
+}
+
+__device__ __forceinline__ bool box_overlaps(float4 box, int wx, int wy) {
+  return box.y >= (float)wx && box.x <= (float)(wx + 7) && box.w >= (float)wy &&
+         box.z <= (float)(wy + 3);
+}
+
+template <int K>
+__device__ __forceinline__ void load_feats(const float4* srec, int j, float v2w, float* f) {
+  f[0] = v2w;
+#pragma unroll
+  for (int k = 1; k < K; ++k) {
+    const int idx = 11 + k;  // float index inside the record
+    const float4 q = srec[(idx >> 2) * kBatch + j];
+    f[k] = (idx & 3) == 0 ? q.x : (idx & 3) == 1 ? q.y : (idx & 3) == 2 ? q.z : q.w;
+  }
+}
+
+// ------------------------------------------------------------- forward
+template <int K>
+__global__ void __launch_bounds__(kDrawThreads, 4)
+    k_draw(int H, int W, int gx, const int2* __restrict__ ranges, const int32_t* __restrict__ gsid,
+           const float4* __restrict__ records, float tau_init, float* __restrict__ out,
+           int32_t* __restrict__ contrib, float* __restrict__ final_tau) {
+  constexpr int V = RecordLayout<K>::kVec4;
+  __shared__ float4 srec[V * kBatch];
+  int wx, wy, px, py;
+  pixel_of(blockIdx.x, gx, wx, wy, px, py);
+  const bool inside = px < W && py < H;
+  const int2 rg = ranges[blockIdx.x];
+  const int n = rg.y - rg.x;
+  float acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.f;
+  float T = 1.f;
+  int cont = 0;
+  bool done = !inside;
+  for (int base = 0; base < n; base += kBatch) {
+    const int cnt = min(kBatch, n - base);
+    __syncthreads();
+    stage_batch<V>(gsid, rg.x + base, cnt, records, srec, nullptr);
+    __syncthreads();
+    if (!__all_sync(0xffffffffu, done)) {
+      for (int s = 0; s < cnt; s += 32) {
+        const int j = s + (threadIdx.x & 31);
+        const bool ov = j < cnt && box_overlaps(srec[j], wx, wy);
+        unsigned mask = __ballot_sync(0xffffffffu, ov);
+        while (mask) {
+          const int jj = s + __ffs(mask) - 1;
+          mask &= mask - 1;
+          if (done) continue;
+          const float4 v1 = srec[kBatch + jj];      // ux uy qa qb
+          const float4 v2 = srec[2 * kBatch + jj];  // qc cut alpha f0
+          const float dx = v1.x - (float)px, dy = v1.y - (float)py;
+          const float maha = fmaxf(0.0f, maha_sq(v1.z, v1.w, v2.x, dx, dy));
+          if (maha > v2.y) continue;
+          const float ap = fminf(kAlphaMax, v2.z * expf(-0.5f * maha));
+          if (ap < kAlphaMin) continue;
+          float f[K];
+          load_feats<K>(srec, jj, v2.w, f);
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] += T * ap * f[k];
+          cont = base + jj + 1;
+          T *= (1.f - ap);
+          if (T < kTransMin) done = true;
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+      }
+    }
+    if (!__syncthreads_or(!done)) break;
+  }
+  if (inside) {
+    const int64_t pix = (int64_t)py * W + px, hw = (int64_t)H * W;
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k * hw + pix] = acc[k];
+    contrib[pix] = cont;
+    final_tau[pix] = n > 0 ? T : tau_init;
+  }
+}
+
+// ------------------------------------------------------------- adjoint
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Walks each pixel's contributors back to front from its `contrib` index,
+// recovering T by division by (1 - alpha') from the saved final T.  Per
+// Gaussian the warp's contributions are summed with shuffles and added once.
+// GEOM adds the opacity / centre / conic adjoint (draw_color_B's terms, for
+// any channel count); DTAU adds dL/dT_final (vanilla_3dgs/gsplatcu/
+// kernel.cu:912-919).  As in the reference, the 0.99 clamp and max(0, .) are
+// not differentiated.
+template <int K, bool GEOM, bool DTAU>
+__global__ void __launch_bounds__(kDrawThreads, 3)
+    k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
+                    const int32_t* __restrict__ gsid, const float4* __restrict__ records,
+                    const int32_t* __restrict__ contrib, const float* __restrict__ final_tau,
+                    const float* __restrict__ dout, const float* __restrict__ dtau,
+                    float* __restrict__ dfeat, float* __restrict__ dalpha,
+                    float* __restrict__ du, float* __restrict__ dconic) {
+  constexpr int V = RecordLayout<K>::kVec4;
+  __shared__ float4 srec[V * kBatch];
+  __shared__ int32_t sgid[kBatch];
+  __shared__ unsigned s_maxc;
+  int wx, wy, px, py;
+  pixel_of(blockIdx.x, gx, wx, wy, px, py);
+  const int lane = threadIdx.x & 31;
+  const bool inside = px < W && py < H;
+  const int2 rg = ranges[blockIdx.x];
+  if (rg.y - rg.x == 0) return;  // uniform per block
+  const int64_t pix = (int64_t)py * W + px, hw = (int64_t)H * W;
+  float dl[K], G[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    dl[k] = inside ? dout[k * hw + pix] : 0.f;
+    G[k] = 0.f;
+  }
+  const float Tf = inside ? final_tau[pix] : 0.f;
+  const float dTf = (DTAU && inside) ? dtau[pix] : 0.f;
+  const int cont = inside ? contrib[pix] : 0;
+  float T = Tf;
+  const int wmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)cont);
+  if (threadIdx.x == 0) s_maxc = 0u;
+  __syncthreads();
+  if (lane == 0) atomicMax(&s_maxc, (unsigned)wmax);
+  __syncthreads();
+  // contributor indices never exceed the tile's list (clamped for safety
+  // against mismatched inputs)
+  const int maxc = min((int)s_maxc, rg.y - rg.x);
+  for (int top = maxc; top > 0; top -= kBatch) {
+    const int base = max(0, top - kBatch);
+    const int cnt = top - base;
+    __syncthreads();
+    stage_batch<V>(gsid, rg.x + base, cnt, records, srec, sgid);
+    __syncthreads();
+    const int hi = min(cnt, wmax - base);
+    for (int s_hi = hi; s_hi > 0; s_hi -= 32) {
+      const int s_lo = max(0, s_hi - 32);
+      const int j = s_lo + lane;
+      const bool ov = j < s_hi && box_overlaps(srec[j], wx, wy);
+      unsigned mask = __ballot_sync(0xffffffffu, ov);
+      while (mask) {
+        const int msb = 31 - __clz(mask);
+        mask &= ~(1u << msb);
+        const int jj = s_lo + msb;
+        const int p = base + jj;
+        bool hit = false;
+        float gk[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) gk[k] = 0.f;
+        float ga = 0.f, gux = 0.f, guy = 0.f, gqa = 0.f, gqb = 0.f, gqc = 0.f;
+        if (p < cont) {
+          const float4 v1 = srec[kBatch + jj];
+          const float4 v2 = srec[2 * kBatch + jj];
+          const float dx = v1.x - (float)px, dy = v1.y - (float)py;
+          const float maha = fmaxf(0.f, maha_sq(v1.z, v1.w, v2.x, dx, dy));
+          if (!(maha > v2.y)) {
+            const float g = expf(-0.5f * maha);
+            const float ap = fminf(kAlphaMax, v2.z * g);
+            if (!(ap < kAlphaMin)) {
+              hit = true;
+              T /= (1.f - ap);
+              const float wgt = ap * T;
+#pragma unroll
+              for (int k = 0; k < K; ++k) gk[k] = dl[k] * wgt;
+              if (GEOM) {
+                float f[K];
+                load_feats<K>(srec, jj, v2.w, f);
+                float dap = 0.f;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                  dap += dl[k] * (T * (f[k] - G[k]));
+                  G[k] = ap * f[k] + (1.f - ap) * G[k];
+                }
+                if (DTAU) dap += dTf * (-Tf / (1.f - ap));
+                ga = dap * g;
+                gux = dap * ((-v1.z * dx - v1.w * dy) * ap);
+                guy = dap * ((-v1.w * dx - v2.x * dy) * ap);
+                gqa = dap * (-0.5f * ap * (dx * dx));
+                gqb = dap * (-1.0f * ap * (dx * dy));
+                gqc = dap * (-0.5f * ap * (dy * dy));
+              }
+            }
+          }
+        }
+        const unsigned cm = __ballot_sync(0xffffffffu, hit);
+        if (!cm) continue;
+        const int g = sgid[jj];
+        if (__popc(cm) == 1) {
+          if (hit) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) atomicAdd(dfeat + (int64_t)g * K + k, gk[k]);
+            if (GEOM) {
+              atomicAdd(dalpha + g, ga);
+              atomicAdd(du + 2 * (int64_t)g, gux);
+              atomicAdd(du + 2 * (int64_t)g + 1, guy);
+              atomicAdd(dconic + 3 * (int64_t)g, gqa);
+              atomicAdd(dconic + 3 * (int64_t)g + 1, gqb);
+              atomicAdd(dconic + 3 * (int64_t)g + 2, gqc);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < K; ++k) gk[k] = warp_sum(gk[k]);
+          if (GEOM) {
+            ga = warp_sum(ga);
+            gux = warp_sum(gux);
+            guy = warp_sum(guy);
+            gqa = warp_sum(gqa);
+            gqb = warp_sum(gqb);
+            gqc = warp_sum(gqc);
+          }
+          if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) atomicAdd(dfeat + (int64_t)g * K + k, gk[k]);
+            if (GEOM) {
+              atomicAdd(dalpha + g, ga);
+              atomicAdd(du + 2 * (int64_t)g, gux);
+              atomicAdd(du + 2 * (int64_t)g + 1, guy);
+              atomicAdd(dconic + 3 * (int64_t)g, gqa);
+              atomicAdd(dconic + 3 * (int64_t)g + 1, gqb);
+              atomicAdd(dconic + 3 * (int64_t)g + 2, gqc);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ launchers
+int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, const int32_t* gsid,
+                const SplatState& s, float tau_init, float* out, int32_t* contrib,
+                float* final_tau, cudaStream_t st) {
+  (void)n;
+  const int gx = div_up(W, kTile), gy = div_up(H, kTile);
+  const int tiles = gx * gy;
+  if (tiles == 0) return GSB_OK;
+  const int2* rg = (const int2*)ranges;
+  switch (channels) {
+#define GSB_K(KK)                                                                           \
+  case KK:                                                                                  \
+    k_draw<KK><<<tiles, kDrawThreads, 0, st>>>(H, W, gx, rg, gsid, s.records, tau_init, out, \
+                                               contrib, final_tau);                         \
+    break;
+    GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
+#undef GSB_K
+    default: return GSB_ERR_INVALID_ARGUMENT;
+  }
+  return check_launch("splat_draw");
+}
+
+template <int K>
+static void draw_bwd_k(int tiles, int H, int W, int gx, const int2* rg, const int32_t* gsid,
+                       const float4* rec, const int32_t* contrib, const float* ft, const float* dout,
+                       const float* dtau, float* dfeat, float* dalpha, float* du, float* dq,
+                       cudaStream_t st) {
+  const bool geom = dalpha != nullptr;
+  if (geom && dtau)
+    k_draw_backward<K, true, true><<<tiles, kDrawThreads, 0, st>>>(
+        H, W, gx, rg, gsid, rec, contrib, ft, dout, dtau, dfeat, dalpha, du, dq);
+  else if (geom)
+    k_draw_backward<K, true, false><<<tiles, kDrawThreads, 0, st>>>(
+        H, W, gx, rg, gsid, rec, contrib, ft, dout, dtau, dfeat, dalpha, du, dq);
+  else
+    k_draw_backward<K, false, false><<<tiles, kDrawThreads, 0, st>>>(
+        H, W, gx, rg, gsid, rec, contrib, ft, dout, dtau, dfeat, dalpha, du, dq);
+}
+
+int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* ranges,
+                         const int32_t* gsid, const SplatState& s, const int32_t* contrib,
+                         const float* final_tau, const float* dout, const float* dtau,
+                         float* dfeat, float* dalpha, float* du, float* dconic, cudaStream_t st) {
+  (void)n;
+  const int gx = div_up(W, kTile), gy = div_up(H, kTile);
+  const int tiles = gx * gy;
+  if (tiles == 0) return GSB_OK;
+  const int2* rg = (const int2*)ranges;
+  switch (channels) {
+#define GSB_K(KK)                                                                              \
+  case KK:                                                                                     \
+    draw_bwd_k<KK>(tiles, H, W, gx, rg, gsid, s.records, contrib, final_tau, dout, dtau, dfeat, \
+                   dalpha, du, dconic, st);                                                    \
+    break;
+    GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
+#undef GSB_K
+    default: return GSB_ERR_INVALID_ARGUMENT;
+  }
+  return check_launch("splat_backward");
+}
+
+}  // namespace gsb
