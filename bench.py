@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Benchmark of the palette-weight rasterizer on B200.
+
+Workload (one step): a finetune step of ReparamGS-Palette's low-rank fused
+path (WeightGSFunctionFast, gsplat/gsmodel.py:151-200) over 1,000,000
+synthetic Gaussians at 1920x1080 with rank-3 factors A [N,5,3], B [N,3,15]
+(P=5, Q=15, K=5, SH order 3, FP32 storage): forward through the gsplatcu
+operators (project, computeCov3D, computeCov2D, sh2Weight_fast, inverseCov2D,
+splat_weight), colour image = palette^T . layer and its L1 loss against a seeded random
+target (one fused kernel, palette_b200.loss), backward (splat_weight_B, sh2Weight_fast_B, dc and palette
+gradients).  `value` is whole-job fwd+bwd iterations per second with the
+scene resident in HBM; `frames_per_s` is the forward alone.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (under torchrun): independent replicas, one per GPU (the path has no
+exchange step); rank 0 prints the line with the max-over-ranks time.
+--impl reference times the reference algorithm's CPU implementation (the
+CPU oracle port) on this host's cores on a bounded sample of the same step.
+"""
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "reparamgs-palette_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "1080p frames/s & fwd+bwd iters/s at 1M Gaussians; p50/p99 palette-edit latency"
+SAMPLE_TILE_STRIDE = 8  # CPU baseline composites every 8th tile and scales
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--gaussians", type=int, default=1_000_000)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--rank", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- workload
+def make_workload(a, device):
+    from palette_b200.scene import look_at, synthetic_scene
+    sc = synthetic_scene(a.gaussians, seed=a.seed, mode="lowrank", rank=a.rank)
+    cam = look_at((0.0, -8.0, 0.0), width=a.width, height=a.height, device=device)
+    t = lambda x: torch.from_numpy(x).to(device).contiguous()
+    wl = dict(sc=sc, cam=cam, K=5, Q=15, pws=t(sc["pws"]), rots=t(sc["rots"]),
+              scales=t(sc["scales"]), alphas=t(sc["alphas"]),
+              dc=t(sc["dc"]).requires_grad_(), A=t(sc["A"]).requires_grad_(),
+              B=t(sc["B"]).requires_grad_(), palette=t(sc["palette"]).requires_grad_())
+    g = torch.Generator(device="cpu").manual_seed(a.seed)
+    target = torch.rand((3, a.height, a.width), generator=g)
+    wl["target_host"] = target.pin_memory() if device.type == "cuda" else target
+    wl["target"] = target.to(device)
+    wl["param_bytes"] = sum(int(x.numel()) * 4 for x in (wl["pws"], wl["rots"], wl["scales"],
+                                                         wl["alphas"], wl["dc"], wl["A"], wl["B"]))
+    return wl
+
+
+def step(wl, cam=None, target=None, backward=True):
+    from palette_b200.autograd import WeightGSFunctionFast
+    from palette_b200.loss import palette_l1_loss
+    cam = cam or wl["cam"]
+    target = wl["target"] if target is None else target
+    for p in (wl["dc"], wl["A"], wl["B"], wl["palette"]):
+        p.grad = None
+    layer, _ = WeightGSFunctionFast.apply(wl["pws"], wl["dc"], wl["A"], wl["B"], wl["alphas"],
+                                          wl["scales"], wl["rots"], cam, wl["K"], wl["Q"])
+    loss = palette_l1_loss(layer, wl["palette"], target)
+    if backward:
+        loss.backward()
+    return loss
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.path = index, None, None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def dist_setup(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(v, world, device):
+    if world == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel_tag):
+    """Per-launch DRAM traffic of a kernel from a committed ncu summary
+    (profiles/<kernel_tag>.md, line 'traffic_bytes_per_launch: N')."""
+    p = os.path.join(ROOT, "profiles", kernel_tag + ".md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def timed(fn, reps, stream):
+    """Device time (ms) of `reps` calls of fn on `stream`, CUDA events, synced both sides."""
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(reps):
+        fn()
+    e.record(stream)
+    torch.cuda.synchronize()
+    return s.elapsed_time(e)
+
+
+# ------------------------------------------------------------- stage timing
+def stage_breakdown(wl, reps=5):
+    """Per-stage device times (ms) of one step, each stage run alone through the
+    C ABI with CUDA events on the launching stream, plus the algorithmic bytes
+    of the compositing kernels."""
+    import gsplatcu as gsc
+    from gsplatcu import _lib
+    cam, K, Q = wl["cam"], wl["K"], wl["Q"]
+    H, W = cam.height, cam.width
+    st = torch.cuda.current_stream()
+    L = _lib.lib()
+    with torch.no_grad():
+        dc, A, B = wl["dc"].detach(), wl["A"].detach(), wl["B"].detach()
+        out = {}
+
+        def pre():
+            us, pcs, d = gsc.project(wl["pws"], cam.Rcw, cam.tcw, cam.fx, cam.fy, cam.cx, cam.cy, False)
+            c3, = gsc.computeCov3D(wl["rots"], wl["scales"], d, False)
+            c2, = gsc.computeCov2D(c3, pcs, cam.Rcw, d, cam.fx, cam.fy, W, H, False)
+            w, ddc, ylm = gsc.sh2Weight_fast(dc, A, B, wl["pws"], cam.twc, True, K, Q)
+            cinv, areas = gsc.inverseCov2D(c2, d, False)
+            return us, cinv, d, areas, w, ylm
+        out["preprocess"] = timed(pre, reps, st) / reps
+        us, cinv, d, areas, w, ylm = pre()
+        n = us.shape[0]
+        state = torch.empty(int(L.gsb_splat_state_bytes(n, K)), dtype=torch.uint8, device=us.device)
+        import ctypes as C
+        sp = _lib.stream_of(us)
+        d0, a0 = d.clone(), areas.clone()
+
+        def pack():
+            d.copy_(d0)
+            areas.copy_(a0)
+            _lib.call("bench", "gsb_splat_pack", n, H, W, K, _lib.ptr(us), _lib.ptr(cinv),
+                      _lib.ptr(wl["alphas"]), _lib.ptr(w), 0, _lib.ptr(d), _lib.ptr(areas),
+                      _lib.ptr(state), sp)
+        out["bin_pack_scan"] = timed(pack, reps, st) / reps
+        pack()
+        host = (C.c_uint32 * 2)()
+        _lib.call("bench", "gsb_splat_counts", n, _lib.ptr(state), host, sp)
+        M, maxdk = int(host[0]), int(host[1])
+        ws = torch.empty(int(L.gsb_splat_sort_bytes(n, H, W, M, maxdk)), dtype=torch.uint8,
+                         device=us.device)
+        gx, gy = (W + 15) // 16, (H + 15) // 16
+        gsid = torch.empty(M, dtype=torch.int32, device=us.device)
+        ranges = torch.empty((gx * gy, 2), dtype=torch.int32, device=us.device)
+        out["bin_sort"] = timed(lambda: _lib.call(
+            "bench", "gsb_splat_sort", n, H, W, M, maxdk, _lib.ptr(state), _lib.ptr(ws),
+            _lib.ptr(gsid), _lib.ptr(ranges), sp), reps, st) / reps
+        layer = torch.empty((K, H, W), device=us.device)
+        contrib = torch.empty((H, W), dtype=torch.int32, device=us.device)
+        ft = torch.empty((H, W), device=us.device)
+        out["draw"] = timed(lambda: _lib.call(
+            "bench", "gsb_splat_draw", n, H, W, K, _lib.ptr(ranges), _lib.ptr(gsid), _lib.ptr(state),
+            0.0, _lib.ptr(layer), _lib.ptr(contrib), _lib.ptr(ft), sp), reps, st) / reps
+        g = torch.rand((K, H, W), device=us.device)
+        dW = torch.zeros((n, 1, K), device=us.device)
+        out["draw_backward"] = timed(lambda: _lib.call(
+            "bench", "gsb_splat_backward_packed", n, H, W, K, _lib.ptr(ranges), _lib.ptr(gsid),
+            _lib.ptr(contrib), _lib.ptr(ft), _lib.ptr(g), None, _lib.ptr(state), _lib.ptr(dW), None,
+            None, None, sp), reps, st) / reps
+        out["lowrank_backward"] = timed(lambda: gsc.sh2Weight_fast_B(A, B, ylm, dW[:, 0], K, Q),
+                                        reps, st) / reps
+        visible = int((d > 0.2).sum())
+        pix = H * W
+        # algorithmic bytes: per patch 48 B record + 4 B id; per pixel K*4 + 8 B out;
+        # backward: per pixel K*4 + 8 B in, per patch 52 B, per visible Gaussian K*4 B out
+        bytes_draw = M * 52 + pix * (4 * K + 8)
+        bytes_bwd = pix * (4 * K + 8) + M * 52 + visible * 4 * K
+        return out, dict(M=M, visible=visible, bytes_draw=bytes_draw, bytes_bwd=bytes_bwd)
+
+
+# ----------------------------------------------------------- CPU baseline
+def cpu_step(wl, orc, stride):
+    """One bounded sample of the step on the host cores (CPU oracle, FP32):
+    full preprocess and binning of all Gaussians; forward and adjoint
+    compositing of every `stride`-th tile.  Returns extrapolated seconds for
+    one full step and the sample's own seconds."""
+    sc, cam, K, Q = wl["sc"], wl["cam"], wl["K"], wl["Q"]
+    H, W = cam.height, cam.width
+    t0 = time.perf_counter()
+    pre = orc.preprocess(sc["pws"], sc["rots"], sc["scales"], cam, np.float32)
+    w, _, ylm = orc.sh2weight_fast(sc["dc"], sc["A"], sc["B"], sc["pws"], pre["twc"], K, Q, True)
+    b = orc.bin_gaussians(pre["us"], pre["areas"], pre["depths"], H, W)
+    t1 = time.perf_counter()
+    ranges = b["ranges"].copy()
+    keep = np.zeros(len(ranges), bool)
+    keep[::stride] = True
+    ranges[~keep] = 0
+    out, contrib, ft = orc.draw(H, W, K, ranges, b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w, 0.0)
+    pal = sc["palette"]
+    img = np.einsum("kc,khw->chw", pal, out)
+    dimg = np.sign(img - wl["target_host"].numpy()) / img.size
+    dlayer = np.einsum("kc,chw->khw", pal, dimg).astype(np.float32)
+    g = orc.draw_backward(H, W, K, ranges, b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w, ft,
+                          contrib, dlayer)
+    t2 = time.perf_counter()
+    orc.sh2weight_fast_b(sc["A"], sc["B"], ylm, g["dfeat"], K, Q)
+    t3 = time.perf_counter()
+    frac = keep.sum() / len(keep)
+    full = (t1 - t0) + (t2 - t1) / frac + (t3 - t2)
+    return full, t3 - t0
+
+
+def cpu_baseline(wl, steps, warmup):
+    from oracle import oracle as orc
+    orc.set_threads(os.cpu_count() or 1)
+    for _ in range(max(0, warmup)):
+        cpu_step(wl, orc, SAMPLE_TILE_STRIDE)
+    fulls, samples = [], []
+    for _ in range(max(1, steps)):
+        f, s = cpu_step(wl, orc, SAMPLE_TILE_STRIDE)
+        fulls.append(f)
+        samples.append(s)
+    v = 1.0 / statistics.median(fulls)
+    return dict(value=v, unit="iters/s", cores=orc.get_threads(), kind="port",
+                sample=(f"CPU oracle (FP32, from-scratch restatement of gsplatcu's kernels) on "
+                        f"{orc.get_threads()} host threads: full preprocess + binning of all "
+                        f"{wl['sc']['pws'].shape[0]} Gaussians, forward+adjoint compositing of every "
+                        f"{SAMPLE_TILE_STRIDE}th tile scaled x{SAMPLE_TILE_STRIDE}; "
+                        f"{len(fulls)} timed samples, median; sample wall "
+                        f"{statistics.median(samples):.1f}s"),
+                ms_per_step=1000.0 / v)
+
+
+# ------------------------------------------------------------------- arms
+def run_reference(a):
+    world, rank, local = dist_setup(a)
+    if rank != 0:
+        return
+    wl = make_workload(a, torch.device("cpu"))
+    cb = cpu_baseline(wl, a.steps, a.warmup)
+    line = dict(metric=METRIC, value=cb["value"], unit="iters/s", n_gpus=a.gpus, steps=a.steps,
+                warmup=a.warmup, ms_per_step=cb["ms_per_step"], higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                config=config(a), impl="reference",
+                cpu_baseline={k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                e2e=dict(value=cb["value"], unit="iters/s", h2d_bytes_per_step=0,
+                         d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def config(a):
+    return dict(workload=(f"palette-weight finetune step, low-rank fused path: {a.gaussians} "
+                          f"Gaussians, {a.width}x{a.height}, rank-{a.rank} factors P=5 Q=15, K=5, "
+                          "SH order 3, FP32 storage, L1 loss on palette colour image"),
+                gaussians=a.gaussians, width=a.width, height=a.height, rank=a.rank,
+                parallelism="replicas" if a.gpus > 1 else "single-gpu",
+                l2="inputs larger than L2 (scene parameters ~%d MB > 126 MB L2)"
+                   % int(a.gaussians * 4 * (3 + 4 + 3 + 1 + 5 + 15 * a.rank + 5 * a.rank) / 1e6))
+
+
+def run_b200(a):
+    world, rank, local = dist_setup(a)
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: CUDA is required for --impl b200 (no CPU fallback)")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    from gsplatcu import _lib
+    L = _lib.lib()
+    wl = make_workload(a, device)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, a.warmup)):
+        step(wl)
+    torch.cuda.synchronize()
+
+    # timed region: K fwd+bwd steps
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = L.gsb_launch_count()
+    ms = timed(lambda: step(wl), a.steps, stream)
+    launches = int(L.gsb_launch_count() - l0)
+    clk = clocks.stop()
+    barrier(world)
+    ms = allreduce_max(ms, world, device)
+    ms_per_step = ms / a.steps
+    value = world * a.steps / (ms / 1000.0)
+
+    # forward only
+    with torch.no_grad():
+        fms = timed(lambda: step(wl, backward=False), a.steps, stream) / a.steps
+    fms = allreduce_max(fms, world, device)
+
+    # end to end: per step H2D of the camera and target from pinned host memory,
+    # D2H of the loss into pinned host memory
+    cam = wl["cam"]
+    R_h = cam.Rcw.cpu().pin_memory()
+    t_h = cam.tcw.cpu().pin_memory()
+    c_h = cam.twc.cpu().pin_memory()
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+    tgt_d = torch.empty_like(wl["target"])
+    from palette_b200.scene import Camera
+
+    def e2e_step():
+        Rd = R_h.to(device, non_blocking=True)
+        td = t_h.to(device, non_blocking=True)
+        cd = c_h.to(device, non_blocking=True)
+        tgt_d.copy_(wl["target_host"], non_blocking=True)
+        c = Camera(0, cam.width, cam.height, cam.fx, cam.fy, cam.cx, cam.cy, Rd, td, twc=cd)
+        loss = step(wl, cam=c, target=tgt_d)
+        loss_h.copy_(loss.detach(), non_blocking=True)
+    for _ in range(2):
+        e2e_step()
+    barrier(world)
+    ems = allreduce_max(timed(e2e_step, a.steps, stream), world, device)
+    h2d = int((R_h.numel() + t_h.numel() + c_h.numel() + wl["target_host"].numel()) * 4)
+
+    stages, alg = stage_breakdown(wl)
+    dom = max(("draw", "draw_backward"), key=lambda k: stages[k])
+    dom_bytes = alg["bytes_draw"] if dom == "draw" else alg["bytes_bwd"]
+    peak, peak_kind = measured_peaks()
+    achieved = dom_bytes / (stages[dom] / 1000.0) / 1e9
+    tag = {"draw": "k_draw_1M_1080p", "draw_backward": "k_draw_backward_1M_1080p"}[dom]
+    roof = dict(bound="hbm", kernel=f"k_{dom}", achieved=round(achieved, 1), peak=peak,
+                unit="GB/s", frac=round(achieved / peak, 4), traffic=profile_traffic(tag),
+                algorithmic_bytes=int(dom_bytes), launch_ms=round(stages[dom], 4),
+                peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s")
+
+    cb = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cb = cpu_baseline(wl, steps=2, warmup=0)
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        line = dict(metric=METRIC, value=round(value, 3), unit="iters/s", n_gpus=world,
+                    steps=a.steps, warmup=a.warmup, ms_per_step=round(ms_per_step, 4),
+                    higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                    data="synthetic (seeded; distributions of the benchmark configs)",
+                    config=config(a),
+                    frames_per_s=round(world * 1000.0 / fms, 2), forward_ms=round(fms, 4),
+                    e2e=dict(value=round(world * a.steps / (ems / 1000.0), 3), unit="iters/s",
+                             h2d_bytes_per_step=h2d, d2h_bytes_per_step=4),
+                    gpu_launches=launches, clocks=clk, roofline=roof, cpu_baseline=cb,
+                    stages_ms={k: round(v, 4) for k, v in stages.items()},
+                    patches=alg["M"])
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

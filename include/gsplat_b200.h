@@ -44,6 +44,10 @@ extern "C" {
 const char* gsb_last_error(void);
 /* Library ABI version, major * 100 + minor. */
 int gsb_version(void);
+/* Number of kernels this library has launched in the process so far
+ * (diagnostic; used to report how many of the library's kernels a timed
+ * region ran). */
+unsigned long long gsb_launch_count(void);
 
 /* ===================================================== reference operators */
 
@@ -168,6 +172,27 @@ int gsb_splat_backward(int64_t n, int height, int width, int channels, const flo
                        const int32_t* contrib, const float* final_tau, const float* dloss_dout,
                        const float* dloss_dtau, void* state, float* dfeats, float* dalphas,
                        float* dus, float* dcinv2ds, void* stream);
+
+/* The same adjoint on records already packed into `state` by gsb_splat_pack
+ * for these inputs (no re-pack).  Used when the forward's state is kept. */
+int gsb_splat_backward_packed(int64_t n, int height, int width, int channels,
+                              const int32_t* ranges, const int32_t* gsid, const int32_t* contrib,
+                              const float* final_tau, const float* dloss_dout,
+                              const float* dloss_dtau, const void* state, float* dfeats,
+                              float* dalphas, float* dus, float* dcinv2ds, void* stream);
+
+/* ------------------------------------------------------------- loss side
+ * Palette colour composite and L1 loss in one pass (no counterpart in the
+ * reference extension, whose callers compute the loss in torch,
+ * finetune.py:356-389):
+ *   image[c] = sum_k palette[k][c] layer[k]   (palette [K,3], layer [K,H,W]);
+ *   *loss = mean |image - target| over the 3*H*W values (target [3,H,W]);
+ *   dlayer[k] = sum_c palette[k][c] sign(image[c] - target[c]) / (3HW);
+ *   dpalette[k][c] = sum_pixels layer[k] sign(image[c] - target[c]) / (3HW).
+ * image, dlayer and dpalette may be NULL; loss and dpalette are overwritten. */
+int gsb_palette_l1(int K, int height, int width, const float* layer, const float* palette,
+                   const float* target, float* image, float* loss, float* dlayer,
+                   float* dpalette, void* stream);
 
 #ifdef __cplusplus
 }

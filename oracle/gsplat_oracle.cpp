@@ -622,58 +622,67 @@ void draw(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const
 // reference, neither the 0.99 clamp nor max(0, .) is differentiated.
 // Gradient outputs are accumulated (+=); any may be null.
 template <typename R>
+inline void atomic_add(R* p, R v) {
+  std::atomic_ref<R>(*p).fetch_add(v, std::memory_order_relaxed);
+}
+
+template <typename R>
 void draw_backward(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const R* us,
                    const R* cinv, const R* alphas, const R* feat, const R* final_tau,
                    const int32_t* contrib, const R* dout, const R* dT, R* dfeat, R* dalpha, R* du,
                    R* dq) {
   int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   int64_t n_tiles = (int64_t)gx * gy;
-  // Serial over tiles: the gradient outputs are shared between tiles.
-  std::vector<R> G(K), dl(K);
-  for (int64_t t = 0; t < n_tiles; ++t) {
-    int32_t s = ranges[2 * t], en = ranges[2 * t + 1];
-    if (en - s == 0) continue;
-    int tx = (int)(t % gx), ty = (int)(t / gx);
-    for (int py = ty * kTile; py < std::min(H, ty * kTile + kTile); ++py)
-      for (int px = tx * kTile; px < std::min(W, tx * kTile + kTile); ++px) {
-        int64_t pix = (int64_t)py * W + px;
-        for (int k = 0; k < K; ++k) {
-          dl[k] = dout[(int64_t)k * H * W + pix];
-          G[k] = 0;
-        }
-        R Tf = final_tau[pix];
-        R dTf = dT ? dT[pix] : R(0);
-        R T = Tf;
-        for (int32_t j = s + contrib[pix] - 1; j >= s; --j) {
-          int32_t g = gsid[j];
-          R dx = us[2 * g] - (R)px, dy = us[2 * g + 1] - (R)py;
-          const R* q = cinv + 3 * g;
-          R maha = std::max(R(0), q[0] * dx * dx + q[2] * dy * dy + R(2) * q[1] * dx * dy);
-          R gg = std::exp(R(-0.5) * maha);
-          R ap = std::min((R)kAlphaMax, alphas[g] * gg);
-          if (ap < (R)kAlphaMin) continue;
-          T = T / (R(1) - ap);
-          R dap = 0;
+  // Tiles run in parallel; the per-Gaussian gradient sums they share are
+  // accumulated with atomic adds.
+  parallel_for(n_tiles, [&](int64_t tb, int64_t te) {
+    std::vector<R> G(K), dl(K);
+    for (int64_t t = tb; t < te; ++t) {
+      int32_t s = ranges[2 * t], en = ranges[2 * t + 1];
+      if (en - s == 0) continue;
+      int tx = (int)(t % gx), ty = (int)(t / gx);
+      for (int py = ty * kTile; py < std::min(H, ty * kTile + kTile); ++py)
+        for (int px = tx * kTile; px < std::min(W, tx * kTile + kTile); ++px) {
+          int64_t pix = (int64_t)py * W + px;
           for (int k = 0; k < K; ++k) {
-            R f = feat[(int64_t)g * K + k];
-            if (dfeat) dfeat[(int64_t)g * K + k] += dl[k] * (ap * T);
-            dap += dl[k] * (T * (f - G[k]));
-            G[k] = ap * f + (R(1) - ap) * G[k];
+            dl[k] = dout[(int64_t)k * H * W + pix];
+            G[k] = 0;
           }
-          dap += dTf * (-Tf / (R(1) - ap));
-          if (dalpha) dalpha[g] += dap * gg;
-          if (du) {
-            du[2 * g] += dap * ((-q[0] * dx - q[1] * dy) * ap);
-            du[2 * g + 1] += dap * ((-q[1] * dx - q[2] * dy) * ap);
-          }
-          if (dq) {
-            dq[3 * g] += dap * (R(-0.5) * ap * dx * dx);
-            dq[3 * g + 1] += dap * (R(-1) * ap * dx * dy);
-            dq[3 * g + 2] += dap * (R(-0.5) * ap * dy * dy);
+          R Tf = final_tau[pix];
+          R dTf = dT ? dT[pix] : R(0);
+          R T = Tf;
+          int32_t top = std::min(contrib[pix], en - s);
+          for (int32_t j = s + top - 1; j >= s; --j) {
+            int32_t g = gsid[j];
+            R dx = us[2 * g] - (R)px, dy = us[2 * g + 1] - (R)py;
+            const R* q = cinv + 3 * g;
+            R maha = std::max(R(0), q[0] * dx * dx + q[2] * dy * dy + R(2) * q[1] * dx * dy);
+            R gg = std::exp(R(-0.5) * maha);
+            R ap = std::min((R)kAlphaMax, alphas[g] * gg);
+            if (ap < (R)kAlphaMin) continue;
+            T = T / (R(1) - ap);
+            R dap = 0;
+            for (int k = 0; k < K; ++k) {
+              R f = feat[(int64_t)g * K + k];
+              if (dfeat) atomic_add(dfeat + (int64_t)g * K + k, dl[k] * (ap * T));
+              dap += dl[k] * (T * (f - G[k]));
+              G[k] = ap * f + (R(1) - ap) * G[k];
+            }
+            dap += dTf * (-Tf / (R(1) - ap));
+            if (dalpha) atomic_add(dalpha + g, dap * gg);
+            if (du) {
+              atomic_add(du + 2 * g, dap * ((-q[0] * dx - q[1] * dy) * ap));
+              atomic_add(du + 2 * g + 1, dap * ((-q[1] * dx - q[2] * dy) * ap));
+            }
+            if (dq) {
+              atomic_add(dq + 3 * g, dap * (R(-0.5) * ap * dx * dx));
+              atomic_add(dq + 3 * g + 1, dap * (R(-1) * ap * dx * dy));
+              atomic_add(dq + 3 * g + 2, dap * (R(-0.5) * ap * dy * dy));
+            }
           }
         }
-      }
-  }
+    }
+  }, 1);
 }
 
 }  // namespace

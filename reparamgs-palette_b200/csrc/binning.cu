@@ -435,7 +435,7 @@ int launch_pack(int64_t n, int H, int W, int channels, const float* us, const fl
                 const float* alphas, const void* feats, int feat_dtype, float* depths,
                 int32_t* areas, bool bin, const SplatState& s, cudaStream_t st) {
   if (bin && cudaMemsetAsync(s.stats, 0, 16 * sizeof(uint32_t), st) != cudaSuccess)
-    return check_launch("splat_pack (memset)");
+    return check_launch("splat_pack (memset)", 0);
   if (n == 0) return GSB_OK;
   const uint32_t gx = (uint32_t)div_up(W, kTile), gy = (uint32_t)div_up(H, kTile);
   if (feat_dtype == GSB_DTYPE_BF16)
@@ -509,7 +509,7 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
   const size_t smem = (size_t)kSortTile * (sizeof(KT) + 4) + (8 * 256 + 256 + 256 + 8) * 4;
   if (cudaFuncSetAttribute(k_radix_downsweep<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
-    return check_launch("splat_sort (smem attribute)");
+    return check_launch("splat_sort (smem attribute)", 0);
   KT* ks = ka;
   KT* kd = kb;
   int32_t* vs = va;
@@ -524,7 +524,7 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
     k_radix_scan<<<(int)mask + 1, 256, 0, st>>>(hist, p.n_sort_blocks, dtot);
     k_radix_downsweep<KT><<<nbk, kSortThreads, smem, st>>>(ks, vs, kd, vdst, p.M, shift, mask,
                                                            hist, dtot, p.n_sort_blocks);
-    rc = check_launch("splat_sort (radix pass)");
+    rc = check_launch("splat_sort (radix pass)", 3);
     if (rc) return rc;
     KT* kt = ks;
     ks = kd;
@@ -541,7 +541,7 @@ int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
                 int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st) {
   (void)H;
   if (cudaMemsetAsync(ranges_out, 0, (size_t)p.n_tiles * 2 * sizeof(int32_t), st) != cudaSuccess)
-    return check_launch("splat_sort (memset)");
+    return check_launch("splat_sort (memset)", 0);
   if (p.M == 0) return GSB_OK;
   return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, st)
                 : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, st);

@@ -2,6 +2,7 @@
 // argument validation, workspace carving and kernel launches.  No entry point
 // allocates device memory or synchronises, except gsb_splat_counts, which
 // must return the patch count to the host.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -12,6 +13,7 @@
 namespace gsb {
 
 static thread_local char g_err[512] = {0};
+static std::atomic<unsigned long long> g_launches{0};
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -20,12 +22,13 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
-int check_launch(const char* what) {
+int check_launch(const char* what, int launches) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error("%s: %s", what, cudaGetErrorString(e));
     return GSB_ERR_CUDA;
   }
+  g_launches.fetch_add((unsigned long long)launches, std::memory_order_relaxed);
   return GSB_OK;
 }
 
@@ -72,6 +75,9 @@ using namespace gsb;
 
 GSB_API const char* gsb_last_error(void) { return g_err; }
 GSB_API int gsb_version(void) { return 100; }
+GSB_API unsigned long long gsb_launch_count(void) {
+  return g_launches.load(std::memory_order_relaxed);
+}
 
 GSB_API int gsb_project(int64_t n, const float* pws, const float* Rcw, const float* tcw, float fx,
                         float fy, float cx, float cy, float* us, float* pcs, float* depths,
@@ -216,7 +222,7 @@ GSB_API int gsb_splat_counts(int64_t n, const void* state, uint32_t* host_out, v
   uint32_t v[4];
   if (cudaMemcpyAsync(v, s.stats, sizeof(v), cudaMemcpyDeviceToHost, ST(stream)) != cudaSuccess ||
       cudaStreamSynchronize(ST(stream)) != cudaSuccess)
-    return check_launch("splat_counts");
+    return check_launch("splat_counts", 0);
   GSB_CHECK_ARG(v[3] == 0 && v[0] < (uint32_t)INT32_MAX,
                 "splat_counts: patch count exceeds the int32 index range");
   host_out[0] = v[0];
@@ -278,4 +284,35 @@ GSB_API int gsb_splat_backward(int64_t n, int height, int width, int channels, c
   if (rc) return rc;
   return launch_draw_backward(n, height, width, channels, ranges, gsid, s, contrib, final_tau,
                               dloss_dout, dloss_dtau, dfeats, dalphas, dus, dcinv2ds, ST(stream));
+}
+
+GSB_API int gsb_splat_backward_packed(int64_t n, int height, int width, int channels,
+                                      const int32_t* ranges, const int32_t* gsid,
+                                      const int32_t* contrib, const float* final_tau,
+                                      const float* dloss_dout, const float* dloss_dtau,
+                                      const void* state, float* dfeats, float* dalphas, float* dus,
+                                      float* dcinv2ds, void* stream) {
+  int rc = check_image("splat_backward_packed", n, height, width, channels);
+  if (rc) return rc;
+  GSB_CHECK_ARG(state && ranges && contrib && final_tau && dloss_dout && dfeats,
+                "splat_backward_packed: null pointer");
+  const bool geom = dalphas || dus || dcinv2ds;
+  GSB_CHECK_ARG(!geom || (dalphas && dus && dcinv2ds),
+                "splat_backward_packed: pass all of dalphas/dus/dcinv2ds or none");
+  GSB_CHECK_ARG(!dloss_dtau || geom, "splat_backward_packed: dloss_dtau needs the geometry outputs");
+  const SplatState s = carve_state((void*)state, n, channels);
+  return launch_draw_backward(n, height, width, channels, ranges, gsid, s, contrib, final_tau,
+                              dloss_dout, dloss_dtau, dfeats, dalphas, dus, dcinv2ds, ST(stream));
+}
+
+GSB_API int gsb_palette_l1(int K, int height, int width, const float* layer,
+                           const float* palette, const float* target, float* image, float* loss,
+                           float* dlayer, float* dpalette, void* stream) {
+  GSB_CHECK_ARG(K >= 1 && K <= GSB_MAX_CHANNELS, "palette_l1: channels must be in [1, %d]",
+                GSB_MAX_CHANNELS);
+  GSB_CHECK_ARG(height >= 0 && width >= 0, "palette_l1: negative image size");
+  GSB_CHECK_ARG(palette && loss, "palette_l1: null pointer");
+  GSB_CHECK_ARG(((int64_t)height * width == 0) || (layer && target), "palette_l1: null input");
+  return launch_palette_l1(K, height, width, layer, palette, target, image, loss, dlayer, dpalette,
+                           ST(stream));
 }

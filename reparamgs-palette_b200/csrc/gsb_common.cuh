@@ -72,7 +72,9 @@ struct RecordLayout {
 
 // ----------------------------------------------------------- error plumbing
 void set_error(const char* fmt, ...);
-int check_launch(const char* what);
+// Records `launches` kernel launches (when the last launch succeeded) and
+// converts a launch error into GSB_ERR_CUDA with a message.
+int check_launch(const char* what, int launches = 1);
 
 }  // namespace gsb
 

@@ -28,6 +28,11 @@ int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtyp
                                int L, float* dA, float* dB, cudaStream_t st);
 int launch_lab2rgb(int H, int W, const float* lab, float* rgb, cudaStream_t st);
 
+// loss.cu
+int launch_palette_l1(int K, int H, int W, const float* layer, const float* palette,
+                      const float* target, float* image, float* loss, float* dlayer, float* dpal,
+                      cudaStream_t st);
+
 // binning.cu -- per-Gaussian binning state carved out of one caller buffer.
 struct SplatState {
   float4* records;       // [n * rec_vec4]

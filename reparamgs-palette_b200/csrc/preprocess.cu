@@ -309,79 +309,6 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// sh2Weight_fast -- gsplatcu/kernel.cu:884-987, generalised to rank r:
-// coefficient (l, k) of the L*K block (g = l*K + k) is C[g / Q][g % Q] with
-// C = A B, A [P,r], B [r,Q].
-template <int K, typename T>
-__global__ void __launch_bounds__(kThreads)
-    k_sh2weight_lowrank(int64_t n, const T* __restrict__ dc, const T* __restrict__ A,
-                        const T* __restrict__ B, int P, int Q, int rank, int L,
-                        const float* __restrict__ pws, const float* __restrict__ twc,
-                        float* __restrict__ w, float* __restrict__ ddc, float* __restrict__ ylm) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float wk[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    wk[k] = SH_C0 * ld(dc, i * K + k);
-    if (ddc) ddc[i * K + k] = SH_C0;
-  }
-  if (L > 0) {
-    float dir[3], Y[16];
-    const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
-    const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
-    view_direction(pw, cam, dir, nullptr, nullptr);
-    sh_basis(dir, L + 1, Y);
-    if (ylm)
-      for (int l = 0; l < L; ++l) ylm[i * L + l] = Y[l + 1];
-    const T* a = A + i * (int64_t)P * rank;
-    const T* b = B + i * (int64_t)rank * Q;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      float acc = 0.f;
-      for (int l = 0; l < L; ++l) {
-        const int g = l * K + k, row = g / Q, col = g % Q;
-        float coef = ld(a, row * rank) * ld(b, col);
-        for (int r = 1; r < rank; ++r) coef += ld(a, row * rank + r) * ld(b, r * Q + col);
-        acc += coef * Y[l + 1];
-      }
-      wk[k] += acc;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < K; ++k) w[i * K + k] = wk[k];
-}
-
-// sh2Weight_fast_B -- gsplatcu/kernel.cu:994-1032, rank r.  One thread owns
-// one Gaussian's rows of dA / dB, so the sums are accumulated sequentially in
-// the reference's (k, l) order without atomics.
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
-    k_sh2weight_lowrank_b(int64_t n, const T* __restrict__ A, const T* __restrict__ B,
-                          const float* __restrict__ ylm, const float* __restrict__ dw, int K,
-                          int P, int Q, int rank, int L, float* __restrict__ dA,
-                          float* __restrict__ dB) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const T* a = A + i * (int64_t)P * rank;
-  const T* b = B + i * (int64_t)rank * Q;
-  float* da = dA + i * (int64_t)P * rank;
-  float* db = dB + i * (int64_t)rank * Q;
-  for (int k = 0; k < P * rank; ++k) da[k] = 0.f;
-  for (int k = 0; k < rank * Q; ++k) db[k] = 0.f;
-  for (int k = 0; k < K; ++k) {
-    const float g0 = dw[i * K + k];
-    for (int l = 0; l < L; ++l) {
-      const int g = l * K + k, row = g / Q, col = g % Q;
-      const float y = ylm[i * L + l];
-      for (int r = 0; r < rank; ++r) {
-        da[row * rank + r] = __fadd_rn(da[row * rank + r], g0 * ld(b, r * Q + col) * y);
-        db[r * Q + col] = __fadd_rn(db[r * Q + col], g0 * ld(a, row * rank + r) * y);
-      }
-    }
-  }
-}
-
 // ------------------------------------------------------------ launchers
 static int grid_for(int64_t n) { return div_up(n > 0 ? n : 1, kThreads); }
 
@@ -436,48 +363,6 @@ int launch_sh2feat(int64_t n, const void* shs, int dtype, int nb, int K, const f
   return dtype == GSB_DTYPE_BF16
              ? sh2feat_t<__nv_bfloat16>(n, shs, nb, K, pws, twc, feat, dshs, dpws, st)
              : sh2feat_t<float>(n, shs, nb, K, pws, twc, feat, dshs, dpws, st);
-}
-
-template <typename T>
-static int lowrank_t(int64_t n, const void* dc, const void* A, const void* B, int K, int P, int Q,
-                     int rank, int L, const float* pws, const float* twc, float* w, float* ddc,
-                     float* ylm, cudaStream_t st) {
-  const int g = grid_for(n);
-  const T *d = (const T*)dc, *a = (const T*)A, *b = (const T*)B;
-  switch (K) {
-#define GSB_K(KK)                                                                             \
-  case KK:                                                                                    \
-    k_sh2weight_lowrank<KK, T><<<g, kThreads, 0, st>>>(n, d, a, b, P, Q, rank, L, pws, twc, w, \
-                                                       ddc, ylm);                             \
-    break;
-    GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
-#undef GSB_K
-    default: return GSB_ERR_INVALID_ARGUMENT;
-  }
-  return check_launch("sh2Weight_fast");
-}
-
-int launch_sh2weight_lowrank(int64_t n, const void* dc, const void* A, const void* B, int dtype,
-                             int K, int P, int Q, int rank, int L, const float* pws,
-                             const float* twc, float* w, float* ddc, float* ylm, cudaStream_t st) {
-  if (n == 0) return GSB_OK;
-  return dtype == GSB_DTYPE_BF16
-             ? lowrank_t<__nv_bfloat16>(n, dc, A, B, K, P, Q, rank, L, pws, twc, w, ddc, ylm, st)
-             : lowrank_t<float>(n, dc, A, B, K, P, Q, rank, L, pws, twc, w, ddc, ylm, st);
-}
-
-int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtype,
-                               const float* ylm, const float* dw, int K, int P, int Q, int rank,
-                               int L, float* dA, float* dB, cudaStream_t st) {
-  if (n == 0) return GSB_OK;
-  const int g = grid_for(n);
-  if (dtype == GSB_DTYPE_BF16)
-    k_sh2weight_lowrank_b<__nv_bfloat16><<<g, kThreads, 0, st>>>(
-        n, (const __nv_bfloat16*)A, (const __nv_bfloat16*)B, ylm, dw, K, P, Q, rank, L, dA, dB);
-  else
-    k_sh2weight_lowrank_b<float><<<g, kThreads, 0, st>>>(n, (const float*)A, (const float*)B, ylm,
-                                                         dw, K, P, Q, rank, L, dA, dB);
-  return check_launch("sh2Weight_fast_B");
 }
 
 }  // namespace gsb

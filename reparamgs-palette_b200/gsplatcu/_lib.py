@@ -28,6 +28,7 @@ _i64, _i32, _u32, _f32, _p, _sz = C.c_int64, C.c_int, C.c_uint32, C.c_float, C.c
 _SIGS = {
     "gsb_last_error": (C.c_char_p, []),
     "gsb_version": (_i32, []),
+    "gsb_launch_count": (C.c_ulonglong, []),
     "gsb_project": (_i32, [_i64, _p, _p, _p, _f32, _f32, _f32, _f32, _p, _p, _p, _p, _p]),
     "gsb_compute_cov3d": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_compute_cov2d": (_i32, [_i64, _p, _p, _p, _p, _f32, _f32, _f32, _f32, _p, _p, _p, _p]),
@@ -47,6 +48,9 @@ _SIGS = {
     "gsb_splat_draw": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _f32, _p, _p, _p, _p]),
     "gsb_splat_backward": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _i32, _p, _p, _p, _p,
                                   _p, _p, _p, _p, _p, _p, _p, _p]),
+    "gsb_palette_l1": (_i32, [_i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "gsb_splat_backward_packed": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p,
+                                         _p, _p, _p, _p]),
 }
 
 _lib = None

@@ -23,7 +23,7 @@ import torch
 
 
 class Camera:
-    def __init__(self, id, width, height, fx, fy, cx, cy, Rcw, tcw, path=""):
+    def __init__(self, id, width, height, fx, fy, cx, cy, Rcw, tcw, path="", twc=None):
         self.id = id
         self.width = width
         self.height = height
@@ -33,7 +33,9 @@ class Camera:
         self.cy = cy
         self.Rcw = Rcw
         self.tcw = tcw
-        self.twc = -torch.linalg.inv(Rcw) @ tcw
+        # camera centre; callers that already have it (e.g. computed on the host)
+        # may pass it to skip the device-side 3x3 inverse
+        self.twc = -torch.linalg.inv(Rcw) @ tcw if twc is None else twc
         self.path = path
 
     def to(self, device):

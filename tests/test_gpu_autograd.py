@@ -1,0 +1,86 @@
+"""GPU tests of the autograd layer: WeightGSFunctionTest / WeightGSFunctionFast
+(reference semantics, gsplat/gsmodel.py:104-200) and the fused palette L1 loss,
+against torch / the CPU oracle."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as orc
+from palette_b200.autograd import WeightGSFunctionFast, WeightGSFunctionTest
+from palette_b200.loss import palette_image, palette_l1_loss
+from palette_b200.scene import look_at, synthetic_scene, to_torch
+from helpers import np_of, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def test_palette_l1_matches_torch(cuda_ok):
+    g = torch.Generator("cuda").manual_seed(0)
+    K, H, W = 5, 67, 129
+    layer = torch.rand((K, H, W), device="cuda", generator=g).requires_grad_()
+    pal = torch.rand((K, 3), device="cuda", generator=g).requires_grad_()
+    tgt = torch.rand((3, H, W), device="cuda", generator=g)
+    loss = palette_l1_loss(layer, pal, tgt)
+    loss.backward()
+    l2 = layer.detach().clone().requires_grad_()
+    p2 = pal.detach().clone().requires_grad_()
+    ref = (torch.einsum("kc,khw->chw", p2, l2) - tgt).abs().mean()
+    ref.backward()
+    assert abs(float(loss) - float(ref)) < 1e-6 * max(1.0, abs(float(ref)))
+    assert rel_err(layer.grad, l2.grad) < 1e-6
+    assert rel_err(pal.grad, p2.grad) < 1e-5
+    img = palette_image(layer.detach(), pal.detach())
+    assert rel_err(img, torch.einsum("kc,khw->chw", pal.detach(), layer.detach())) < 1e-6
+
+
+def _oracle_grads(st, sc, cam, w, layer_grad):
+    """dL/dweights of the reference backward through the oracle."""
+    from gsplatcu import project, computeCov3D, computeCov2D, inverseCov2D, splat_weight
+    H, W = cam.height, cam.width
+    us, pcs, d = project(st["pws"], cam.Rcw, cam.tcw, cam.fx, cam.fy, cam.cx, cam.cy, False)
+    c3, = computeCov3D(st["rots"], st["scales"], d, False)
+    c2, = computeCov2D(c3, pcs, cam.Rcw, d, cam.fx, cam.fy, W, H, False)
+    cinv, areas = inverseCov2D(c2, d, False)
+    layer, contrib, ft, ranges, gsid = splat_weight(H, W, 5, us, cinv, st["alphas"], d, w, areas)
+    r = orc.draw_backward(H, W, 5, np_of(ranges), np_of(gsid), np_of(us), np_of(cinv),
+                          np_of(st["alphas"]), np_of(w), np_of(ft), np_of(contrib), np_of(layer_grad))
+    return r["dfeat"]
+
+
+@pytest.mark.parametrize("rank", [1, 3])
+def test_weight_function_fast_gradients(cuda_ok, rank):
+    sc = synthetic_scene(6000, seed=60 + rank, mode="lowrank", rank=rank)
+    st = to_torch(sc)
+    cam = look_at((0.5, -7.5, 1.0), width=96, height=80)
+    A, B = st["A"], st["B"]
+    if rank == 1:
+        A, B = A[:, :, 0].contiguous(), B[:, 0, :].contiguous()
+    dc, A, B = st["dc"].requires_grad_(), A.requires_grad_(), B.requires_grad_()
+    layer, mask = WeightGSFunctionFast.apply(st["pws"], dc, A, B, st["alphas"], st["scales"],
+                                             st["rots"], cam, 5, 15)
+    G = torch.randn_like(layer)
+    (layer * G).sum().backward()
+    import gsplatcu as gsc
+    w, ddc, ylm = gsc.sh2Weight_fast(dc.detach(), A.detach(), B.detach(), st["pws"], cam.twc, True, 5, 15)
+    dw = _oracle_grads(st, sc, cam, w, G)
+    twc = orc.camera_arrays(cam, np.float32)[2]
+    o_dA, o_dB = orc.sh2weight_fast_b(np_of(A), np_of(B), np_of(ylm), dw, 5, 15)
+    assert rel_err(dc.grad, dw * np.float32(0.28209479177387814)) < 1e-4
+    assert rel_err(A.grad, o_dA) < 1e-4 and rel_err(B.grad, o_dB) < 1e-4
+    assert mask.dtype == torch.bool and mask.shape == (6000,)
+
+
+def test_weight_function_test_gradients(cuda_ok):
+    sc = synthetic_scene(6000, seed=70)
+    st = to_torch(sc)
+    cam = look_at((0.5, -7.5, 1.0), width=96, height=80)
+    shs = st["shs"].requires_grad_()
+    layer, mask = WeightGSFunctionTest.apply(st["pws"], shs, st["alphas"], st["scales"], st["rots"],
+                                             cam, 5)
+    G = torch.randn_like(layer)
+    (layer * G).sum().backward()
+    import gsplatcu as gsc
+    w, dshs, _ = gsc.sh2Weight(shs.detach(), st["pws"], cam.twc, True, 5)
+    dw = _oracle_grads(st, sc, cam, w, G)
+    expect = (dw[:, None, :] * np_of(dshs)[:, 0, :, None]).reshape(6000, -1)  # [N,16,K] outer
+    assert rel_err(shs.grad, expect) < 1e-4
