@@ -193,7 +193,9 @@ def profile_traffic(kernel_tag):
 
 
 def timed(fn, reps, stream):
-    """Device time (ms) of `reps` calls of fn on `stream`, CUDA events, synced both sides."""
+    """Device time (ms) of `reps` calls of fn on `stream` (after one untimed
+    call), CUDA events, synced both sides."""
+    fn()
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record(stream)
@@ -229,7 +231,8 @@ def stage_breakdown(wl, reps=5):
         out["preprocess"] = timed(pre, reps, st) / reps
         us, cinv, d, areas, w, ylm = pre()
         n = us.shape[0]
-        state = torch.empty(int(L.gsb_splat_state_bytes(n, K)), dtype=torch.uint8, device=us.device)
+        state = torch.empty(int(L.gsb_splat_state_bytes(n, K, H, W)), dtype=torch.uint8,
+                            device=us.device)
         import ctypes as C
         sp = _lib.stream_of(us)
         d0, a0 = d.clone(), areas.clone()
@@ -242,16 +245,16 @@ def stage_breakdown(wl, reps=5):
                       _lib.ptr(state), sp)
         out["bin_pack_scan"] = timed(pack, reps, st) / reps
         pack()
-        host = (C.c_uint32 * 2)()
-        _lib.call("bench", "gsb_splat_counts", n, _lib.ptr(state), host, sp)
-        M, maxdk = int(host[0]), int(host[1])
-        ws = torch.empty(int(L.gsb_splat_sort_bytes(n, H, W, M, maxdk)), dtype=torch.uint8,
+        plan = _lib.SplatPlan()
+        _lib.call("bench", "gsb_splat_counts", n, H, W, _lib.ptr(state), C.byref(plan), sp)
+        M = int(plan.patches)
+        ws = torch.empty(int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan))), dtype=torch.uint8,
                          device=us.device)
         gx, gy = (W + 15) // 16, (H + 15) // 16
         gsid = torch.empty(M, dtype=torch.int32, device=us.device)
         ranges = torch.empty((gx * gy, 2), dtype=torch.int32, device=us.device)
         out["bin_sort"] = timed(lambda: _lib.call(
-            "bench", "gsb_splat_sort", n, H, W, M, maxdk, _lib.ptr(state), _lib.ptr(ws),
+            "bench", "gsb_splat_sort", n, H, W, C.byref(plan), _lib.ptr(state), _lib.ptr(ws),
             _lib.ptr(gsid), _lib.ptr(ranges), sp), reps, st) / reps
         layer = torch.empty((K, H, W), device=us.device)
         contrib = torch.empty((H, W), dtype=torch.int32, device=us.device)

@@ -44,6 +44,12 @@ extern "C" {
 const char* gsb_last_error(void);
 /* Library ABI version, major * 100 + minor. */
 int gsb_version(void);
+/* Device-side status word of the library's kernels on the current device:
+ * bit 0 (GSB_STATUS_BULK_TIMEOUT) -- a bounded wait for a bulk (TMA) copy gave
+ * up and the kernel returned without results.  Synchronises `stream`;
+ * clears the word when `clear` is non-zero. */
+#define GSB_STATUS_BULK_TIMEOUT 1u
+int gsb_device_status(uint32_t* status, int clear, void* stream);
 /* Number of kernels this library has launched in the process so far
  * (diagnostic; used to report how many of the library's kernels a timed
  * region ran). */
@@ -110,42 +116,51 @@ int gsb_lab2rgb(int height, int width, const float* lab, float* rgb, void* strea
 
 /* ------------------------------------------------------ splatting pipeline
  * splat_weight / splat_color (gsplatcu/gausplat.cu:161-249, 25-109) run as
- * three calls so that the caller owns every allocation:
+ * four calls so that the caller owns every allocation:
  *
  *   1. gsb_splat_pack      -- per-Gaussian tile rectangles and patch counts
  *                             (getRects, gsplatcu/kernel.cu:127-162, updating
  *                             depths/areas in place like the reference), the
- *                             packed compositing records, and the patch-count
+ *                             packed compositing records and the patch-count
  *                             prefix sum.  Needs `state` of
- *                             gsb_splat_state_bytes(n, channels) bytes.
- *   2. gsb_splat_counts    -- copies {patch count M, max depth key} to host
- *                             memory (synchronises `stream`).
- *   3. gsb_splat_sort      -- key emission, radix sort and per-tile ranges
+ *                             gsb_splat_state_bytes(...) bytes.
+ *   2. gsb_splat_counts    -- copies the sizes the next step needs into a
+ *                             gsb_splat_plan (synchronises `stream`, as the
+ *                             reference reads its patch count back).
+ *   3. gsb_splat_sort      -- key emission, sort and per-tile ranges
  *                             (createKeys / sort_by_key / getRanges).  Needs
- *                             `sort_ws` of gsb_splat_sort_bytes(...) bytes.
+ *                             `sort_ws` of gsb_splat_sort_bytes(plan) bytes.
  *   4. gsb_splat_draw      -- front-to-back compositing (draw_weight /
  *                             draw_color, gsplatcu/kernel.cu:194-372).
  *
  * Tile lists and ranges are bit-identical to the reference's given identical
- * us/areas/depths: keys are (tile, uint32(depth*1000)) sorted stably in
- * Gaussian order.  `channels` is K for weights, 3 for colours. */
-size_t gsb_splat_state_bytes(int64_t n, int channels);
+ * us/areas/depths: keys (tile << b | uint32(depth*1000)) are emitted in
+ * Gaussian order and sorted stably, b being the bit length of the largest
+ * depth key, so each tile's list is ordered by (depth key, Gaussian id) as
+ * the reference's stable 64-bit sort orders it; the LSD radix sort runs
+ * ceil(key bits / 9) passes.  `channels` is K for weights, 3 for colours. */
+typedef struct gsb_splat_plan {
+  int64_t patches;        /* M, total (tile, Gaussian) patches          */
+  uint32_t max_depth_key; /* max uint32(depth*1000) of binned Gaussians */
+  uint32_t reserved;      /* zero                                       */
+} gsb_splat_plan;
+
+size_t gsb_splat_state_bytes(int64_t n, int channels, int height, int width);
 
 int gsb_splat_pack(int64_t n, int height, int width, int channels, const float* us,
                    const float* cinv2ds, const float* alphas, const void* feats, int feat_dtype,
                    float* depths, int32_t* areas, void* state, void* stream);
 
-/* host_out[0] = M (patches), host_out[1] = max uint32(depth*1000) over
- * binned Gaussians.  Blocks until `stream` has finished step 1. */
-int gsb_splat_counts(int64_t n, const void* state, uint32_t* host_out, void* stream);
+/* Fills *plan; blocks until `stream` has finished step 1. */
+int gsb_splat_counts(int64_t n, int height, int width, const void* state, gsb_splat_plan* plan,
+                     void* stream);
 
-size_t gsb_splat_sort_bytes(int64_t n, int height, int width, int64_t patches,
-                            uint32_t max_depth_key);
+size_t gsb_splat_sort_bytes(int64_t n, int height, int width, const gsb_splat_plan* plan);
 
 /* gsid_out [patches] (int32) receives the sorted Gaussian ids; ranges_out
  * [tiles,2] (int32) the per-tile [start,end) -- (0,0) for empty tiles and,
  * as in the reference's getRanges, (0,0) for the single tile when M == 1. */
-int gsb_splat_sort(int64_t n, int height, int width, int64_t patches, uint32_t max_depth_key,
+int gsb_splat_sort(int64_t n, int height, int width, const gsb_splat_plan* plan,
                    const void* state, void* sort_ws, int32_t* gsid_out, int32_t* ranges_out,
                    void* stream);
 
@@ -159,7 +174,8 @@ int gsb_splat_draw(int64_t n, int height, int width, int channels, const int32_t
 
 /* splat_weight_B / splat_color_B (gsplatcu/gausplat.cu:252-292, 111-155):
  * reverse-order adjoint of the compositing.  Re-packs the records into
- * `state` (gsb_splat_state_bytes) from the forward's inputs.  Outputs are
+ * `state` (gsb_splat_state_bytes(n, channels, height, width) bytes) from the
+ * forward's inputs.  Outputs are
  * ACCUMULATED (+=) and may be NULL:
  *   dfeats [n,channels]  -- dL/dweights (splat_weight_B) / dL/dcolors
  *   dalphas [n], dus [n,2], dcinv2ds [n,3]  -- the geometry/opacity adjoint of

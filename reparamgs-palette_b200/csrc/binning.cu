@@ -9,6 +9,8 @@
 // reference's stable 64-bit thrust::sort_by_key produces.  Keys here hold
 // only ceil(log2 T) tile bits above the depth-key bits actually used, so the
 // sort runs ceil(bits/8) passes instead of eight.
+#include <algorithm>
+
 #include "gsb_geometry.cuh"
 #include "gsb_internal.h"
 
@@ -21,34 +23,42 @@ static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Layout: channel-independent arrays first (so that callers that do not know
 // the channel count can locate them), packed records last.
-size_t splat_state_bytes(int64_t n, int channels) {
+static void state_layout(int64_t n, int channels, int H, int W, size_t* offs) {
   const int64_t nb = (n + kBinBlock - 1) / kBinBlock;
+  const int64_t gx = div_up(W, kTile), gy = div_up(H, kTile);
   size_t b = 0;
-  b += align256((size_t)n * 8);                       // rects
-  b += align256((size_t)n * 4);                       // dkeys
-  b += align256((size_t)n * 4);                       // counts
-  b += align256((size_t)(nb > 0 ? nb : 1) * 4);       // block sums
-  b += align256(16 * 4);                              // stats
-  b += align256((size_t)n * record_vec4(channels) * 16);  // records
-  return b;
+  offs[0] = b; b += align256((size_t)n * 8);                          // rects
+  offs[1] = b; b += align256((size_t)n * 4);                          // dkeys
+  offs[2] = b; b += align256((size_t)n * 4);                          // counts
+  offs[3] = b; b += align256((size_t)(nb > 0 ? nb : 1) * 4);          // block sums
+  offs[4] = b; b += align256(16 * 4);                                 // stats
+  offs[5] = b; b += align256((size_t)n * record_vec4(channels) * 16); // records
+  offs[6] = b;
+  (void)gx;
+  (void)gy;
 }
 
-SplatState carve_state(void* base, int64_t n, int channels) {
-  SplatState s;
+size_t splat_state_bytes(int64_t n, int channels, int H, int W) {
+  size_t offs[7];
+  state_layout(n, channels, H, W, offs);
+  return offs[6];
+}
+
+SplatState carve_state(void* base, int64_t n, int channels, int H, int W) {
+  size_t o[7];
+  state_layout(n, channels, H, W, o);
   char* p = (char*)base;
+  SplatState s;
   s.rec_vec4 = record_vec4(channels);
   s.n_blocks = (n + kBinBlock - 1) / kBinBlock;
-  s.rects = (uint2*)p;
-  p += align256((size_t)n * 8);
-  s.dkeys = (uint32_t*)p;
-  p += align256((size_t)n * 4);
-  s.counts = (uint32_t*)p;
-  p += align256((size_t)n * 4);
-  s.block_sums = (uint32_t*)p;
-  p += align256((size_t)(s.n_blocks > 0 ? s.n_blocks : 1) * 4);
-  s.stats = (uint32_t*)p;
-  p += align256(16 * 4);
-  s.records = (float4*)p;
+  s.gx = div_up(W, kTile);
+  s.gy = div_up(H, kTile);
+  s.rects = (uint2*)(p + o[0]);
+  s.dkeys = (uint32_t*)(p + o[1]);
+  s.counts = (uint32_t*)(p + o[2]);
+  s.block_sums = (uint32_t*)(p + o[3]);
+  s.stats = (uint32_t*)(p + o[4]);
+  s.records = (float4*)(p + o[5]);
   return s;
 }
 
@@ -281,9 +291,9 @@ template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
     k_radix_upsweep(const KT* __restrict__ keys, int64_t M, int shift, uint32_t mask,
                     uint32_t* __restrict__ hist, int64_t nblocks) {
-  __shared__ uint32_t h[8][256];
+  __shared__ uint32_t h[8][kRadixBins];
   const int w = threadIdx.x >> 5;
-  for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) (&h[0][0])[k] = 0u;
+  for (int k = threadIdx.x; k < 8 * kRadixBins; k += kSortThreads) (&h[0][0])[k] = 0u;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortTile;
 #pragma unroll 4
@@ -292,11 +302,11 @@ __global__ void __launch_bounds__(kSortThreads)
     if (idx < M) atomicAdd(&h[w][(uint32_t)(keys[idx] >> shift) & mask], 1u);
   }
   __syncthreads();
-  if (threadIdx.x <= mask) {
+  for (uint32_t d = threadIdx.x; d <= mask; d += kSortThreads) {
     uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) s += h[k][threadIdx.x];
-    hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = s;
+    for (int k = 0; k < 8; ++k) s += h[k][d];
+    hist[(int64_t)d * nblocks + blockIdx.x] = s;
   }
 }
 
@@ -320,70 +330,72 @@ __global__ void __launch_bounds__(256)
 // Stable scatter of one digit pass.  Items of a block are ranked in their
 // original order (warp w owns items [512w, 512w+512), lane-minor), staged in
 // shared memory in digit order and written out in digit-contiguous runs.
+// Thread t owns digits 2t and 2t+1 in the per-digit phases.
 template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
     k_radix_downsweep(const KT* __restrict__ kin, const int32_t* __restrict__ vin,
                       KT* __restrict__ kout, int32_t* __restrict__ vout, int64_t M, int shift,
                       uint32_t mask, const uint32_t* __restrict__ hist,
                       const uint32_t* __restrict__ digit_tot, int64_t nblocks) {
+  static_assert(kRadixBins == 2 * kSortThreads, "two digits per thread");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   KT* sk = (KT*)smem_raw;
   int32_t* sv = (int32_t*)(sk + kSortTile);
-  uint32_t* wcnt = (uint32_t*)(sv + kSortTile);  // [8][256]
-  uint32_t* lstart = wcnt + 8 * 256;            // [256]
-  uint32_t* gstart = lstart + 256;              // [256]
-  uint32_t* warp_tot = gstart + 256;            // [8]
+  uint32_t* wcnt = (uint32_t*)(sv + kSortTile);  // [8][kRadixBins]
+  uint32_t* lstart = wcnt + 8 * kRadixBins;      // [kRadixBins]
+  uint32_t* gstart = lstart + kRadixBins;        // [kRadixBins]
+  uint32_t* warp_tot = gstart + kRadixBins;      // [8]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int k = threadIdx.x; k < 8 * 256; k += kSortThreads) wcnt[k] = 0u;
+  for (int k = threadIdx.x; k < 8 * kRadixBins; k += kSortThreads) wcnt[k] = 0u;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortTile + w * (32 * kSortItems);
   KT key[kSortItems];
   int32_t val[kSortItems];
-  uint32_t dig[kSortItems], rnk[kSortItems];
+  uint32_t rnk[kSortItems];
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
     const int64_t idx = base + r * 32 + lane;
     const bool ok = idx < M;
     key[r] = ok ? kin[idx] : (KT)0;
     val[r] = ok ? vin[idx] : 0;
-    dig[r] = ok ? ((uint32_t)(key[r] >> shift) & mask) : 0xffffu;
   }
   const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
-    const uint32_t d = dig[r];
+    const bool ok = base + r * 32 + lane < M;
+    const uint32_t d = ok ? ((uint32_t)(key[r] >> shift) & mask) : 0xffffu;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t before = (d < 256u) ? wcnt[w * 256 + d] : 0u;
+    const uint32_t before = ok ? wcnt[w * kRadixBins + d] : 0u;
     rnk[r] = before + __popc(peers & lt);
     __syncwarp();
-    if (d < 256u && lane == __ffs(peers) - 1) wcnt[w * 256 + d] = before + __popc(peers);
+    if (ok && lane == __ffs(peers) - 1) wcnt[w * kRadixBins + d] = before + __popc(peers);
     __syncwarp();
   }
   __syncthreads();
   // per digit: exclusive offsets across warps, block-local start, global start
-  const uint32_t d = threadIdx.x;
-  uint32_t tot = 0;
-  if (d <= mask) {
+  const uint32_t d0 = 2 * threadIdx.x, d1 = d0 + 1;
+  uint32_t tot0 = 0, tot1 = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const uint32_t c = wcnt[k * 256 + d];
-      wcnt[k * 256 + d] = tot;
-      tot += c;
-    }
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t c0 = wcnt[k * kRadixBins + d0], c1 = wcnt[k * kRadixBins + d1];
+    wcnt[k * kRadixBins + d0] = tot0;
+    wcnt[k * kRadixBins + d1] = tot1;
+    tot0 += c0;
+    tot1 += c1;
   }
-  const uint32_t dt = (d <= mask) ? digit_tot[d] : 0u;
-  const uint32_t ls = block_excl_scan256(tot, warp_tot, nullptr);
-  const uint32_t gd = block_excl_scan256(dt, warp_tot, nullptr);
-  if (d <= mask) {
-    lstart[d] = ls;
-    gstart[d] = gd + hist[(int64_t)d * nblocks + blockIdx.x];
-  }
+  const uint32_t dt0 = d0 <= mask ? digit_tot[d0] : 0u, dt1 = d1 <= mask ? digit_tot[d1] : 0u;
+  const uint32_t ls = block_excl_scan256(tot0 + tot1, warp_tot, nullptr);
+  const uint32_t gd = block_excl_scan256(dt0 + dt1, warp_tot, nullptr);
+  lstart[d0] = ls;
+  lstart[d1] = ls + tot0;
+  gstart[d0] = gd + (d0 <= mask ? hist[(int64_t)d0 * nblocks + blockIdx.x] : 0u);
+  gstart[d1] = gd + dt0 + (d1 <= mask ? hist[(int64_t)d1 * nblocks + blockIdx.x] : 0u);
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
-    const uint32_t dd = dig[r];
-    if (dd < 256u) {
-      const uint32_t pos = lstart[dd] + wcnt[w * 256 + dd] + rnk[r];
+    if (base + r * 32 + lane < M) {
+      const uint32_t dd = (uint32_t)(key[r] >> shift) & mask;
+      const uint32_t pos = lstart[dd] + wcnt[w * kRadixBins + dd] + rnk[r];
       sk[pos] = key[r];
       sv[pos] = val[r];
     }
@@ -460,6 +472,7 @@ static int bit_length(uint64_t v) {
   return b;
 }
 
+// Radix passes of at most kRadixBits bits each over the key bits in use.
 SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey) {
   SortPlan p;
   const int64_t gx = div_up(W, kTile), gy = div_up(H, kTile);
@@ -469,7 +482,7 @@ SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey) {
   p.dkey_bits = bit_length(max_dkey);
   p.key_bits = p.tile_bits + p.dkey_bits;
   p.wide = p.key_bits > 32;
-  p.passes = (p.key_bits + 7) / 8;
+  p.passes = (p.key_bits + kRadixBits - 1) / kRadixBits;
   p.n_sort_blocks = (M + kSortTile - 1) / kSortTile;
   p.key_bytes = p.wide ? 8 : 4;
   size_t off = 0;
@@ -482,9 +495,9 @@ SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey) {
   p.off_vals_b = off;
   off += align256((size_t)M * 4);
   p.off_hist = off;
-  off += align256((size_t)256 * (p.n_sort_blocks > 0 ? p.n_sort_blocks : 1) * 4);
+  off += align256((size_t)kRadixBins * (p.n_sort_blocks > 0 ? p.n_sort_blocks : 1) * 4);
   p.off_digit_tot = off;
-  off += align256(256 * 4);
+  off += align256(kRadixBins * 4);
   p.bytes_total = off;
   (void)n;
   return p;
@@ -506,7 +519,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
                                                     p.passes == 0 ? gsid_out : va);
   int rc = check_launch("splat_sort (emit)");
   if (rc) return rc;
-  const size_t smem = (size_t)kSortTile * (sizeof(KT) + 4) + (8 * 256 + 256 + 256 + 8) * 4;
+  const size_t smem =
+      (size_t)kSortTile * (sizeof(KT) + 4) + (8 * kRadixBins + 2 * kRadixBins + 8) * 4;
   if (cudaFuncSetAttribute(k_radix_downsweep<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return check_launch("splat_sort (smem attribute)", 0);
@@ -516,8 +530,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
   int32_t* vd = vb;
   const int nbk = (int)p.n_sort_blocks;
   for (int pass = 0; pass < p.passes; ++pass) {
-    const int shift = 8 * pass;
-    const int bits = (p.key_bits - shift) < 8 ? (p.key_bits - shift) : 8;
+    const int shift = kRadixBits * pass;
+    const int bits = (p.key_bits - shift) < kRadixBits ? (p.key_bits - shift) : kRadixBits;
     const uint32_t mask = (1u << bits) - 1u;
     int32_t* vdst = (pass == p.passes - 1) ? gsid_out : vd;
     k_radix_upsweep<KT><<<nbk, kSortThreads, 0, st>>>(ks, p.M, shift, mask, hist, p.n_sort_blocks);

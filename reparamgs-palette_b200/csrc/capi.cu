@@ -75,6 +75,11 @@ using namespace gsb;
 
 GSB_API const char* gsb_last_error(void) { return g_err; }
 GSB_API int gsb_version(void) { return 100; }
+GSB_API int gsb_device_status(uint32_t* status, int clear, void* stream) {
+  GSB_CHECK_ARG(status, "device_status: null pointer");
+  return lowrank_status(status, clear != 0, ST(stream));
+}
+
 GSB_API unsigned long long gsb_launch_count(void) {
   return g_launches.load(std::memory_order_relaxed);
 }
@@ -194,9 +199,9 @@ static int check_image(const char* op, int64_t n, int H, int W, int C) {
   return GSB_OK;
 }
 
-GSB_API size_t gsb_splat_state_bytes(int64_t n, int channels) {
-  if (n < 0 || channels < 1 || channels > GSB_MAX_CHANNELS) return 0;
-  return splat_state_bytes(n, channels);
+GSB_API size_t gsb_splat_state_bytes(int64_t n, int channels, int height, int width) {
+  if (n < 0 || channels < 1 || channels > GSB_MAX_CHANNELS || height < 0 || width < 0) return 0;
+  return splat_state_bytes(n, channels, height, width);
 }
 
 GSB_API int gsb_splat_pack(int64_t n, int height, int width, int channels, const float* us,
@@ -209,43 +214,45 @@ GSB_API int gsb_splat_pack(int64_t n, int height, int width, int channels, const
   GSB_CHECK_ARG(state && ((uintptr_t)state & 255) == 0, "splat_pack: state must be 256-byte aligned");
   GSB_CHECK_ARG(n == 0 || (us && cinv2ds && alphas && feats && depths && areas),
                 "splat_pack: null pointer");
-  const SplatState s = carve_state(state, n, channels);
+  const SplatState s = carve_state(state, n, channels, height, width);
   rc = launch_pack(n, height, width, channels, us, cinv2ds, alphas, feats, feat_dtype, depths,
                    areas, true, s, ST(stream));
   if (rc) return rc;
   return launch_count_scan(n, s, ST(stream));
 }
 
-GSB_API int gsb_splat_counts(int64_t n, const void* state, uint32_t* host_out, void* stream) {
-  GSB_CHECK_ARG(n >= 0 && state && host_out, "splat_counts: bad argument");
-  const SplatState s = carve_state((void*)state, n, 1);
+GSB_API int gsb_splat_counts(int64_t n, int height, int width, const void* state,
+                             gsb_splat_plan* plan, void* stream) {
+  GSB_CHECK_ARG(n >= 0 && height >= 0 && width >= 0 && state && plan,
+                "splat_counts: bad argument");
+  const SplatState s = carve_state((void*)state, n, 1, height, width);
   uint32_t v[4];
   if (cudaMemcpyAsync(v, s.stats, sizeof(v), cudaMemcpyDeviceToHost, ST(stream)) != cudaSuccess ||
       cudaStreamSynchronize(ST(stream)) != cudaSuccess)
     return check_launch("splat_counts", 0);
   GSB_CHECK_ARG(v[3] == 0 && v[0] < (uint32_t)INT32_MAX,
                 "splat_counts: patch count exceeds the int32 index range");
-  host_out[0] = v[0];
-  host_out[1] = v[1];
+  plan->patches = v[0];
+  plan->max_depth_key = v[1];
   return GSB_OK;
 }
 
-GSB_API size_t gsb_splat_sort_bytes(int64_t n, int height, int width, int64_t patches,
-                                    uint32_t max_depth_key) {
-  if (n < 0 || height < 0 || width < 0 || patches < 0) return 0;
-  return make_sort_plan(n, height, width, patches, max_depth_key).bytes_total;
+GSB_API size_t gsb_splat_sort_bytes(int64_t n, int height, int width, const gsb_splat_plan* plan) {
+  if (n < 0 || height < 0 || width < 0 || !plan || plan->patches < 0) return 0;
+  return make_sort_plan(n, height, width, plan->patches, plan->max_depth_key).bytes_total;
 }
 
-GSB_API int gsb_splat_sort(int64_t n, int height, int width, int64_t patches,
-                           uint32_t max_depth_key, const void* state, void* sort_ws,
-                           int32_t* gsid_out, int32_t* ranges_out, void* stream) {
+GSB_API int gsb_splat_sort(int64_t n, int height, int width, const gsb_splat_plan* plan,
+                           const void* state, void* sort_ws, int32_t* gsid_out,
+                           int32_t* ranges_out, void* stream) {
   int rc = check_image("splat_sort", n, height, width, 1);
   if (rc) return rc;
-  GSB_CHECK_ARG(patches >= 0 && patches < (int64_t)INT32_MAX, "splat_sort: bad patch count");
+  GSB_CHECK_ARG(plan && plan->patches >= 0 && plan->patches < (int64_t)INT32_MAX,
+                "splat_sort: bad plan");
   GSB_CHECK_ARG(state && ranges_out, "splat_sort: null pointer");
-  GSB_CHECK_ARG(patches == 0 || (sort_ws && gsid_out), "splat_sort: null workspace/output");
-  const SortPlan p = make_sort_plan(n, height, width, patches, max_depth_key);
-  const SplatState s = carve_state((void*)state, n, 1);
+  GSB_CHECK_ARG(plan->patches == 0 || (sort_ws && gsid_out), "splat_sort: null workspace/output");
+  const SortPlan p = make_sort_plan(n, height, width, plan->patches, plan->max_depth_key);
+  const SplatState s = carve_state((void*)state, n, 1, height, width);
   return launch_sort(p, n, height, width, s, sort_ws, gsid_out, ranges_out, ST(stream));
 }
 
@@ -255,7 +262,7 @@ GSB_API int gsb_splat_draw(int64_t n, int height, int width, int channels, const
   int rc = check_image("splat_draw", n, height, width, channels);
   if (rc) return rc;
   GSB_CHECK_ARG(ranges && state && out && contrib && final_tau, "splat_draw: null pointer");
-  const SplatState s = carve_state((void*)state, n, channels);
+  const SplatState s = carve_state((void*)state, n, channels, height, width);
   return launch_draw(n, height, width, channels, ranges, gsid, s, tau_init, out, contrib,
                      final_tau, ST(stream));
 }
@@ -278,7 +285,7 @@ GSB_API int gsb_splat_backward(int64_t n, int height, int width, int channels, c
                 "splat_backward: pass all of dalphas/dus/dcinv2ds or none");
   GSB_CHECK_ARG(!dloss_dtau || geom, "splat_backward: dloss_dtau needs the geometry outputs");
   GSB_CHECK_ARG(n == 0 || (us && cinv2ds && alphas && feats), "splat_backward: null input");
-  const SplatState s = carve_state(state, n, channels);
+  const SplatState s = carve_state(state, n, channels, height, width);
   rc = launch_pack(n, height, width, channels, us, cinv2ds, alphas, feats, feat_dtype, nullptr,
                    nullptr, false, s, ST(stream));
   if (rc) return rc;
@@ -300,7 +307,7 @@ GSB_API int gsb_splat_backward_packed(int64_t n, int height, int width, int chan
   GSB_CHECK_ARG(!geom || (dalphas && dus && dcinv2ds),
                 "splat_backward_packed: pass all of dalphas/dus/dcinv2ds or none");
   GSB_CHECK_ARG(!dloss_dtau || geom, "splat_backward_packed: dloss_dtau needs the geometry outputs");
-  const SplatState s = carve_state((void*)state, n, channels);
+  const SplatState s = carve_state((void*)state, n, channels, height, width);
   return launch_draw_backward(n, height, width, channels, ranges, gsid, s, contrib, final_tau,
                               dloss_dout, dloss_dtau, dfeats, dalphas, dus, dcinv2ds, ST(stream));
 }

@@ -27,6 +27,7 @@ int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtyp
                                const float* ylm, const float* dw, int K, int P, int Q, int rank,
                                int L, float* dA, float* dB, cudaStream_t st);
 int launch_lab2rgb(int H, int W, const float* lab, float* rgb, cudaStream_t st);
+int lowrank_status(uint32_t* out, bool clear, cudaStream_t st);
 
 // loss.cu
 int launch_palette_l1(int K, int H, int W, const float* layer, const float* palette,
@@ -40,14 +41,16 @@ struct SplatState {
   uint32_t* dkeys;       // [n] uint32(depth * 1000)
   uint32_t* counts;      // [n] patches per Gaussian
   uint32_t* block_sums;  // [n_blocks] -> exclusive block offsets after the scan
-  uint32_t* stats;       // [16]: 0 = M, 1 = max depth key, 2 = device error flags
+  uint32_t* stats;       // [16]: 0/3 = M low/high, 1 = max depth key
   int rec_vec4;          // float4 vectors per record
   int64_t n_blocks;
+  int gx, gy;
 };
-constexpr int kBinBlock = 256;  // Gaussians per binning block
-int record_vec4(int channels);
-size_t splat_state_bytes(int64_t n, int channels);
-SplatState carve_state(void* base, int64_t n, int channels);
+constexpr int kBinBlock = 256;      // Gaussians per binning block
+constexpr int kRadixBits = 9;                  // digit width of one radix pass
+constexpr int kRadixBins = 1 << kRadixBits;int record_vec4(int channels);
+size_t splat_state_bytes(int64_t n, int channels, int H, int W);
+SplatState carve_state(void* base, int64_t n, int channels, int H, int W);
 
 int launch_pack(int64_t n, int H, int W, int channels, const float* us, const float* cinv,
                 const float* alphas, const void* feats, int feat_dtype, float* depths,

@@ -16,57 +16,135 @@
 
 #include "gsb_geometry.cuh"
 #include "gsb_internal.h"
+#include "gsb_stage.cuh"
+#include "gsb_tma.cuh"
 
 namespace gsb {
 
 constexpr int kLrThreads = 128;
 
 // ------------------------------------------------------------- forward
+// Status word of this file's kernels (bit kStatusBulkTimeout: a bulk-copy wait
+// gave up).  Read and cleared through gsb_device_status.
+static __device__ uint32_t g_lowrank_status;
+
+// Shared-memory layout of the fixed-shape kernels: one region per array, the
+// rows of the block's Gaussians back to back (row stride = row length), so a
+// full block's span of every array moves as one 1-D bulk copy.
+template <int K, int P, int Q, int R>
+struct LrSmem {
+  static constexpr int L = P * Q / K;
+  static constexpr int LL = L > 0 ? L : 1;
+  // forward: dc, A, B, pws in; w, ylm out
+  static constexpr int fwd_floats = K + P * R + R * Q + 3 + K + LL;
+  // backward: A, B, ylm, dw in; dA, dB out
+  static constexpr int bwd_floats = P * R + R * Q + LL + K + P * R + R * Q;
+};
+
+// Copies the block's rows of one input array into shared memory: a bulk copy
+// when `bulk` (issued by thread 0, counted on `bar`), else a batched
+// per-thread copy.  Returns the bytes the bulk copy will deliver.
+template <int ROWLEN, typename T>
+__device__ __forceinline__ uint32_t stage_rows(const T* g, int64_t row0, int64_t n, float* s,
+                                               bool bulk, uint64_t* bar) {
+  if (bulk) {
+    const uint32_t bytes = (uint32_t)(blockDim.x * ROWLEN * sizeof(float));
+    if (threadIdx.x == 0) bulk_load(s, g + row0 * ROWLEN, bytes, bar);
+    return bytes;
+  }
+  stage_in_plain<ROWLEN>(g, row0, n, s);
+  return 0;
+}
+
 template <int K, int P, int Q, int R, typename T>
 __global__ void __launch_bounds__(kLrThreads)
     k_lowrank_fixed(int64_t n, const T* __restrict__ dc, const T* __restrict__ A,
                     const T* __restrict__ B, const float* __restrict__ pws,
                     const float* __restrict__ twc, float* __restrict__ w, float* __restrict__ ddc,
                     float* __restrict__ ylm) {
-  constexpr int L = P * Q / K;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float wk[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    wk[k] = SH_C0 * ld(dc, i * K + k);
-    if (ddc) ddc[i * K + k] = SH_C0;
+  using S = LrSmem<K, P, Q, R>;
+  constexpr int L = S::L, PR = P * R, RQ = R * Q;
+  extern __shared__ __align__(16) float sm[];
+  __shared__ __align__(8) uint64_t bar;
+  const int nt = blockDim.x;
+  float* s_dc = sm;
+  float* s_a = s_dc + nt * K;
+  float* s_b = s_a + nt * PR;
+  float* s_p = s_b + nt * RQ;
+  float* s_w = s_p + nt * 3;
+  float* s_y = s_w + nt * K;
+  const int64_t row0 = (int64_t)blockIdx.x * nt;
+  const bool full = row0 + nt <= n;
+  const bool bulk = full && sizeof(T) == 4 && aligned16(dc + row0 * K) &&
+                    aligned16(A + row0 * PR) && aligned16(B + row0 * RQ) &&
+                    aligned16(pws + row0 * 3);
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, (uint32_t)(nt * (K + PR + RQ + 3) * 4));
   }
-  if (L > 0) {
-    float a[P * R], b[R * Q];
+  stage_rows<K>(dc, row0, n, s_dc, bulk, &bar);
+  stage_rows<PR>(A, row0, n, s_a, bulk, &bar);
+  stage_rows<RQ>(B, row0, n, s_b, bulk, &bar);
+  stage_rows<3>(pws, row0, n, s_p, bulk, &bar);
+  __syncthreads();
+  if (bulk && !mbar_wait(&bar, 0)) {
+    if (threadIdx.x == 0) atomicOr(&g_lowrank_status, kStatusBulkTimeout);
+    mbar_wait(&bar, 0);  // bounded second wait for copies still in flight
+    return;
+  }
+  const int t = threadIdx.x;
+  if (row0 + t < n) {
+    float wk[K];
 #pragma unroll
-    for (int j = 0; j < P * R; ++j) a[j] = ld(A, i * (P * R) + j);
+    for (int k = 0; k < K; ++k) wk[k] = SH_C0 * s_dc[t * K + k];
+    if (L > 0) {
+      float a[PR], b[RQ];
 #pragma unroll
-    for (int j = 0; j < R * Q; ++j) b[j] = ld(B, i * (R * Q) + j);
-    float dir[3], Y[16];
-    const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
-    const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
-    view_direction(pw, cam, dir, nullptr, nullptr);
-    sh_basis(dir, L + 1, Y);
-    if (ylm)
+      for (int j = 0; j < PR; ++j) a[j] = s_a[t * PR + j];
 #pragma unroll
-      for (int l = 0; l < L; ++l) ylm[i * L + l] = Y[l + 1];
+      for (int j = 0; j < RQ; ++j) b[j] = s_b[t * RQ + j];
+      float dir[3], Y[16];
+      const float3 pw = make_float3(s_p[t * 3], s_p[t * 3 + 1], s_p[t * 3 + 2]);
+      const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
+      view_direction(pw, cam, dir, nullptr, nullptr);
+      sh_basis(dir, L + 1, Y);
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      float acc = 0.f;
+      for (int l = 0; l < L; ++l) s_y[t * S::LL + l] = Y[l + 1];
 #pragma unroll
-      for (int l = 0; l < L; ++l) {
-        const int g = l * K + k, row = g / Q, col = g % Q;
-        float coef = a[row * R] * b[col];
+      for (int k = 0; k < K; ++k) {
+        float acc = 0.f;
 #pragma unroll
-        for (int r = 1; r < R; ++r) coef += a[row * R + r] * b[r * Q + col];
-        acc += coef * Y[l + 1];
+        for (int l = 0; l < L; ++l) {
+          const int g = l * K + k, row = g / Q, col = g % Q;
+          float coef = a[row * R] * b[col];
+#pragma unroll
+          for (int r = 1; r < R; ++r) coef += a[row * R + r] * b[r * Q + col];
+          acc += coef * Y[l + 1];
+        }
+        wk[k] += acc;
       }
-      wk[k] += acc;
     }
-  }
 #pragma unroll
-  for (int k = 0; k < K; ++k) w[i * K + k] = wk[k];
+    for (int k = 0; k < K; ++k) s_w[t * K + k] = wk[k];
+  }
+  if (ddc) {
+    const int64_t rows = min((int64_t)nt, n - row0);
+    for (int64_t j = t; j < rows * K; j += nt) ddc[row0 * K + j] = SH_C0;
+  }
+  const bool bulk_out = full && aligned16(w + row0 * K) && (L == 0 || !ylm || aligned16(ylm + row0 * L));
+  if (bulk_out) {
+    fence_proxy_async_shared();
+    __syncthreads();
+    if (t == 0) {
+      bulk_store(w + row0 * K, s_w, (uint32_t)(nt * K * 4));
+      if (L > 0 && ylm) bulk_store(ylm + row0 * L, s_y, (uint32_t)(nt * L * 4));
+      bulk_store_drain();
+    }
+  } else {
+    __syncthreads();
+    stage_out_plain<K>(w, row0, n, s_w);
+    if (L > 0 && ylm) stage_out_plain<S::LL>(ylm, row0, n, s_y);
+  }
 }
 
 template <int K, typename T>
@@ -111,45 +189,137 @@ __global__ void __launch_bounds__(kLrThreads)
 
 // ------------------------------------------------------------ backward
 // dA[row][r] += (dw_k B[r][col]) Y_l ;  dB[r][col] += (dw_k A[row][r]) Y_l
+// Rank 1 accumulates in the reference's (k outer, l inner) order.  Higher
+// ranks (no reference counterpart) use dC[p][q] = dw_k Y_l with g = p*Q + q
+// and two register-light sweeps: dA = dC B^T row by row, then dB = A^T dC
+// column by column.
 template <int K, int P, int Q, int R, typename T>
 __global__ void __launch_bounds__(kLrThreads)
     k_lowrank_b_fixed(int64_t n, const T* __restrict__ A, const T* __restrict__ B,
                       const float* __restrict__ ylm, const float* __restrict__ dw,
                       float* __restrict__ dA, float* __restrict__ dB) {
-  constexpr int L = P * Q / K;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float a[P * R], b[R * Q], y[L > 0 ? L : 1], g0[K];
-  float da[P * R], db[R * Q];
-#pragma unroll
-  for (int j = 0; j < P * R; ++j) {
-    a[j] = ld(A, i * (P * R) + j);
-    da[j] = 0.f;
+  using S = LrSmem<K, P, Q, R>;
+  constexpr int L = S::L, LL = S::LL, PR = P * R, RQ = R * Q;
+  extern __shared__ __align__(16) float sm[];
+  __shared__ __align__(8) uint64_t bar;
+  const int nt = blockDim.x;
+  float* s_a = sm;
+  float* s_b = s_a + nt * PR;
+  float* s_y = s_b + nt * RQ;
+  float* s_g = s_y + nt * LL;
+  float* s_da = s_g + nt * K;
+  float* s_db = s_da + nt * PR;
+  const int64_t row0 = (int64_t)blockIdx.x * nt;
+  const bool full = row0 + nt <= n;
+  const bool bulk = full && sizeof(T) == 4 && L > 0 && aligned16(A + row0 * PR) &&
+                    aligned16(B + row0 * RQ) && aligned16(ylm + row0 * L) &&
+                    aligned16(dw + row0 * K);
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, (uint32_t)(nt * (PR + RQ + L + K) * 4));
   }
-#pragma unroll
-  for (int j = 0; j < R * Q; ++j) {
-    b[j] = ld(B, i * (R * Q) + j);
-    db[j] = 0.f;
+  stage_rows<PR>(A, row0, n, s_a, bulk, &bar);
+  stage_rows<RQ>(B, row0, n, s_b, bulk, &bar);
+  if (L > 0) stage_rows<LL>(ylm, row0, n, s_y, bulk, &bar);
+  stage_rows<K>(dw, row0, n, s_g, bulk, &bar);
+  __syncthreads();
+  if (bulk && !mbar_wait(&bar, 0)) {
+    if (threadIdx.x == 0) atomicOr(&g_lowrank_status, kStatusBulkTimeout);
+    mbar_wait(&bar, 0);  // bounded second wait for copies still in flight
+    return;
   }
+  const int t = threadIdx.x;
+  if (row0 + t < n) {
+    float y[LL], g0[K];
 #pragma unroll
-  for (int l = 0; l < L; ++l) y[l] = ylm[i * L + l];
+    for (int l = 0; l < L; ++l) y[l] = s_y[t * LL + l];
 #pragma unroll
-  for (int k = 0; k < K; ++k) g0[k] = dw[i * K + k];
+    for (int k = 0; k < K; ++k) g0[k] = s_g[t * K + k];
+    if constexpr (R == 1) {
+      float a[P], b[Q], da[P], db[Q];
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+      for (int j = 0; j < P; ++j) {
+        a[j] = s_a[t * P + j];
+        da[j] = 0.f;
+      }
 #pragma unroll
-    for (int l = 0; l < L; ++l) {
-      const int g = l * K + k, row = g / Q, col = g % Q;
+      for (int j = 0; j < Q; ++j) {
+        b[j] = s_b[t * Q + j];
+        db[j] = 0.f;
+      }
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        da[row * R + r] = __fadd_rn(da[row * R + r], (g0[k] * b[r * Q + col]) * y[l]);
-        db[r * Q + col] = __fadd_rn(db[r * Q + col], (g0[k] * a[row * R + r]) * y[l]);
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          const int g = l * K + k, row = g / Q, col = g % Q;
+          da[row] = __fadd_rn(da[row], (g0[k] * b[col]) * y[l]);
+          db[col] = __fadd_rn(db[col], (g0[k] * a[row]) * y[l]);
+        }
+#pragma unroll
+      for (int j = 0; j < P; ++j) s_da[t * P + j] = da[j];
+#pragma unroll
+      for (int j = 0; j < Q; ++j) s_db[t * Q + j] = db[j];
+    } else {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {  // dA[p][r] = sum_q dC[p][q] B[r][q]
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0.f;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const int g = p * Q + q;
+          const float c = g0[g % K] * y[g / K];
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] += c * s_b[t * RQ + r * Q + q];
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) s_da[t * PR + p * R + r] = acc[r];
+      }
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {  // dB[r][q] = sum_p dC[p][q] A[p][r]
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0.f;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const int g = p * Q + q;
+          const float c = g0[g % K] * y[g / K];
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] += c * s_a[t * PR + p * R + r];
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) s_db[t * RQ + r * Q + q] = acc[r];
       }
     }
-#pragma unroll
-  for (int j = 0; j < P * R; ++j) dA[i * (P * R) + j] = da[j];
-#pragma unroll
-  for (int j = 0; j < R * Q; ++j) dB[i * (R * Q) + j] = db[j];
+  }
+  const bool bulk_out = full && aligned16(dA + row0 * PR) && aligned16(dB + row0 * RQ);
+  if (bulk_out) {
+    fence_proxy_async_shared();
+    __syncthreads();
+    if (t == 0) {
+      bulk_store(dA + row0 * PR, s_da, (uint32_t)(nt * PR * 4));
+      bulk_store(dB + row0 * RQ, s_db, (uint32_t)(nt * RQ * 4));
+      bulk_store_drain();
+    }
+  } else {
+    __syncthreads();
+    stage_out_plain<PR>(dA, row0, n, s_da);
+    stage_out_plain<RQ>(dB, row0, n, s_db);
+  }
+}
+
+int lowrank_status(uint32_t* out, bool clear, cudaStream_t st) {
+  if (cudaMemcpyFromSymbolAsync(out, g_lowrank_status, sizeof(uint32_t), 0,
+                                cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return check_launch("device_status", 0);
+  if (clear) {
+    const uint32_t zero = 0;
+    if (cudaMemcpyToSymbolAsync(g_lowrank_status, &zero, sizeof(uint32_t), 0,
+                                cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return check_launch("device_status", 0);
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("device_status", 0);
+  return GSB_OK;
 }
 
 // Any valid shape: each thread's dA/dB accumulators in dynamic shared memory.
@@ -191,11 +361,16 @@ static bool lowrank_fixed(int64_t n, const void* dc, const void* A, const void* 
                           float* ylm, cudaStream_t st) {
   const int g = grid_lr(n, kLrThreads);
   const T *d = (const T*)dc, *a = (const T*)A, *b = (const T*)B;
-#define GSB_LR(KK, PP, QQ, RR)                                                          \
-  if (K == KK && P == PP && Q == QQ && rank == RR) {                                    \
-    k_lowrank_fixed<KK, PP, QQ, RR, T><<<g, kLrThreads, 0, st>>>(n, d, a, b, pws, twc, w, \
-                                                                 ddc, ylm);            \
-    return true;                                                                        \
+#define GSB_LR(KK, PP, QQ, RR)                                                              \
+  if (K == KK && P == PP && Q == QQ && rank == RR) {                                        \
+    const int sm = LrSmem<KK, PP, QQ, RR>::fwd_floats * kLrThreads * 4;                     \
+    auto kern = k_lowrank_fixed<KK, PP, QQ, RR, T>;                                         \
+    static bool attr_set = false; /* once per process; set before first launch */          \
+    if (sm > 48 * 1024 && !attr_set)                                                        \
+      attr_set = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                      sm) == cudaSuccess;                                   \
+    kern<<<g, kLrThreads, sm, st>>>(n, d, a, b, pws, twc, w, ddc, ylm);                     \
+    return true;                                                                            \
   }
   GSB_LR(5, 5, 15, 1) GSB_LR(5, 5, 15, 2) GSB_LR(5, 5, 15, 3) GSB_LR(5, 5, 15, 4)
   GSB_LR(3, 3, 15, 1) GSB_LR(4, 4, 15, 1) GSB_LR(6, 6, 15, 1) GSB_LR(7, 7, 15, 1)
@@ -240,10 +415,16 @@ static int lowrank_b_t(int64_t n, const void* A, const void* B, const float* ylm
                        cudaStream_t st) {
   const T *a = (const T*)A, *b = (const T*)B;
   const int g = grid_lr(n, kLrThreads);
-#define GSB_LRB(KK, PP, QQ, RR)                                                               \
-  if (K == KK && P == PP && Q == QQ && rank == RR) {                                          \
-    k_lowrank_b_fixed<KK, PP, QQ, RR, T><<<g, kLrThreads, 0, st>>>(n, a, b, ylm, dw, dA, dB); \
-    return check_launch("sh2Weight_fast_B");                                                  \
+#define GSB_LRB(KK, PP, QQ, RR)                                                              \
+  if (K == KK && P == PP && Q == QQ && rank == RR) {                                         \
+    const int sm = LrSmem<KK, PP, QQ, RR>::bwd_floats * kLrThreads * 4;                      \
+    auto kern = k_lowrank_b_fixed<KK, PP, QQ, RR, T>;                                        \
+    static bool attr_set = false; /* once per process; set before first launch */           \
+    if (sm > 48 * 1024 && !attr_set)                                                         \
+      attr_set = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                      sm) == cudaSuccess;                                    \
+    kern<<<g, kLrThreads, sm, st>>>(n, a, b, ylm, dw, dA, dB);                               \
+    return check_launch("sh2Weight_fast_B");                                                 \
   }
   GSB_LRB(5, 5, 15, 1) GSB_LRB(5, 5, 15, 2) GSB_LRB(5, 5, 15, 3) GSB_LRB(5, 5, 15, 4)
   GSB_LRB(3, 3, 15, 1) GSB_LRB(4, 4, 15, 1) GSB_LRB(6, 6, 15, 1) GSB_LRB(7, 7, 15, 1)

@@ -124,19 +124,51 @@ __global__ void __launch_bounds__(kDrawThreads, 4)
 }
 
 // ------------------------------------------------------------- adjoint
-__device__ __forceinline__ float warp_sum(float v) {
+// Sum of NV per-lane values over the warp with NV-1 + 5-log2(NV) shuffles:
+// each exchange step halves the values a lane carries (lanes with the step's
+// bit set keep the upper half), so the totals end up spread over the lanes.
+// Returns this lane's total; *idx is the value index it holds and *owner is
+// set on exactly one lane per index.
+template <int NV>
+__device__ __forceinline__ float warp_transpose_sum(float (&x)[NV], int lane, int* idx,
+                                                    bool* owner) {
+  static_assert(NV >= 1 && NV <= 16 && (NV & (NV - 1)) == 0, "NV must be a power of two <= 16");
+  int id = 0;
+  int off = 16;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int w = NV / 2; w >= 1; w >>= 1, off >>= 1) {
+    const bool hi = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < w; ++i) {
+      const float send = hi ? x[i] : x[i + w];
+      const float keep = hi ? x[i + w] : x[i];
+      x[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+    id += hi ? w : 0;
+  }
+  float v = x[0];
+#pragma unroll
+  for (int o = off; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  *idx = id;
+  *owner = (lane & (2 * off - 1)) == 0;
   return v;
 }
 
+template <int NV>
+struct Pow2 {
+  static constexpr int value = NV <= 1 ? 1 : NV <= 2 ? 2 : NV <= 4 ? 4 : NV <= 8 ? 8 : NV <= 16 ? 16 : 32;
+};
+
 // Walks each pixel's contributors back to front from its `contrib` index,
-// recovering T by division by (1 - alpha') from the saved final T.  Per
-// Gaussian the warp's contributions are summed with shuffles and added once.
-// GEOM adds the opacity / centre / conic adjoint (draw_color_B's terms, for
-// any channel count); DTAU adds dL/dT_final (vanilla_3dgs/gsplatcu/
-// kernel.cu:912-919).  As in the reference, the 0.99 clamp and max(0, .) are
-// not differentiated.
+// recovering T by division by (1 - alpha') from the saved final T.  The
+// per-pixel skip decisions use the forward's exact expressions, so the walk
+// visits exactly the Gaussians the forward blended; T itself is recovered
+// with a fast reciprocal division (relative error ~1e-7 per step).  Per
+// Gaussian the warp's contributions are summed with one transposed reduction
+// and added with one atomic per value.  GEOM adds the opacity / centre / conic
+// adjoint (draw_color_B's terms, for any channel count); DTAU adds
+// dL/dT_final (vanilla_3dgs/gsplatcu/kernel.cu:912-919).  As in the
+// reference, the 0.99 clamp and max(0, .) are not differentiated.
 template <int K, bool GEOM, bool DTAU>
 __global__ void __launch_bounds__(kDrawThreads, 3)
     k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
@@ -146,6 +178,8 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
                     float* __restrict__ dfeat, float* __restrict__ dalpha,
                     float* __restrict__ du, float* __restrict__ dconic) {
   constexpr int V = RecordLayout<K>::kVec4;
+  constexpr int NREAL = GEOM ? K + 6 : K;
+  constexpr int NV = Pow2<NREAL>::value;
   __shared__ float4 srec[V * kBatch];
   __shared__ int32_t sgid[kBatch];
   __shared__ unsigned s_maxc;
@@ -192,10 +226,9 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
         const int jj = s_lo + msb;
         const int p = base + jj;
         bool hit = false;
-        float gk[K];
+        float x[NV];
 #pragma unroll
-        for (int k = 0; k < K; ++k) gk[k] = 0.f;
-        float ga = 0.f, gux = 0.f, guy = 0.f, gqa = 0.f, gqb = 0.f, gqc = 0.f;
+        for (int v = 0; v < NV; ++v) x[v] = 0.f;
         if (p < cont) {
           const float4 v1 = srec[kBatch + jj];
           const float4 v2 = srec[2 * kBatch + jj];
@@ -206,10 +239,11 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
             const float ap = fminf(kAlphaMax, v2.z * g);
             if (!(ap < kAlphaMin)) {
               hit = true;
-              T /= (1.f - ap);
+              const float one_m = 1.f - ap;
+              T = __fdividef(T, one_m);
               const float wgt = ap * T;
 #pragma unroll
-              for (int k = 0; k < K; ++k) gk[k] = dl[k] * wgt;
+              for (int k = 0; k < K; ++k) x[k] = dl[k] * wgt;
               if (GEOM) {
                 float f[K];
                 load_feats<K>(srec, jj, v2.w, f);
@@ -217,58 +251,51 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                   dap += dl[k] * (T * (f[k] - G[k]));
-                  G[k] = ap * f[k] + (1.f - ap) * G[k];
+                  G[k] = ap * f[k] + one_m * G[k];
                 }
-                if (DTAU) dap += dTf * (-Tf / (1.f - ap));
-                ga = dap * g;
-                gux = dap * ((-v1.z * dx - v1.w * dy) * ap);
-                guy = dap * ((-v1.w * dx - v2.x * dy) * ap);
-                gqa = dap * (-0.5f * ap * (dx * dx));
-                gqb = dap * (-1.0f * ap * (dx * dy));
-                gqc = dap * (-0.5f * ap * (dy * dy));
+                if (DTAU) dap += dTf * __fdividef(-Tf, one_m);
+                x[K] = dap * g;                                    // alpha
+                x[K + 1] = dap * ((-v1.z * dx - v1.w * dy) * ap);  // u.x
+                x[K + 2] = dap * ((-v1.w * dx - v2.x * dy) * ap);  // u.y
+                x[K + 3] = dap * (-0.5f * ap * (dx * dx));         // conic a
+                x[K + 4] = dap * (-1.0f * ap * (dx * dy));         // conic b
+                x[K + 5] = dap * (-0.5f * ap * (dy * dy));         // conic c
               }
             }
           }
         }
         const unsigned cm = __ballot_sync(0xffffffffu, hit);
         if (!cm) continue;
-        const int g = sgid[jj];
+        const int64_t g = sgid[jj];
         if (__popc(cm) == 1) {
           if (hit) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) atomicAdd(dfeat + (int64_t)g * K + k, gk[k]);
+            for (int k = 0; k < K; ++k) atomicAdd(dfeat + g * K + k, x[k]);
             if (GEOM) {
-              atomicAdd(dalpha + g, ga);
-              atomicAdd(du + 2 * (int64_t)g, gux);
-              atomicAdd(du + 2 * (int64_t)g + 1, guy);
-              atomicAdd(dconic + 3 * (int64_t)g, gqa);
-              atomicAdd(dconic + 3 * (int64_t)g + 1, gqb);
-              atomicAdd(dconic + 3 * (int64_t)g + 2, gqc);
+              atomicAdd(dalpha + g, x[K]);
+              atomicAdd(du + 2 * g, x[K + 1]);
+              atomicAdd(du + 2 * g + 1, x[K + 2]);
+              atomicAdd(dconic + 3 * g, x[K + 3]);
+              atomicAdd(dconic + 3 * g + 1, x[K + 4]);
+              atomicAdd(dconic + 3 * g + 2, x[K + 5]);
             }
           }
-        } else {
-#pragma unroll
-          for (int k = 0; k < K; ++k) gk[k] = warp_sum(gk[k]);
-          if (GEOM) {
-            ga = warp_sum(ga);
-            gux = warp_sum(gux);
-            guy = warp_sum(guy);
-            gqa = warp_sum(gqa);
-            gqb = warp_sum(gqb);
-            gqc = warp_sum(gqc);
-          }
-          if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) atomicAdd(dfeat + (int64_t)g * K + k, gk[k]);
-            if (GEOM) {
-              atomicAdd(dalpha + g, ga);
-              atomicAdd(du + 2 * (int64_t)g, gux);
-              atomicAdd(du + 2 * (int64_t)g + 1, guy);
-              atomicAdd(dconic + 3 * (int64_t)g, gqa);
-              atomicAdd(dconic + 3 * (int64_t)g + 1, gqb);
-              atomicAdd(dconic + 3 * (int64_t)g + 2, gqc);
-            }
-          }
+          continue;
+        }
+        int idx;
+        bool owner;
+        const float tot = warp_transpose_sum<NV>(x, lane, &idx, &owner);
+        if (owner && idx < NREAL) {
+          float* dst;
+          if (idx < K)
+            dst = dfeat + g * K + idx;
+          else if (idx == K)
+            dst = dalpha + g;
+          else if (idx < K + 3)
+            dst = du + 2 * g + (idx - K - 1);
+          else
+            dst = dconic + 3 * g + (idx - K - 3);
+          atomicAdd(dst, tot);
         }
       }
     }

@@ -245,20 +245,24 @@ def _splat_forward(op, H, W, C_, us, cinv2ds, alphas, depths, feats, areas, tau_
     L = _lib.lib()
     with torch.cuda.device(dev):
         st = stream_of(us)
-        state = torch.empty(int(L.gsb_splat_state_bytes(n, C_)), dtype=torch.uint8, device=dev)
+        state = torch.empty(int(L.gsb_splat_state_bytes(n, C_, H, W)), dtype=torch.uint8,
+                            device=dev)
         call(op, "gsb_splat_pack", n, H, W, C_, ptr(us), ptr(cinv), ptr(alphas), ptr(feats),
              _sh_dtype(feats), ptr(depths), ptr(areas), ptr(state), st)
-        host = (C.c_uint32 * 2)()
-        call(op, "gsb_splat_counts", n, ptr(state), host, st)
-        M, maxdk = int(host[0]), int(host[1])
-        ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, M, maxdk))), dtype=torch.uint8,
-                         device=dev)
-        gsid = torch.empty((M,), dtype=torch.int32, device=dev)
+        # outputs that do not depend on the patch count are allocated while the
+        # device is still packing
         ranges = torch.empty((gx * gy, 2), dtype=torch.int32, device=dev)
-        call(op, "gsb_splat_sort", n, H, W, M, maxdk, ptr(state), ptr(ws), ptr(gsid), ptr(ranges), st)
         out = torch.empty((C_, H, W), dtype=_F32, device=dev)
         contrib = torch.empty((H, W), dtype=torch.int32, device=dev)
         final_tau = torch.empty((H, W), dtype=_F32, device=dev)
+        plan = _lib.SplatPlan()
+        call(op, "gsb_splat_counts", n, H, W, ptr(state), C.byref(plan), st)
+        M = int(plan.patches)
+        ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan)))),
+                         dtype=torch.uint8, device=dev)
+        gsid = torch.empty((M,), dtype=torch.int32, device=dev)
+        call(op, "gsb_splat_sort", n, H, W, C.byref(plan), ptr(state), ptr(ws), ptr(gsid),
+             ptr(ranges), st)
         call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(gsid), ptr(state), float(tau_init),
              ptr(out), ptr(contrib), ptr(final_tau), st)
     return [out, contrib, final_tau, ranges, gsid]
@@ -300,8 +304,8 @@ def _splat_backward(op, H, W, C_, us, cinv2ds, alphas, feats, contrib, final_tau
     du = torch.zeros((n, 1, 2), dtype=_F32, device=dev) if geom else None
     dq = torch.zeros((n, 1, 3), dtype=_F32, device=dev) if geom else None
     with torch.cuda.device(dev):
-        state = torch.empty(int(_lib.lib().gsb_splat_state_bytes(n, C_)), dtype=torch.uint8,
-                            device=dev)
+        state = torch.empty(int(_lib.lib().gsb_splat_state_bytes(n, C_, H, W)),
+                            dtype=torch.uint8, device=dev)
         call(op, "gsb_splat_backward", n, H, W, C_, ptr(us), ptr(cinv), ptr(alphas), ptr(feats),
              _sh_dtype(feats), ptr(ranges), ptr(gsid), ptr(contrib), ptr(final_tau), ptr(dloss),
              ptr(dtau), ptr(state), ptr(dfeat), ptr(dalpha), ptr(du), ptr(dq), stream_of(us))

@@ -29,6 +29,7 @@ _SIGS = {
     "gsb_last_error": (C.c_char_p, []),
     "gsb_version": (_i32, []),
     "gsb_launch_count": (C.c_ulonglong, []),
+    "gsb_device_status": (_i32, [_p, _i32, _p]),
     "gsb_project": (_i32, [_i64, _p, _p, _p, _f32, _f32, _f32, _f32, _p, _p, _p, _p, _p]),
     "gsb_compute_cov3d": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_compute_cov2d": (_i32, [_i64, _p, _p, _p, _p, _f32, _f32, _f32, _f32, _p, _p, _p, _p]),
@@ -40,11 +41,11 @@ _SIGS = {
                                            _p, _p, _p]),
     "gsb_sh2color": (_i32, [_i64, _p, _i32, _i32, _p, _p, _p, _p, _p, _p]),
     "gsb_lab2rgb": (_i32, [_i32, _i32, _p, _p, _p]),
-    "gsb_splat_state_bytes": (_sz, [_i64, _i32]),
+    "gsb_splat_state_bytes": (_sz, [_i64, _i32, _i32, _i32]),
     "gsb_splat_pack": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _i32, _p, _p, _p, _p]),
-    "gsb_splat_counts": (_i32, [_i64, _p, _p, _p]),
-    "gsb_splat_sort_bytes": (_sz, [_i64, _i32, _i32, _i64, _u32]),
-    "gsb_splat_sort": (_i32, [_i64, _i32, _i32, _i64, _u32, _p, _p, _p, _p, _p]),
+    "gsb_splat_counts": (_i32, [_i64, _i32, _i32, _p, _p, _p]),
+    "gsb_splat_sort_bytes": (_sz, [_i64, _i32, _i32, _p]),
+    "gsb_splat_sort": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p, _p]),
     "gsb_splat_draw": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _f32, _p, _p, _p, _p]),
     "gsb_splat_backward": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _i32, _p, _p, _p, _p,
                                   _p, _p, _p, _p, _p, _p, _p, _p]),
@@ -54,6 +55,12 @@ _SIGS = {
 }
 
 _lib = None
+
+
+class SplatPlan(C.Structure):
+    """gsb_splat_plan: sizes gsb_splat_counts reads back for the sort step."""
+    _fields_ = [("patches", C.c_int64), ("max_depth_key", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class GsplatError(RuntimeError):

@@ -53,17 +53,20 @@ def test_argument_errors_need_no_gpu():
     assert b"1, 4, 9 or 16" in L.gsb_last_error()
     rc = L.gsb_sh2weight_fast(10, None, None, None, 0, 5, 4, 15, 1, None, None, None, None, None, None)
     assert rc == _lib.GSB_ERR_INVALID_ARGUMENT
-    assert L.gsb_splat_state_bytes(-1, 5) == 0
-    assert L.gsb_splat_state_bytes(1000, 9) == 0
+    assert L.gsb_splat_state_bytes(-1, 5, 64, 64) == 0
+    assert L.gsb_splat_state_bytes(1000, 9, 64, 64) == 0
 
 
 def test_workspace_sizes_grow_with_problem():
     from gsplatcu import _lib
     L = _lib.lib()
-    a = L.gsb_splat_state_bytes(1000, 5)
-    b = L.gsb_splat_state_bytes(100000, 5)
+    import ctypes
+    a = L.gsb_splat_state_bytes(1000, 5, 1080, 1920)
+    b = L.gsb_splat_state_bytes(100000, 5, 1080, 1920)
     assert 0 < a < b
     assert b >= 100000 * (8 + 4 + 4 + 64)
-    s1 = L.gsb_splat_sort_bytes(1000, 1080, 1920, 50000, 20000)
-    s2 = L.gsb_splat_sort_bytes(1000, 1080, 1920, 50000, 1 << 25)  # > 32 key bits -> 64-bit keys
+    plan = _lib.SplatPlan(50000, 20000, 0)
+    s1 = L.gsb_splat_sort_bytes(1000, 1080, 1920, ctypes.byref(plan))
+    plan = _lib.SplatPlan(50000, 1 << 25, 0)  # > 32 key bits -> 64-bit radix keys
+    s2 = L.gsb_splat_sort_bytes(1000, 1080, 1920, ctypes.byref(plan))
     assert s2 > s1 > 50000 * 16

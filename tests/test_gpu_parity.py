@@ -294,3 +294,30 @@ def test_weight_function_sequence_end_to_end(cuda_ok):
     o = orc.render_weights(sc["pws"], sc["rots"], sc["scales"], sc["alphas"], o_w, cam)
     assert np.mean(np_of(r["gsid"]) == o["gsid"]) > 0.999 if len(o["gsid"]) == r["gsid"].numel() else True
     assert np.mean(np.abs(np_of(r["layer"]) - o["layer"])) < 1e-6
+
+
+@pytest.mark.parametrize("crowd", [300, 5000, 17000])
+def test_sort_long_lists_and_ties_bitexact(cuda_ok, crowd):
+    """Crowded tiles (up to 17k patches) and many equal depth keys: the sort
+    gives the reference's order (ties by Gaussian id)."""
+    rng = np.random.default_rng(crowd)
+    n = 3000 + crowd
+    us = np.concatenate([rng.uniform(0, 200, (3000, 2)), 40 + rng.uniform(-1, 1, (crowd, 2))])
+    areas = np.concatenate([rng.integers(1, 30, (3000, 2)), np.full((crowd, 2), 3)]).astype(np.int32)
+    depths = rng.uniform(0.1, 30.0, n).astype(np.float32)
+    depths[::7] = depths[3]  # many equal depth keys: ties ordered by id
+    cinv = np.tile(np.array([[0.3, 0.01, 0.2]], np.float32), (n, 1))
+    al = rng.uniform(0.01, 0.9, (n, 1)).astype(np.float32)
+    w = rng.uniform(0, 1, (n, 5)).astype(np.float32)
+    H, W = 120, 200
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=a.dtype)).cuda()
+    d_g, a_g = t(depths.copy()), t(areas.copy())
+    layer, contrib, ft, ranges, gsid = gsc.splat_weight(H, W, 5, t(us.astype(np.float32)), t(cinv),
+                                                        t(al), d_g, t(w), a_g)
+    dd, aa = depths.copy(), areas.copy()
+    b = orc.bin_gaussians(us.astype(np.float32), aa, dd, H, W)
+    assert np.array_equal(np_of(gsid), b["gsid"])
+    assert np.array_equal(np_of(ranges), b["ranges"])
+    assert np.array_equal(np_of(d_g), dd) and np.array_equal(np_of(a_g), aa)
+    counts = b["ranges"][:, 1] - b["ranges"][:, 0]
+    assert counts.max() >= crowd
