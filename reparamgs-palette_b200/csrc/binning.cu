@@ -284,8 +284,8 @@ __global__ void __launch_bounds__(kBinBlock)
 
 // ------------------------------------------------------------ radix sort
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per block
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
 
 template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
@@ -328,7 +328,8 @@ __global__ void __launch_bounds__(256)
 }
 
 // Stable scatter of one digit pass.  Items of a block are ranked in their
-// original order (warp w owns items [512w, 512w+512), lane-minor), staged in
+// original order (warp w owns items [32 kSortItems w, 32 kSortItems (w+1)),
+// lane-minor), staged in
 // shared memory in digit order and written out in digit-contiguous runs.
 // Thread t owns digits 2t and 2t+1 in the per-digit phases.
 template <typename KT>

@@ -2,13 +2,17 @@
 // 194-372) and its reverse-order adjoint (draw_weight_B / draw_color_B,
 // gsplatcu/kernel.cu:1176-1379).
 //
-// One 256-thread CTA per 16x16 tile.  Each warp owns an 8x4 block of pixels.
-// The tile's Gaussian list is staged through shared memory in batches of 256
-// packed records; within a batch every warp first tests 32 records at a time
-// against its pixel block (one record per lane, ballot) using the record's
-// conservative support box, then walks only the overlapping records in list
-// order.  Per pixel, a record whose Mahalanobis distance exceeds its cut is
-// skipped without evaluating exp() -- the reference would skip it too
+// One CTA per 16x16 tile.  In the forward each of the 8 warps owns an 8x4
+// block of pixels, one per lane.  In the adjoint each of the 4 warps owns an
+// 8x8 block and each lane two pixels of one column, four rows apart, so the
+// per-Gaussian loop control and the warp reduction of the gradient terms are
+// shared by 64 pixels.  The tile's Gaussian
+// list is staged through shared memory in batches of 256 packed records;
+// within a batch every warp first tests 32 records at a time against its
+// pixel block (one record per lane, ballot) using the record's conservative
+// support box, then walks only the overlapping records in list order.  Per
+// pixel, a record whose Mahalanobis distance exceeds its cut is skipped
+// without evaluating exp() -- the reference would skip it too
 // (alpha' < 0.002) -- and every other record is evaluated with the
 // reference's own FP32 expressions, so skip/stop decisions, contributor
 // indices and blended values agree with it.
@@ -18,9 +22,29 @@
 namespace gsb {
 
 constexpr int kBatch = 256;
-constexpr int kDrawThreads = 256;
+constexpr int kDrawFwdThreads = 256;  // forward: one pixel per thread, 8x4 pixels per warp
+constexpr int kDrawThreads = 128;     // adjoint: two pixels per thread, 8x8 pixels per warp
 
-__device__ __forceinline__ void pixel_of(int tile, int gx, int& wx, int& wy, int& px, int& py) {
+struct PixelPair {
+  int wx, wy;    // warp block origin (8x8)
+  int px;        // column
+  int py0, py1;  // rows (py1 = py0 + 4)
+};
+
+__device__ __forceinline__ PixelPair pixels_of(int tile, int gx) {
+  const int tx = tile % gx, ty = tile / gx;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  PixelPair p;
+  p.wx = tx * kTile + (w & 1) * 8;
+  p.wy = ty * kTile + (w >> 1) * 8;
+  p.px = p.wx + (lane & 7);
+  p.py0 = p.wy + (lane >> 3);
+  p.py1 = p.py0 + 4;
+  return p;
+}
+
+__device__ __forceinline__ void pixel_of_1px(int tile, int gx, int& wx, int& wy, int& px,
+                                             int& py) {
   const int tx = tile % gx, ty = tile / gx;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   wx = tx * kTile + (w & 1) * 8;
@@ -32,22 +56,22 @@ __device__ __forceinline__ void pixel_of(int tile, int gx, int& wx, int& wy, int
 // Stage records [first, first+cnt) of the tile list into shared memory,
 // vector-major (srec[v * kBatch + slot]) so that per-slot broadcasts and the
 // lane-per-slot box test are both conflict-free.
-template <int V>
+template <int V, int NT>
 __device__ __forceinline__ void stage_batch(const int32_t* __restrict__ gsid, int first, int cnt,
                                             const float4* __restrict__ records, float4* srec,
                                             int32_t* sgid) {
-  if ((int)threadIdx.x < cnt) {
-    const int g = gsid[first + threadIdx.x];
+  for (int t = threadIdx.x; t < cnt; t += NT) {
+    const int g = gsid[first + t];
     const float4* src = records + (int64_t)g * V;
 #pragma unroll
-    for (int v = 0; v < V; ++v) srec[v * kBatch + threadIdx.x] = __ldg(src + v);
-    if (sgid) sgid[threadIdx.x] = g;
+    for (int v = 0; v < V; ++v) srec[v * kBatch + t] = __ldg(src + v);
+    if (sgid) sgid[t] = g;
   }
 }
 
-__device__ __forceinline__ bool box_overlaps(float4 box, int wx, int wy) {
-  return box.y >= (float)wx && box.x <= (float)(wx + 7) && box.w >= (float)wy &&
-         box.z <= (float)(wy + 3);
+__device__ __forceinline__ bool box_overlaps_rect(float4 box, int wx, int wy, int ex, int ey) {
+  return box.y >= (float)wx && box.x <= (float)(wx + ex) && box.w >= (float)wy &&
+         box.z <= (float)(wy + ey);
 }
 
 template <int K>
@@ -63,14 +87,14 @@ __device__ __forceinline__ void load_feats(const float4* srec, int j, float v2w,
 
 // ------------------------------------------------------------- forward
 template <int K>
-__global__ void __launch_bounds__(kDrawThreads, 4)
+__global__ void __launch_bounds__(kDrawFwdThreads, 4)
     k_draw(int H, int W, int gx, const int2* __restrict__ ranges, const int32_t* __restrict__ gsid,
            const float4* __restrict__ records, float tau_init, float* __restrict__ out,
            int32_t* __restrict__ contrib, float* __restrict__ final_tau) {
   constexpr int V = RecordLayout<K>::kVec4;
   __shared__ float4 srec[V * kBatch];
   int wx, wy, px, py;
-  pixel_of(blockIdx.x, gx, wx, wy, px, py);
+  pixel_of_1px(blockIdx.x, gx, wx, wy, px, py);
   const bool inside = px < W && py < H;
   const int2 rg = ranges[blockIdx.x];
   const int n = rg.y - rg.x;
@@ -83,12 +107,12 @@ __global__ void __launch_bounds__(kDrawThreads, 4)
   for (int base = 0; base < n; base += kBatch) {
     const int cnt = min(kBatch, n - base);
     __syncthreads();
-    stage_batch<V>(gsid, rg.x + base, cnt, records, srec, nullptr);
+    stage_batch<V, kDrawFwdThreads>(gsid, rg.x + base, cnt, records, srec, nullptr);
     __syncthreads();
     if (!__all_sync(0xffffffffu, done)) {
       for (int s = 0; s < cnt; s += 32) {
         const int j = s + (threadIdx.x & 31);
-        const bool ov = j < cnt && box_overlaps(srec[j], wx, wy);
+        const bool ov = j < cnt && box_overlaps_rect(srec[j], wx, wy, 7, 3);
         unsigned mask = __ballot_sync(0xffffffffu, ov);
         while (mask) {
           const int jj = s + __ffs(mask) - 1;
@@ -159,18 +183,62 @@ struct Pow2 {
   static constexpr int value = NV <= 1 ? 1 : NV <= 2 ? 2 : NV <= 4 ? 4 : NV <= 8 ? 8 : NV <= 16 ? 16 : 32;
 };
 
+// Per-pixel back-to-front state of the adjoint.
+template <int K>
+struct BwdPixel {
+  float dl[K], G[K];
+  float T, Tf, dTf;
+  int cont;
+};
+
+// One contributor of one pixel in the adjoint: recovers T, accumulates the
+// pixel's gradient terms into x (x[0..K) features, then alpha, u, conic).
+template <int K, bool GEOM, bool DTAU>
+__device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, float4 v1,
+                                              float4 v2, float dx, float dy, const float4* srec,
+                                              int jj, float* x) {
+  if (!(idx < p.cont) || m > v2.y) return false;
+  const float g = expf(-0.5f * m);
+  const float ap = fminf(kAlphaMax, v2.z * g);
+  if (ap < kAlphaMin) return false;
+  const float one_m = 1.f - ap;
+  p.T = __fdividef(p.T, one_m);
+  const float wgt = ap * p.T;
+#pragma unroll
+  for (int k = 0; k < K; ++k) x[k] += p.dl[k] * wgt;
+  if (GEOM) {
+    float f[K];
+    load_feats<K>(srec, jj, v2.w, f);
+    float dap = 0.f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      dap += p.dl[k] * (p.T * (f[k] - p.G[k]));
+      p.G[k] = ap * f[k] + one_m * p.G[k];
+    }
+    if (DTAU) dap += p.dTf * __fdividef(-p.Tf, one_m);
+    x[K] += dap * g;                                    // alpha
+    x[K + 1] += dap * ((-v1.z * dx - v1.w * dy) * ap);  // u.x
+    x[K + 2] += dap * ((-v1.w * dx - v2.x * dy) * ap);  // u.y
+    x[K + 3] += dap * (-0.5f * ap * (dx * dx));         // conic a
+    x[K + 4] += dap * (-1.0f * ap * (dx * dy));         // conic b
+    x[K + 5] += dap * (-0.5f * ap * (dy * dy));         // conic c
+  }
+  return true;
+}
+
 // Walks each pixel's contributors back to front from its `contrib` index,
 // recovering T by division by (1 - alpha') from the saved final T.  The
 // per-pixel skip decisions use the forward's exact expressions, so the walk
 // visits exactly the Gaussians the forward blended; T itself is recovered
 // with a fast reciprocal division (relative error ~1e-7 per step).  Per
-// Gaussian the warp's contributions are summed with one transposed reduction
-// and added with one atomic per value.  GEOM adds the opacity / centre / conic
-// adjoint (draw_color_B's terms, for any channel count); DTAU adds
-// dL/dT_final (vanilla_3dgs/gsplatcu/kernel.cu:912-919).  As in the
-// reference, the 0.99 clamp and max(0, .) are not differentiated.
+// Gaussian each lane first adds its two pixels' terms, then the warp's 64
+// pixels are summed with one transposed reduction and added with one atomic
+// per value.  GEOM adds the opacity / centre / conic adjoint (draw_color_B's
+// terms, for any channel count); DTAU adds dL/dT_final
+// (vanilla_3dgs/gsplatcu/kernel.cu:912-919).  As in the reference, the 0.99
+// clamp and max(0, .) are not differentiated.
 template <int K, bool GEOM, bool DTAU>
-__global__ void __launch_bounds__(kDrawThreads, 3)
+__global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 6)
     k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
                     const int32_t* __restrict__ gsid, const float4* __restrict__ records,
                     const int32_t* __restrict__ contrib, const float* __restrict__ final_tau,
@@ -183,24 +251,28 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
   __shared__ float4 srec[V * kBatch];
   __shared__ int32_t sgid[kBatch];
   __shared__ unsigned s_maxc;
-  int wx, wy, px, py;
-  pixel_of(blockIdx.x, gx, wx, wy, px, py);
+  const PixelPair pp = pixels_of(blockIdx.x, gx);
   const int lane = threadIdx.x & 31;
-  const bool inside = px < W && py < H;
   const int2 rg = ranges[blockIdx.x];
   if (rg.y - rg.x == 0) return;  // uniform per block
-  const int64_t pix = (int64_t)py * W + px, hw = (int64_t)H * W;
-  float dl[K], G[K];
+  const int64_t hw = (int64_t)H * W;
+  BwdPixel<K> p[2];
+  const int rows[2] = {pp.py0, pp.py1};
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    dl[k] = inside ? dout[k * hw + pix] : 0.f;
-    G[k] = 0.f;
+  for (int q = 0; q < 2; ++q) {
+    const bool in = pp.px < W && rows[q] < H;
+    const int64_t pix = (int64_t)rows[q] * W + pp.px;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      p[q].dl[k] = in ? dout[k * hw + pix] : 0.f;
+      p[q].G[k] = 0.f;
+    }
+    p[q].Tf = in ? final_tau[pix] : 0.f;
+    p[q].T = p[q].Tf;
+    p[q].dTf = (DTAU && in) ? dtau[pix] : 0.f;
+    p[q].cont = in ? contrib[pix] : 0;
   }
-  const float Tf = inside ? final_tau[pix] : 0.f;
-  const float dTf = (DTAU && inside) ? dtau[pix] : 0.f;
-  const int cont = inside ? contrib[pix] : 0;
-  float T = Tf;
-  const int wmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)cont);
+  const int wmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(p[0].cont, p[1].cont));
   if (threadIdx.x == 0) s_maxc = 0u;
   __syncthreads();
   if (lane == 0) atomicMax(&s_maxc, (unsigned)wmax);
@@ -208,62 +280,34 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
   // contributor indices never exceed the tile's list (clamped for safety
   // against mismatched inputs)
   const int maxc = min((int)s_maxc, rg.y - rg.x);
+  const float fx = (float)pp.px, fy0 = (float)pp.py0, fy1 = (float)pp.py1;
   for (int top = maxc; top > 0; top -= kBatch) {
     const int base = max(0, top - kBatch);
     const int cnt = top - base;
     __syncthreads();
-    stage_batch<V>(gsid, rg.x + base, cnt, records, srec, sgid);
+    stage_batch<V, kDrawThreads>(gsid, rg.x + base, cnt, records, srec, sgid);
     __syncthreads();
     const int hi = min(cnt, wmax - base);
     for (int s_hi = hi; s_hi > 0; s_hi -= 32) {
       const int s_lo = max(0, s_hi - 32);
       const int j = s_lo + lane;
-      const bool ov = j < s_hi && box_overlaps(srec[j], wx, wy);
+      const bool ov = j < s_hi && box_overlaps_rect(srec[j], pp.wx, pp.wy, 7, 7);
       unsigned mask = __ballot_sync(0xffffffffu, ov);
       while (mask) {
         const int msb = 31 - __clz(mask);
         mask &= ~(1u << msb);
         const int jj = s_lo + msb;
-        const int p = base + jj;
-        bool hit = false;
+        const int idx = base + jj;
         float x[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) x[v] = 0.f;
-        if (p < cont) {
-          const float4 v1 = srec[kBatch + jj];
-          const float4 v2 = srec[2 * kBatch + jj];
-          const float dx = v1.x - (float)px, dy = v1.y - (float)py;
-          const float maha = fmaxf(0.f, maha_sq(v1.z, v1.w, v2.x, dx, dy));
-          if (!(maha > v2.y)) {
-            const float g = expf(-0.5f * maha);
-            const float ap = fminf(kAlphaMax, v2.z * g);
-            if (!(ap < kAlphaMin)) {
-              hit = true;
-              const float one_m = 1.f - ap;
-              T = __fdividef(T, one_m);
-              const float wgt = ap * T;
-#pragma unroll
-              for (int k = 0; k < K; ++k) x[k] = dl[k] * wgt;
-              if (GEOM) {
-                float f[K];
-                load_feats<K>(srec, jj, v2.w, f);
-                float dap = 0.f;
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                  dap += dl[k] * (T * (f[k] - G[k]));
-                  G[k] = ap * f[k] + one_m * G[k];
-                }
-                if (DTAU) dap += dTf * __fdividef(-Tf, one_m);
-                x[K] = dap * g;                                    // alpha
-                x[K + 1] = dap * ((-v1.z * dx - v1.w * dy) * ap);  // u.x
-                x[K + 2] = dap * ((-v1.w * dx - v2.x * dy) * ap);  // u.y
-                x[K + 3] = dap * (-0.5f * ap * (dx * dx));         // conic a
-                x[K + 4] = dap * (-1.0f * ap * (dx * dy));         // conic b
-                x[K + 5] = dap * (-0.5f * ap * (dy * dy));         // conic c
-              }
-            }
-          }
-        }
+        const float4 v1 = srec[kBatch + jj];
+        const float4 v2 = srec[2 * kBatch + jj];
+        const float dx = v1.x - fx, dy0 = v1.y - fy0, dy1 = v1.y - fy1;
+        const float m0 = fmaxf(0.f, maha_sq(v1.z, v1.w, v2.x, dx, dy0));
+        const float m1 = fmaxf(0.f, maha_sq(v1.z, v1.w, v2.x, dx, dy1));
+        bool hit = adjoint_pixel<K, GEOM, DTAU>(p[0], idx, m0, v1, v2, dx, dy0, srec, jj, x);
+        hit |= adjoint_pixel<K, GEOM, DTAU>(p[1], idx, m1, v1, v2, dx, dy1, srec, jj, x);
         const unsigned cm = __ballot_sync(0xffffffffu, hit);
         if (!cm) continue;
         const int64_t g = sgid[jj];
@@ -282,19 +326,19 @@ __global__ void __launch_bounds__(kDrawThreads, 3)
           }
           continue;
         }
-        int idx;
+        int vidx;
         bool owner;
-        const float tot = warp_transpose_sum<NV>(x, lane, &idx, &owner);
-        if (owner && idx < NREAL) {
+        const float tot = warp_transpose_sum<NV>(x, lane, &vidx, &owner);
+        if (owner && vidx < NREAL) {
           float* dst;
-          if (idx < K)
-            dst = dfeat + g * K + idx;
-          else if (idx == K)
+          if (vidx < K)
+            dst = dfeat + g * K + vidx;
+          else if (vidx == K)
             dst = dalpha + g;
-          else if (idx < K + 3)
-            dst = du + 2 * g + (idx - K - 1);
+          else if (vidx < K + 3)
+            dst = du + 2 * g + (vidx - K - 1);
           else
-            dst = dconic + 3 * g + (idx - K - 3);
+            dst = dconic + 3 * g + (vidx - K - 3);
           atomicAdd(dst, tot);
         }
       }
@@ -314,7 +358,7 @@ int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, co
   switch (channels) {
 #define GSB_K(KK)                                                                           \
   case KK:                                                                                  \
-    k_draw<KK><<<tiles, kDrawThreads, 0, st>>>(H, W, gx, rg, gsid, s.records, tau_init, out, \
+    k_draw<KK><<<tiles, kDrawFwdThreads, 0, st>>>(H, W, gx, rg, gsid, s.records, tau_init, out, \
                                                contrib, final_tau);                         \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
