@@ -164,6 +164,25 @@ int gsb_splat_sort(int64_t n, int height, int width, const gsb_splat_plan* plan,
                    const void* state, void* sort_ws, int32_t* gsid_out, int32_t* ranges_out,
                    void* stream);
 
+/* gsb_splat_sort without the caller workspace; no counterpart in the
+ * reference extension.  For callers that cannot allocate device memory where
+ * they render (device memory owned by another runtime's pool, a plug-in
+ * handed only its input and output buffers, a fixed start-up footprint):
+ * the sort's temporaries live in one device array inside this library, of
+ * gsb_splat_sort_static_max_bytes() bytes (32 MiB: about 1.9M patches with
+ * 32-bit keys, 1.3M with 64-bit keys), which every GPU that loads the library
+ * holds until the process exits.  Plans needing more return GSB_ERR_CAPACITY
+ * with a message; use gsb_splat_sort then.  Allocates nothing; the first
+ * call on each device looks up the array's device address (once, with that
+ * device current), so make that first call before any stream capture.  All
+ * calls on a device share the array and it keeps the last call's contents
+ * (nothing needs to start at zero), so calls that overlap on the GPU race:
+ * order them on one stream.  Inputs, outputs and results as gsb_splat_sort. */
+size_t gsb_splat_sort_static_max_bytes(void);
+int gsb_splat_sort_static(int64_t n, int height, int width, const gsb_splat_plan* plan,
+                          const void* state, int32_t* gsid_out, int32_t* ranges_out,
+                          void* stream);
+
 /* out [channels,H,W], contrib [H,W] (1-based index of the last blended
  * Gaussian in the tile list), final_tau [H,W].  Pixels of tiles without
  * patches are set to 0 / 0 / tau_init (0 for weights, 1 for colours, as

@@ -46,6 +46,8 @@ _SIGS = {
     "gsb_splat_counts": (_i32, [_i64, _i32, _i32, _p, _p, _p]),
     "gsb_splat_sort_bytes": (_sz, [_i64, _i32, _i32, _p]),
     "gsb_splat_sort": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p, _p]),
+    "gsb_splat_sort_static_max_bytes": (_sz, []),
+    "gsb_splat_sort_static": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p]),
     "gsb_splat_draw": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _f32, _p, _p, _p, _p]),
     "gsb_splat_backward": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _i32, _p, _p, _p, _p,
                                   _p, _p, _p, _p, _p, _p, _p, _p]),
