@@ -91,6 +91,22 @@ def step(wl, cam=None, target=None, backward=True):
     return loss
 
 
+def step_fused(wl, backward=True):
+    """The same step through the fused render path (palette_b200.render): one
+    preprocess kernel instead of five operators; weights-only backward, as
+    the reference's backward (only dc, A, B and the palette need gradients)."""
+    from palette_b200.loss import palette_l1_loss
+    from palette_b200.render import render_palette
+    for p in (wl["dc"], wl["A"], wl["B"], wl["palette"]):
+        p.grad = None
+    layer, _, _ = render_palette(wl["pws"], wl["rots"], wl["scales"], wl["alphas"], wl["cam"],
+                                 dc=wl["dc"], A=wl["A"], B=wl["B"])
+    loss = palette_l1_loss(layer, wl["palette"], wl["target"])
+    if backward:
+        loss.backward()
+    return loss
+
+
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi SM clock / throttle-reason samples during the timed region."""
@@ -270,6 +286,25 @@ def stage_breakdown(wl, reps=5):
             None, None, sp), reps, st) / reps
         out["lowrank_backward"] = timed(lambda: gsc.sh2Weight_fast_B(A, B, ylm, dW[:, 0], K, Q),
                                         reps, st) / reps
+        # fused path: one preprocess kernel (+ count scan), weights-only backward
+        from palette_b200.render import camera_struct
+        camst, _keep = camera_struct(cam)
+        params = _lib.PaletteParams(_lib.WEIGHTS_LOWRANK, _lib.DTYPE_F32, K, 5, Q, int(A.shape[2]),
+                                    dc.data_ptr(), A.data_ptr(), B.data_ptr())
+        fstate = torch.empty_like(state)
+        out["fused_preprocess"] = timed(lambda: _lib.call(
+            "bench", "gsb_render_preprocess", n, C.byref(camst), _lib.ptr(wl["pws"]),
+            _lib.ptr(wl["rots"]), _lib.ptr(wl["scales"]), _lib.ptr(wl["alphas"]), C.byref(params),
+            _lib.ptr(fstate), None, sp), reps, st) / reps
+        scratch = torch.empty(int(L.gsb_render_backward_bytes(n, K)), dtype=torch.uint8,
+                              device=us.device)
+        gdc, gA, gB = torch.empty_like(dc), torch.empty_like(A), torch.empty_like(B)
+        out["fused_backward"] = timed(lambda: _lib.call(
+            "bench", "gsb_render_backward", n, C.byref(camst), _lib.ptr(wl["pws"]),
+            _lib.ptr(wl["rots"]), _lib.ptr(wl["scales"]), _lib.ptr(wl["alphas"]), C.byref(params),
+            _lib.ptr(state), _lib.ptr(ranges), _lib.ptr(gsid), _lib.ptr(contrib), _lib.ptr(ft),
+            _lib.ptr(g), None, _lib.ptr(scratch), None, None, None, None, _lib.ptr(gdc),
+            _lib.ptr(gA), _lib.ptr(gB), sp), reps, st) / reps
         visible = int((d > 0.2).sum())
         pix = H * W
         # algorithmic bytes: per patch 48 B record + 4 B id; per pixel K*4 + 8 B out;
@@ -416,6 +451,14 @@ def run_b200(a):
     ems = allreduce_max(timed(e2e_step, a.steps, stream), world, device)
     h2d = int((R_h.numel() + t_h.numel() + c_h.numel() + wl["target_host"].numel()) * 4)
 
+    # the fused render path, same workload
+    for _ in range(3):
+        step_fused(wl)
+    fu_ms = allreduce_max(timed(lambda: step_fused(wl), a.steps, stream), world, device) / a.steps
+    with torch.no_grad():
+        fu_fms = allreduce_max(timed(lambda: step_fused(wl, backward=False), a.steps, stream),
+                               world, device) / a.steps
+
     stages, alg = stage_breakdown(wl)
     dom = max(("draw", "draw_backward"), key=lambda k: stages[k])
     dom_bytes = alg["bytes_draw"] if dom == "draw" else alg["bytes_bwd"]
@@ -430,7 +473,7 @@ def run_b200(a):
 
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cb = cpu_baseline(wl, steps=2, warmup=0)
+        cb = cpu_baseline(wl, steps=8, warmup=1)
         cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         line = dict(metric=METRIC, value=round(value, 3), unit="iters/s", n_gpus=world,
@@ -442,6 +485,9 @@ def run_b200(a):
                     e2e=dict(value=round(world * a.steps / (ems / 1000.0), 3), unit="iters/s",
                              h2d_bytes_per_step=h2d, d2h_bytes_per_step=4),
                     gpu_launches=launches, clocks=clk, roofline=roof, cpu_baseline=cb,
+                    fused_path=dict(iters_per_s=round(world * 1000.0 / fu_ms, 3),
+                                    ms_per_step=round(fu_ms, 4), forward_ms=round(fu_fms, 4),
+                                    frames_per_s=round(world * 1000.0 / fu_fms, 2)),
                     stages_ms={k: round(v, 4) for k, v in stages.items()},
                     patches=alg["M"])
         print(json.dumps(line), flush=True)

@@ -229,6 +229,67 @@ int gsb_palette_l1(int K, int height, int width, const float* layer, const float
                    const float* target, float* image, float* loss, float* dlayer,
                    float* dpalette, void* stream);
 
+/* ============================================================ fused path
+ * One view of the palette-weight rasterizer with the per-Gaussian work of
+ * project / computeCov3D / computeCov2D / sh2Weight(_fast) / inverseCov2D /
+ * getRects done in one kernel (gsb_render_preprocess, filling the same
+ * `state` as gsb_splat_pack and its count step); then gsb_splat_counts /
+ * gsb_splat_sort / gsb_splat_draw as for splat_weight (gsplat/gsmodel.py:
+ * 107-118, 155-170).  gsb_render_backward is the adjoint of the whole view:
+ * compositing and the per-Gaussian chain to every parameter
+ * (vanilla_3dgs/gsplat/gsmodel.py:65-75 is the reference's chain for the
+ * geometry, gsplat/gsmodel.py:120-130, 172-200 for the weights). */
+#define GSB_WEIGHTS_FULL 0    /* shs [n,16K], SH order 3, band-major          */
+#define GSB_WEIGHTS_LOWRANK 1 /* dc [n,K], A [n,P,rank], B [n,rank,Q]         */
+
+typedef struct gsb_camera {
+  const float* Rcw; /* device [3,3] row-major world -> camera rotation  */
+  const float* tcw; /* device [3] translation                          */
+  const float* twc; /* device [3] camera centre in world coordinates    */
+  float fx, fy, cx, cy;
+  int width, height;
+} gsb_camera;
+
+typedef struct gsb_palette_params {
+  int mode;       /* GSB_WEIGHTS_FULL or GSB_WEIGHTS_LOWRANK              */
+  int dtype;      /* GSB_DTYPE_F32 or GSB_DTYPE_BF16 (FP32 arithmetic)    */
+  int K;          /* palette entries = channels composited               */
+  int P, Q, rank; /* low-rank factor shape                                */
+  const void* w0; /* full: shs [n,16K]; low-rank: dc [n,K]               */
+  const void* A;  /* low-rank: [n,P,rank]                                 */
+  const void* B;  /* low-rank: [n,rank,Q]                                 */
+} gsb_palette_params;
+
+/* pws [n,3], rots [n,4] (w,x,y,z), scales [n,3], alphas [n]; `state` of
+ * gsb_splat_state_bytes(n, K, height, width) bytes, 256-byte aligned;
+ * depths_out [n] (may be NULL) receives the camera depth, or -1 for
+ * Gaussians dropped by the depth, conic or tile tests (the reference's
+ * depths after its in-place updates).  Supported shapes: full K in 3..8;
+ * low-rank (K,P,Q,rank) in {(5,5,15,1..4), (3,3,15,1), (4,4,15,1),
+ * (6,6,15,1), (6,6,15,3)}. */
+int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float* pws, const float* rots,
+                          const float* scales, const float* alphas,
+                          const gsb_palette_params* params, void* state, float* depths_out,
+                          void* stream);
+
+/* Scratch bytes gsb_render_backward needs for the per-Gaussian screen-space
+ * gradients. */
+size_t gsb_render_backward_bytes(int64_t n, int K);
+
+/* dloss_dout [K,H,W]; dloss_dtau [H,W] may be NULL.  Outputs (FP32,
+ * overwritten): dw0 (shs [n,16K] or dc [n,K]), dA [n,P,rank], dB [n,rank,Q]
+ * always; the geometry gradients dpws [n,3], drots [n,4], dscales [n,3],
+ * dalphas [n] either all four or none.  With none (the reference backward's
+ * scope) only the weight gradients are computed and dloss_dtau, which
+ * reaches only geometry and opacity, is ignored. */
+int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* pws, const float* rots,
+                        const float* scales, const float* alphas,
+                        const gsb_palette_params* params, const void* state,
+                        const int32_t* ranges, const int32_t* gsid, const int32_t* contrib,
+                        const float* final_tau, const float* dloss_dout, const float* dloss_dtau,
+                        void* scratch, float* dpws, float* drots, float* dscales, float* dalphas,
+                        float* dw0, float* dA, float* dB, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

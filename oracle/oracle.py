@@ -304,3 +304,59 @@ def render_weights(pws, rots, scales, alphas, weights, cam, dtype=np.float32, li
         ranges, gsid = lists
     out, contrib, ft = draw(H, W, K, ranges, gsid, pre["us"], pre["cinv"], alphas, weights, 0.0, dtype)
     return dict(layer=out, contrib=contrib, final_tau=ft, ranges=ranges, gsid=gsid, pre=pre)
+
+
+def render_weights_backward(pws, rots, scales, alphas, cam, twc, K, shs=None, lowrank=None,
+                            lists=None, dout=None, dT=None, dtype=np.float64):
+    """Gradients of sum(dout * layer) + sum(dT * final_tau) with respect to
+    every input of the palette-weight path, by the reference's own chain rule
+    (vanilla_3dgs/gsplat/gsmodel.py:65-75: per-operator Jacobians composed
+    with the compositing adjoint), with the weights' true view-direction
+    derivative.  Weights come from full SH ``shs [N,16K]`` or from
+    ``lowrank = (dc [N,K], A [N,P,r] or [N,P], B [N,r,Q] or [N,Q])``.
+    `lists` = (ranges, gsid) fixes the tile lists.  Returns a dict of
+    gradients plus the forward (layer, final_tau, contrib)."""
+    dt = np.dtype(dtype).type
+    Rcw, tcw, _ = camera_arrays(cam, dtype)
+    twc = _arr(twc, dtype).reshape(3)
+    H, W = int(cam.height), int(cam.width)
+    us, pcs, depths, du_dpc = project(pws, Rcw, tcw, cam.fx, cam.fy, cam.cx, cam.cy, True, dtype)
+    c3, dc3_dq, dc3_ds = cov3d(rots, scales, depths, True, dtype)
+    c2, dc2_dc3, dc2_dpc = cov2d(c3, pcs, Rcw, depths, cam.fx, cam.fy, W, H, True, dtype)
+    cinv, areas, dci_dc2 = inverse_cov2d(c2, depths, True, dtype)
+    if lowrank is None:
+        shs_eff = _arr(shs, dtype)
+    else:  # C = A B; band l+1, channel k of the weights is C[g], g = l*K + k
+        dc, A, B = (_arr(x, dtype) for x in lowrank)
+        A3 = A[:, :, None] if A.ndim == 2 else A
+        B3 = B[:, None, :] if B.ndim == 2 else B
+        Cm = np.einsum("npr,nrq->npq", A3, B3).reshape(A.shape[0], -1)
+        shs_eff = np.concatenate([dc, Cm], axis=1)
+    feat, Y, dw_dpw = sh2feat(shs_eff, pws, twc, K, True, dtype, ref_quirk=False)
+    if lists is None:
+        b = bin_gaussians(us.astype(np.float32), areas.copy(), depths.astype(np.float32), H, W)
+        lists = (b["ranges"], b["gsid"])
+    ranges, gsid = lists
+    layer, contrib, ft = draw(H, W, K, ranges, gsid, us, cinv, alphas, feat, 0.0, dtype)
+    dout = np.zeros((K, H, W), dtype) if dout is None else _arr(dout, dtype)
+    g = draw_backward(H, W, K, ranges, gsid, us, cinv, alphas, feat, ft, contrib, dout, dT, dtype)
+    live = (np.any(g["dfeat"] != 0, axis=1) | np.any(g["du"] != 0, axis=1) |
+            np.any(g["dconic"] != 0, axis=1))
+    z = lambda a: np.where(live.reshape((-1,) + (1,) * (a.ndim - 1)), a, dt(0))
+    dc2 = np.einsum("nj,nji->ni", g["dconic"], z(dci_dc2))
+    dc3 = np.einsum("nj,nji->ni", dc2, z(dc2_dc3))
+    dpc = np.einsum("nj,nji->ni", g["du"], z(du_dpc)) + np.einsum("nj,nji->ni", dc2, z(dc2_dpc))
+    out = dict(layer=layer, final_tau=ft, contrib=contrib, dalphas=g["dalpha"],
+               drots=np.einsum("nj,nji->ni", dc3, z(dc3_dq)),
+               dscales=np.einsum("nj,nji->ni", dc3, z(dc3_ds)),
+               dpws=dpc @ Rcw + np.einsum("nk,nki->ni", g["dfeat"], z(dw_dpw)),
+               dfeat=g["dfeat"])
+    dshs = (g["dfeat"][:, None, :] * Y.reshape(Y.shape[0], -1)[:, :, None]).reshape(len(feat), -1)
+    if lowrank is None:
+        out["dshs"] = dshs
+    else:
+        dC = dshs[:, K:].reshape(Cm.shape[0], A3.shape[1], B3.shape[2])
+        out["ddc"] = dshs[:, :K]
+        out["dA"] = np.einsum("npq,nrq->npr", dC, B3).reshape(A.shape)
+        out["dB"] = np.einsum("npq,npr->nrq", dC, A3).reshape(B.shape)
+    return out

@@ -13,6 +13,7 @@
 
 #include "gsb_geometry.cuh"
 #include "gsb_internal.h"
+#include "gsb_record.cuh"
 
 namespace gsb {
 
@@ -90,13 +91,7 @@ __device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t* war
 // ------------------------------------------------------------------ pack
 // One thread per Gaussian: tile rectangle and patch count (getRects,
 // gsplatcu/kernel.cu:127-162, including its in-place depth/areas updates),
-// the quantised depth key, and the packed compositing record.
-//
-// The record carries a conservative support box: pixels outside it satisfy
-// d^T Q d > cut, where cut = 2 ln(alpha/0.002) + margin guarantees
-// alpha' < 0.002 in the reference's evaluation.  The box is widened for the
-// rounding error of the FP32 quadratic form (proportional to the conic's
-// condition number) and disabled for degenerate or non-finite conics.
+// the quantised depth key, and the packed compositing record (gsb_record.cuh).
 template <typename T>
 __global__ void __launch_bounds__(kBinBlock)
     k_pack(int64_t n, uint32_t gx, uint32_t gy, int C, int V, const float* __restrict__ us,
@@ -130,33 +125,9 @@ __global__ void __launch_bounds__(kBinBlock)
     }
     const float qa = cinv[3 * i], qb = cinv[3 * i + 1], qc = cinv[3 * i + 2];
     const float a = alphas[i];
-    const float cut = 2.f * logf(a / kAlphaMin) + kCutMargin;
-    float xmin = -INFINITY, xmax = INFINITY, ymin = -INFINITY, ymax = INFINITY;
-    if (cut < 0.f) {  // alpha < 0.002: never blends, empty box
-      xmin = ymin = INFINITY;
-      xmax = ymax = -INFINITY;
-    } else if (isfinite(cut) && isfinite(ux) && isfinite(uy)) {
-      const float det = qa * qc - qb * qb;
-      const float kappa = (qa + qc) * (qa + qc) / det;
-      if (det > 0.f && qa > 0.f && qc > 0.f && kappa < 1e5f) {
-        const float c2 = cut * (1.f + 4e-6f * kappa) + 1e-3f;
-        const float hx = sqrtf(c2 * qc / det) * 1.0001f + 0.02f;
-        const float hy = sqrtf(c2 * qa / det) * 1.0001f + 0.02f;
-        if (isfinite(hx) && isfinite(hy)) {
-          xmin = ux - hx;
-          xmax = ux + hx;
-          ymin = uy - hy;
-          ymax = uy + hy;
-        }
-      }
-    }
-    float4* rec = records + i * V;
     float f[4 * 5];
-#pragma unroll
-    for (int k = 0; k < 20; ++k) f[k] = 0.f;
-    f[0] = xmin; f[1] = xmax; f[2] = ymin; f[3] = ymax;
-    f[4] = ux; f[5] = uy; f[6] = qa; f[7] = qb;
-    f[8] = qc; f[9] = cut; f[10] = a;
+    record_head(ux, uy, qa, qb, qc, a, f);
+    float4* rec = records + i * V;
 #pragma unroll
     for (int k = 0; k < kMaxChannels; ++k)
       if (k < C) f[11 + k] = ld(feats, i * C + k);

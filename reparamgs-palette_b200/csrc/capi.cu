@@ -77,7 +77,13 @@ GSB_API const char* gsb_last_error(void) { return g_err; }
 GSB_API int gsb_version(void) { return 100; }
 GSB_API int gsb_device_status(uint32_t* status, int clear, void* stream) {
   GSB_CHECK_ARG(status, "device_status: null pointer");
-  return lowrank_status(status, clear != 0, ST(stream));
+  uint32_t a = 0, b = 0;
+  int rc = lowrank_status(&a, clear != 0, ST(stream));
+  if (rc) return rc;
+  rc = fused_status(&b, clear != 0, ST(stream));
+  if (rc) return rc;
+  *status = a | b;
+  return GSB_OK;
 }
 
 GSB_API unsigned long long gsb_launch_count(void) {
@@ -322,4 +328,136 @@ GSB_API int gsb_palette_l1(int K, int height, int width, const float* layer,
   GSB_CHECK_ARG(((int64_t)height * width == 0) || (layer && target), "palette_l1: null input");
   return launch_palette_l1(K, height, width, layer, palette, target, image, loss, dlayer, dpalette,
                            ST(stream));
+}
+
+// ------------------------------------------------------------- fused path
+static int check_params(const char* op, int64_t n, const gsb_palette_params* p) {
+  GSB_CHECK_ARG(p, "%s: null palette parameters", op);
+  GSB_CHECK_ARG(p->mode == GSB_WEIGHTS_FULL || p->mode == GSB_WEIGHTS_LOWRANK, "%s: bad mode %d",
+                op, p->mode);
+  GSB_CHECK_ARG(valid_dtype(p->dtype), "%s: bad dtype %d", op, p->dtype);
+  GSB_CHECK_ARG(p->K >= 1 && p->K <= GSB_MAX_CHANNELS, "%s: K must be in [1, %d]", op,
+                GSB_MAX_CHANNELS);
+  GSB_CHECK_ARG(n == 0 || p->w0, "%s: null weight parameters", op);
+  if (p->mode == GSB_WEIGHTS_LOWRANK) {
+    GSB_CHECK_ARG(p->P > 0 && p->Q > 0 && p->rank > 0 && (p->P * p->Q) % p->K == 0,
+                  "%s: bad low-rank shape P=%d Q=%d rank=%d K=%d", op, p->P, p->Q, p->rank, p->K);
+    GSB_CHECK_ARG(n == 0 || (p->A && p->B), "%s: null low-rank factors", op);
+  }
+  return GSB_OK;
+}
+
+static CamArgs cam_args(const gsb_camera* c) {
+  CamArgs a;
+  a.R = c->Rcw;
+  a.t = c->tcw;
+  a.c = c->twc;
+  a.fx = c->fx;
+  a.fy = c->fy;
+  a.cx = c->cx;
+  a.cy = c->cy;
+  // tan of the half field of view, formed in FP32 as gsplatcu/gausplat.cu:357-358
+  a.tanx = c->width / (2 * c->fx);
+  a.tany = c->height / (2 * c->fy);
+  return a;
+}
+
+GSB_API int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float* pws,
+                                  const float* rots, const float* scales, const float* alphas,
+                                  const gsb_palette_params* params, void* state,
+                                  float* depths_out, void* stream) {
+  GSB_CHECK_ARG(cam && cam->Rcw && cam->tcw && cam->twc, "render_preprocess: null camera");
+  int rc = check_image("render_preprocess", n, cam->height, cam->width, params ? params->K : 1);
+  if (rc) return rc;
+  if ((rc = check_params("render_preprocess", n, params))) return rc;
+  GSB_CHECK_ARG(state && ((uintptr_t)state & 255) == 0,
+                "render_preprocess: state must be 256-byte aligned");
+  GSB_CHECK_ARG(n == 0 || (pws && rots && scales && alphas), "render_preprocess: null input");
+  const SplatState s = carve_state(state, n, params->K, cam->height, cam->width);
+  if (cudaMemsetAsync(s.stats, 0, 16 * sizeof(uint32_t), ST(stream)) != cudaSuccess ||
+      cudaMemsetAsync(s.block_sums, 0, (size_t)(s.n_blocks > 0 ? s.n_blocks : 1) * 4,
+                      ST(stream)) != cudaSuccess)
+    return check_launch("render_preprocess (memset)", 0);
+  FusedArgs f{};
+  f.n = n;
+  f.gx = (uint32_t)div_up(cam->width, kTile);
+  f.gy = (uint32_t)div_up(cam->height, kTile);
+  f.cam = cam_args(cam);
+  f.pws = pws;
+  f.rots = rots;
+  f.scales = scales;
+  f.alphas = alphas;
+  f.w0 = params->w0;
+  f.wa = params->A;
+  f.wb = params->B;
+  f.st = s;
+  f.depths_out = depths_out;
+  rc = launch_render(params->mode, params->dtype, params->K, params->P, params->Q, params->rank, f,
+                     false, ST(stream));
+  if (rc) return rc;
+  return launch_count_scan(n, s, ST(stream));
+}
+
+GSB_API size_t gsb_render_backward_bytes(int64_t n, int K) {
+  if (n < 0 || K < 1 || K > GSB_MAX_CHANNELS) return 0;
+  return (size_t)n * (K + 5) * sizeof(float) + 256;
+}
+
+GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* pws,
+                                const float* rots, const float* scales, const float* alphas,
+                                const gsb_palette_params* params, const void* state,
+                                const int32_t* ranges, const int32_t* gsid,
+                                const int32_t* contrib, const float* final_tau,
+                                const float* dloss_dout, const float* dloss_dtau, void* scratch,
+                                float* dpws, float* drots, float* dscales, float* dalphas,
+                                float* dw0, float* dA, float* dB, void* stream) {
+  GSB_CHECK_ARG(cam && cam->Rcw && cam->tcw && cam->twc, "render_backward: null camera");
+  int rc = check_image("render_backward", n, cam->height, cam->width, params ? params->K : 1);
+  if (rc) return rc;
+  if ((rc = check_params("render_backward", n, params))) return rc;
+  GSB_CHECK_ARG(state && ranges && contrib && final_tau && dloss_dout,
+                "render_backward: null pointer");
+  GSB_CHECK_ARG(n == 0 || (scratch && dw0 && pws && rots && scales && alphas),
+                "render_backward: null input/output");
+  GSB_CHECK_ARG(params->mode == GSB_WEIGHTS_FULL || n == 0 || (dA && dB),
+                "render_backward: null low-rank gradient outputs");
+  const bool geom = dpws || drots || dscales || dalphas;
+  GSB_CHECK_ARG(!geom || (dpws && drots && dscales && dalphas),
+                "render_backward: pass all of dpws, drots, dscales, dalphas or none");
+  const int K = params->K;
+  const SplatState s = carve_state((void*)state, n, K, cam->height, cam->width);
+  float* g_feat = (float*)scratch;
+  float* g_u = g_feat + (size_t)n * K;
+  float* g_conic = g_u + (size_t)n * 2;
+  if (n > 0 &&
+      (cudaMemsetAsync(scratch, 0, (size_t)n * (geom ? K + 5 : K) * sizeof(float), ST(stream)) !=
+           cudaSuccess ||
+       (geom && cudaMemsetAsync(dalphas, 0, (size_t)n * sizeof(float), ST(stream)) != cudaSuccess)))
+    return check_launch("render_backward (memset)", 0);
+  rc = launch_draw_backward(n, cam->height, cam->width, K, ranges, gsid, s, contrib, final_tau,
+                            dloss_dout, geom ? dloss_dtau : nullptr, g_feat,
+                            geom ? dalphas : nullptr, geom ? g_u : nullptr,
+                            geom ? g_conic : nullptr, ST(stream));
+  if (rc) return rc;
+  FusedArgs f{};
+  f.n = n;
+  f.cam = cam_args(cam);
+  f.pws = pws;
+  f.rots = rots;
+  f.scales = scales;
+  f.alphas = alphas;
+  f.w0 = params->w0;
+  f.wa = params->A;
+  f.wb = params->B;
+  f.g_feat = g_feat;
+  f.g_u = geom ? g_u : nullptr;
+  f.g_conic = geom ? g_conic : nullptr;
+  f.d_pws = dpws;
+  f.d_rots = drots;
+  f.d_scales = dscales;
+  f.d_w0 = dw0;
+  f.d_wa = dA;
+  f.d_wb = dB;
+  return launch_render(params->mode, params->dtype, K, params->P, params->Q, params->rank, f, true,
+                       ST(stream));
 }

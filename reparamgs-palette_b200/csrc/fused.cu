@@ -1,0 +1,556 @@
+// Fused render path.
+//
+// Forward: one kernel per view does, per Gaussian, everything the reference
+// runs as five operators plus getRects (project, computeCov3D, computeCov2D,
+// sh2Weight / sh2Weight_fast, inverseCov2D; gsplat/gsmodel.py:107-118 and
+// 155-170): projection, 3D and 2D covariance, conic and extents, view-
+// dependent palette weights (full SH order 3 or rank-r low-rank factors,
+// FP32 or BF16 storage, FP32 arithmetic), the tile rectangle and the packed
+// compositing record, with the same device functions as the separate
+// operators.  Sorting and compositing are shared with splat_weight.
+//
+// Backward: the compositing adjoint (opacity / centre / conic / weight terms,
+// raster.cu) followed by a per-Gaussian chain-rule kernel that recomputes the
+// forward quantities from the parameters and maps the screen-space gradients
+// to the parameters: conic -> 2D covariance -> 3D covariance -> (rotation,
+// scale); centre and 2D covariance -> camera-space centre -> world centre;
+// weights -> SH coefficients or low-rank factors, and the view direction ->
+// world centre.  The frustum clamp and the 0.99 opacity clamp are not
+// differentiated, as in the reference's own chain
+// (vanilla_3dgs/gsplat/gsmodel.py:65-75).
+#include "gsb_geometry.cuh"
+#include "gsb_internal.h"
+#include "gsb_record.cuh"
+#include "gsb_stage.cuh"
+#include "gsb_tma.cuh"
+
+namespace gsb {
+
+constexpr int kFuseThreads = 128;
+static __device__ uint32_t g_fused_status;
+
+// Row lengths of the colour-parameter arrays (floats per Gaussian).
+template <int MODE, int K, int P, int Q, int R>
+struct WRows {
+  static constexpr int W0 = MODE == GSB_WEIGHTS_FULL ? 16 * K : K;  // shs or dc
+  static constexpr int WA = MODE == GSB_WEIGHTS_FULL ? 0 : P * R;
+  static constexpr int WB = MODE == GSB_WEIGHTS_FULL ? 0 : R * Q;
+  static constexpr int L = MODE == GSB_WEIGHTS_FULL ? 15 : P * Q / K;
+  static constexpr int IN = 3 + 4 + 3 + 1 + W0 + WA + WB;  // staged floats per Gaussian
+};
+
+// Camera: rotation, translation and centre stay in device memory (so a
+// captured graph can be replayed for a new camera by rewriting them); the
+// intrinsics are kernel arguments.
+struct CamRegs {
+  float R[9], t[3], c[3];
+};
+
+__device__ __forceinline__ CamRegs load_cam(const CamArgs& a) {
+  CamRegs r;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r.R[k] = __ldg(a.R + k);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    r.t[k] = __ldg(a.t + k);
+    r.c[k] = __ldg(a.c + k);
+  }
+  return r;
+}
+
+// Shared-memory regions of one block: the rows of its Gaussians, array by
+// array, back to back.
+template <int MODE, int K, int P, int Q, int R>
+struct Staged {
+  using WS = WRows<MODE, K, P, Q, R>;
+  const float *p, *q, *s, *al, *w0, *wa, *wb;
+  __device__ __forceinline__ explicit Staged(const float* sm) {
+    const int nt = blockDim.x;
+    p = sm;
+    q = p + nt * 3;
+    s = q + nt * 4;
+    al = s + nt * 3;
+    w0 = al + nt;
+    wa = w0 + nt * WS::W0;
+    wb = wa + nt * WS::WA;
+  }
+};
+
+// Stage one block's parameter rows (pws, rots, scales, alphas, colour
+// parameters) into shared memory, by bulk copies when every span is aligned
+// FP32 and the block is full.  Returns false if a bulk wait expired (the
+// status word is set and the block must not use the staged rows).
+template <int MODE, int K, int P, int Q, int R, typename T>
+__device__ __forceinline__ bool stage_params(int64_t n, int64_t row0, const float* pws,
+                                             const float* rots, const float* scales,
+                                             const float* alphas, const T* w0, const T* wa,
+                                             const T* wb, float* sm, uint64_t* bar) {
+  using WS = WRows<MODE, K, P, Q, R>;
+  const Staged<MODE, K, P, Q, R> S(sm);
+  const int nt = blockDim.x;
+  const bool full = row0 + nt <= n;
+  bool bulk = full && sizeof(T) == 4 && aligned16(pws + row0 * 3) && aligned16(rots + row0 * 4) &&
+              aligned16(scales + row0 * 3) && aligned16(alphas + row0) &&
+              aligned16(w0 + row0 * WS::W0);
+  if (MODE != GSB_WEIGHTS_FULL)
+    bulk = bulk && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB);
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, (uint32_t)(nt * WS::IN * 4));
+  }
+  stage_rows<3>(pws, row0, n, (float*)S.p, bulk, bar);
+  stage_rows<4>(rots, row0, n, (float*)S.q, bulk, bar);
+  stage_rows<3>(scales, row0, n, (float*)S.s, bulk, bar);
+  stage_rows<1>(alphas, row0, n, (float*)S.al, bulk, bar);
+  stage_rows<WS::W0>(w0, row0, n, (float*)S.w0, bulk, bar);
+  if constexpr (MODE != GSB_WEIGHTS_FULL) {
+    stage_rows<WS::WA>(wa, row0, n, (float*)S.wa, bulk, bar);
+    stage_rows<WS::WB>(wb, row0, n, (float*)S.wb, bulk, bar);
+  }
+  __syncthreads();
+  if (bulk && !mbar_wait(bar, 0)) {
+    if (threadIdx.x == 0) atomicOr(&g_fused_status, kStatusBulkTimeout);
+    mbar_wait(bar, 0);  // bounded second wait for copies still in flight
+    return false;
+  }
+  return true;
+}
+
+// Palette weights of one Gaussian from its staged parameter rows.
+template <int MODE, int K, int P, int Q, int R>
+__device__ __forceinline__ void weights_of(const float* w0, const float* wa, const float* wb,
+                                           const float* Y, float* w) {
+  if constexpr (MODE == GSB_WEIGHTS_FULL) {
+    sh_weights_full<K>([&](int idx) { return w0[idx]; }, 16, Y, w);
+  } else {
+    lowrank_weights<K, P, Q, R>(w0, wa, wb, Y, w);
+  }
+}
+
+// ------------------------------------------------------------- forward
+template <int MODE, int K, int P, int Q, int R, typename T>
+__global__ void __launch_bounds__(kFuseThreads)
+    k_render_preprocess(int64_t n, uint32_t gx, uint32_t gy, CamArgs cam,
+                        const float* __restrict__ pws, const float* __restrict__ rots,
+                        const float* __restrict__ scales, const float* __restrict__ alphas,
+                        const T* __restrict__ w0, const T* __restrict__ wa,
+                        const T* __restrict__ wb, float4* __restrict__ records,
+                        uint2* __restrict__ rects, uint32_t* __restrict__ dkeys,
+                        uint32_t* __restrict__ counts, uint32_t* __restrict__ block_sums,
+                        uint32_t* __restrict__ stats, float* __restrict__ depths_out) {
+  using WS = WRows<MODE, K, P, Q, R>;
+  constexpr int V = RecordLayout<K>::kVec4;
+  extern __shared__ __align__(16) float sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t warp_tot[kFuseThreads / 32];
+  const int nt = blockDim.x, t = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * nt;
+  const bool staged = stage_params<MODE, K, P, Q, R, T>(n, row0, pws, rots, scales, alphas, w0,
+                                                        wa, wb, sm, &bar);
+  const Staged<MODE, K, P, Q, R> S(sm);
+  const int64_t i = row0 + t;
+  uint32_t cnt = 0, dk = 0;
+  if (staged && i < n) {
+    const CamRegs cr = load_cam(cam);
+    float depth_out = kBadDepth;
+    const float3 pw = make_float3(S.p[3 * t], S.p[3 * t + 1], S.p[3 * t + 2]);
+    const Projected p = project_point(pw, cr.R, make_float3(cr.t[0], cr.t[1], cr.t[2]), cam.fx,
+                                      cam.fy, cam.cx, cam.cy);
+    if (p.valid) {
+      float cov3[6], cov2[3], conic[3];
+      int ext[2];
+      covariance_3d(make_float4(S.q[4 * t], S.q[4 * t + 1], S.q[4 * t + 2], S.q[4 * t + 3]),
+                    make_float3(S.s[3 * t], S.s[3 * t + 1], S.s[3 * t + 2]), cov3, nullptr,
+                    nullptr);
+      covariance_2d(cov3, p.x, p.y, p.z, cr.R, cam.fx, cam.fy, cam.tanx, cam.tany, cov2, nullptr,
+                    nullptr);
+      if (conic_and_extent(cov2[0], cov2[1], cov2[2], conic, ext, nullptr)) {
+        const TileRect r = tile_rect(p.ux, p.uy, (float)ext[0], (float)ext[1], gx, gy);
+        cnt = (r.y1 - r.y0) * (r.x1 - r.x0);
+        if (cnt > 0) {
+          depth_out = p.z;
+          dk = __float2uint_rz(p.z * 1000);
+          rects[i] = make_uint2(r.x0 | (r.y0 << 16), r.x1 | (r.y1 << 16));
+          float dir[3], Y[16], w[K], f[20];
+          view_direction(pw, make_float3(cr.c[0], cr.c[1], cr.c[2]), dir, nullptr, nullptr);
+          sh_basis(dir, WS::L + 1, Y);
+          weights_of<MODE, K, P, Q, R>(S.w0 + t * WS::W0, S.wa + t * WS::WA, S.wb + t * WS::WB,
+                                       Y, w);
+          record_head(p.ux, p.uy, conic[0], conic[1], conic[2], S.al[t], f);
+#pragma unroll
+          for (int k = 0; k < K; ++k) f[11 + k] = w[k];
+          float4* rec = records + i * V;
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            rec[v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
+        }
+      }
+    }
+    counts[i] = cnt;
+    dkeys[i] = dk;
+    if (depths_out) depths_out[i] = depth_out;
+  }
+  // block totals for the patch-count scan and the largest depth key
+  const int lane = t & 31, w = t >> 5;
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  uint32_t m = dk;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0 && m) atomicMax(stats + 1, m);
+  __syncthreads();
+  if (t == 0) {  // block_sums count blocks of kBinBlock Gaussians (zeroed by the caller)
+    uint32_t tot = 0;
+    for (int k = 0; k < nt / 32; ++k) tot += warp_tot[k];
+    if (tot) atomicAdd(block_sums + row0 / kBinBlock, tot);
+  }
+}
+
+// ------------------------------------------------------------ backward
+// Shared-memory plan of the backward kernel: only the rows it reads are
+// staged -- the centre (view direction), the weight gradients from the
+// compositing adjoint, the low-rank factors (their gradients need each
+// other), and with GEOM also rotation, scale, opacity and the SH
+// coefficients (the view-direction term); the parameter gradients are
+// assembled in shared memory and written back as contiguous spans.
+template <int MODE, int K, int P, int Q, int R, bool GEOM>
+struct BwdPlan {
+  using WS = WRows<MODE, K, P, Q, R>;
+  static constexpr bool kW0 = GEOM && MODE == GSB_WEIGHTS_FULL;  // shs needed
+  static constexpr bool kAB = MODE != GSB_WEIGHTS_FULL;
+  // input regions, in floats per Gaussian (offset = prefix * blockDim)
+  static constexpr int P_ = 3, G_ = K, Q_ = GEOM ? 4 : 0, S_ = GEOM ? 3 : 0, W0_ = kW0 ? WS::W0 : 0,
+                       A_ = kAB ? WS::WA : 0, B_ = kAB ? WS::WB : 0;
+  static constexpr int o_p = 0, o_g = o_p + P_, o_q = o_g + G_, o_s = o_q + Q_, o_w0 = o_s + S_,
+                       o_a = o_w0 + W0_, o_b = o_a + A_, in_floats = o_b + B_;
+  // output regions: d_w0, d_wa, d_wb
+  static constexpr int out_floats = WS::W0 + WS::WA + WS::WB;
+  static constexpr int o_dw0 = in_floats, o_dwa = o_dw0 + WS::W0, o_dwb = o_dwa + WS::WA;
+  static constexpr int floats = in_floats + out_floats;
+};
+
+template <int MODE, int K, int P, int Q, int R, bool GEOM, typename T>
+__device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const float* pws,
+                                               const float* rots, const float* scales,
+                                               const T* w0, const T* wa, const T* wb,
+                                               const float* g_feat, float* sm, uint64_t* bar) {
+  using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
+  using WS = WRows<MODE, K, P, Q, R>;
+  const int nt = blockDim.x;
+  const bool full = row0 + nt <= n;
+  bool bulk = full && aligned16(pws + row0 * 3) && aligned16(g_feat + row0 * K);
+  if (GEOM) bulk = bulk && aligned16(rots + row0 * 4) && aligned16(scales + row0 * 3);
+  if (BP::kW0) bulk = bulk && sizeof(T) == 4 && aligned16(w0 + row0 * WS::W0);
+  if (BP::kAB)
+    bulk = bulk && sizeof(T) == 4 && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB);
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, (uint32_t)(nt * BP::in_floats * 4));
+  }
+  stage_rows<3>(pws, row0, n, sm + nt * BP::o_p, bulk, bar);
+  stage_rows<K>(g_feat, row0, n, sm + nt * BP::o_g, bulk, bar);
+  if constexpr (GEOM) {
+    stage_rows<4>(rots, row0, n, sm + nt * BP::o_q, bulk, bar);
+    stage_rows<3>(scales, row0, n, sm + nt * BP::o_s, bulk, bar);
+  }
+  if constexpr (BP::kW0) stage_rows<WS::W0>(w0, row0, n, sm + nt * BP::o_w0, bulk, bar);
+  if constexpr (BP::kAB) {
+    stage_rows<WS::WA>(wa, row0, n, sm + nt * BP::o_a, bulk, bar);
+    stage_rows<WS::WB>(wb, row0, n, sm + nt * BP::o_b, bulk, bar);
+  }
+  __syncthreads();
+  if (bulk && !mbar_wait(bar, 0)) {
+    if (threadIdx.x == 0) atomicOr(&g_fused_status, kStatusBulkTimeout);
+    mbar_wait(bar, 0);  // bounded second wait for copies still in flight
+    return false;
+  }
+  return true;
+}
+
+// Writes one gradient array's block span from shared memory: one bulk copy
+// for a full, aligned block, else a coalesced per-thread copy.
+template <int ROWLEN>
+__device__ __forceinline__ void write_rows(float* g, int64_t row0, int64_t n, const float* s) {
+  const int nt = blockDim.x;
+  if (row0 + nt <= n && aligned16(g + row0 * ROWLEN)) {
+    if (threadIdx.x == 0) bulk_store(g + row0 * ROWLEN, s, (uint32_t)(nt * ROWLEN * 4));
+  } else {
+    stage_out_plain<ROWLEN>(g, row0, n, s);
+  }
+}
+
+// g_feat [n,K] (dL/dweights), g_u [n,2], g_conic [n,3] come from the
+// compositing adjoint, which also writes dL/dalpha directly.  Without GEOM
+// (weights-only backward: g_u, g_conic and the geometry outputs unused) only
+// the weight-parameter gradients are formed.
+template <int MODE, int K, int P, int Q, int R, typename T, bool GEOM>
+__global__ void __launch_bounds__(kFuseThreads)
+    k_render_backward_pre(int64_t n, CamArgs cam, const float* __restrict__ pws,
+                          const float* __restrict__ rots, const float* __restrict__ scales,
+                          const T* __restrict__ w0, const T* __restrict__ wa,
+                          const T* __restrict__ wb, const float* __restrict__ g_feat,
+                          const float* __restrict__ g_u, const float* __restrict__ g_conic,
+                          float* __restrict__ d_pws, float* __restrict__ d_rots,
+                          float* __restrict__ d_scales, float* __restrict__ d_w0,
+                          float* __restrict__ d_wa, float* __restrict__ d_wb) {
+  using WS = WRows<MODE, K, P, Q, R>;
+  using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
+  constexpr int L = WS::L;
+  extern __shared__ __align__(16) float sm[];
+  __shared__ __align__(8) uint64_t bar;
+  const int nt = blockDim.x, t = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * nt;
+  if (!stage_backward<MODE, K, P, Q, R, GEOM, T>(n, row0, pws, rots, scales, w0, wa, wb, g_feat, sm,
+                                                 &bar))
+    return;
+  const int64_t i = row0 + t;
+  float* o_w0 = sm + nt * BP::o_dw0 + t * WS::W0;
+  float* o_wa = sm + nt * BP::o_dwa + t * WS::WA;
+  float* o_wb = sm + nt * BP::o_dwb + t * WS::WB;
+  if (i < n) {
+    const float* s_p = sm + nt * BP::o_p + 3 * t;
+    const float* s_g = sm + nt * BP::o_g + K * t;
+    const float* s_wa = sm + nt * BP::o_a + t * WS::WA;
+    const float* s_wb = sm + nt * BP::o_b + t * WS::WB;
+    const float3 pw = make_float3(s_p[0], s_p[1], s_p[2]);
+    float gw[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) gw[k] = s_g[k];
+    const CamRegs cr = load_cam(cam);
+    float dir[3], nd[3], ninv, Y[16];
+    view_direction(pw, make_float3(cr.c[0], cr.c[1], cr.c[2]), dir, nd, &ninv);
+    sh_basis(dir, L + 1, Y);
+    float dpw[3] = {0.f, 0.f, 0.f}, dq[4] = {0.f, 0.f, 0.f, 0.f}, ds[3] = {0.f, 0.f, 0.f};
+    float G[48];
+    if constexpr (GEOM) {
+      const float* s_q = sm + nt * BP::o_q + 4 * t;
+      const float* s_s = sm + nt * BP::o_s + 3 * t;
+      const float gu[2] = {g_u[2 * i], g_u[2 * i + 1]};
+      const float gq[3] = {g_conic[3 * i], g_conic[3 * i + 1], g_conic[3 * i + 2]};
+      const bool any = gu[0] != 0.f || gu[1] != 0.f || gq[0] != 0.f || gq[1] != 0.f || gq[2] != 0.f;
+      const float4 q = make_float4(s_q[0], s_q[1], s_q[2], s_q[3]);
+      const float3 sc = make_float3(s_s[0], s_s[1], s_s[2]);
+      const Projected p = project_point(pw, cr.R, make_float3(cr.t[0], cr.t[1], cr.t[2]), cam.fx,
+                                        cam.fy, cam.cx, cam.cy);
+      if (any && p.valid) {
+        // conic -> cov2d -> (cov3d, pc); u -> pc
+        float cov3[6], M3[9], Rq[9], cov2[3], M2[6], xy[2];
+        covariance_3d(q, sc, cov3, M3, Rq);
+        covariance_2d(cov3, p.x, p.y, p.z, cr.R, cam.fx, cam.fy, cam.tanx, cam.tany, cov2, M2, xy);
+        const float a = cov2[0], b = cov2[1], c = cov2[2];
+        const float det_inv = 1.f / (a * c - b * b);
+        if (!isnan(det_inv)) {
+          const float d2 = det_inv * det_inv;
+          const float Ji[9] = {-c * c * d2,           2 * b * c * d2,            -a * c * d2 + det_inv,
+                               b * c * d2,            -2 * b * b * d2 - det_inv, a * b * d2,
+                               -a * c * d2 + det_inv, 2 * a * b * d2,            -a * a * d2};
+          float dc2[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) dc2[j] = gq[0] * Ji[j] + gq[1] * Ji[3 + j] + gq[2] * Ji[6 + j];
+          float d3[18], dpc_m[9];
+          cov2d_jacobians(cov3, M2, cr.R, xy[0], xy[1], p.z, cam.fx, cam.fy, d3, dpc_m);
+          float dS[6];
+#pragma unroll
+          for (int u = 0; u < 6; ++u)
+            dS[u] = dc2[0] * d3[u] + dc2[1] * d3[6 + u] + dc2[2] * d3[12 + u];
+          float dpc[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+            dpc[j] = dc2[0] * dpc_m[j] + dc2[1] * dpc_m[3 + j] + dc2[2] * dpc_m[6 + j];
+          const float zi = 1.f / p.z, zi2 = zi * zi;
+          dpc[0] += gu[0] * (cam.fx * zi);
+          dpc[1] += gu[1] * (cam.fy * zi);
+          dpc[2] += gu[0] * (-(p.x * cam.fx) * zi2) + gu[1] * (-(p.y * cam.fy) * zi2);
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+            dpw[j] += cr.R[j] * dpc[0] + cr.R[3 + j] * dpc[1] + cr.R[6 + j] * dpc[2];
+          float jq[24], js[18];
+          cov3d_jacobians(q, sc, M3, Rq, jq, js);
+#pragma unroll
+          for (int u = 0; u < 6; ++u) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dq[j] += dS[u] * jq[4 * u + j];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) ds[j] += dS[u] * js[3 * u + j];
+          }
+        }
+      }
+      sh_basis_grad(dir, L + 1, /*ref_quirk=*/false, G);
+    }
+    // colour parameters, and (GEOM) the view direction's share of d pws
+    float dd[3] = {0.f, 0.f, 0.f};
+    if constexpr (MODE == GSB_WEIGHTS_FULL) {
+      const float* s_w0 = sm + nt * BP::o_w0 + t * WS::W0;
+#pragma unroll
+      for (int l = 0; l < 16; ++l)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          o_w0[l * K + k] = gw[k] * Y[l];
+          if constexpr (GEOM) {
+            if (l > 0) {
+              const float cg = gw[k] * s_w0[l * K + k];
+              dd[0] += cg * G[3 * l];
+              dd[1] += cg * G[3 * l + 1];
+              dd[2] += cg * G[3 * l + 2];
+            }
+          }
+        }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) o_w0[k] = gw[k] * SH_C0;
+      // dC[p][q] = gw_k Y_{l+1} with g = l*K + k = p*Q + q
+#pragma unroll
+      for (int pp = 0; pp < P; ++pp) {
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0.f;
+#pragma unroll
+        for (int qq = 0; qq < Q; ++qq) {
+          const int g = pp * Q + qq, k = g % K, l = g / K;
+          const float dC = gw[k] * Y[l + 1];
+          float coef = 0.f;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            acc[r] += dC * s_wb[r * Q + qq];
+            if constexpr (GEOM) coef += s_wa[pp * R + r] * s_wb[r * Q + qq];
+          }
+          if constexpr (GEOM) {
+            const float cg = gw[k] * coef;
+            dd[0] += cg * G[3 * (l + 1)];
+            dd[1] += cg * G[3 * (l + 1) + 1];
+            dd[2] += cg * G[3 * (l + 1) + 2];
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) o_wa[pp * R + r] = acc[r];
+      }
+#pragma unroll
+      for (int qq = 0; qq < Q; ++qq) {
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0.f;
+#pragma unroll
+        for (int pp = 0; pp < P; ++pp) {
+          const int g = pp * Q + qq, k = g % K, l = g / K;
+          const float dC = gw[k] * Y[l + 1];
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] += dC * s_wa[pp * R + r];
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) o_wb[r * Q + qq] = acc[r];
+      }
+    }
+    if constexpr (GEOM) {
+      float Jd[9];
+      dir_jacobian(nd, ninv, Jd);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dpw[j] += dd[0] * Jd[j] + dd[1] * Jd[3 + j] + dd[2] * Jd[6 + j];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) d_pws[3 * i + j] = dpw[j];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) d_rots[4 * i + j] = dq[j];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) d_scales[3 * i + j] = ds[j];
+    }
+  }
+  // parameter gradients: shared memory -> global, block span by block span
+  fence_proxy_async_shared();
+  __syncthreads();
+  write_rows<WS::W0>(d_w0, row0, n, sm + nt * BP::o_dw0);
+  if constexpr (MODE != GSB_WEIGHTS_FULL) {
+    write_rows<WS::WA>(d_wa, row0, n, sm + nt * BP::o_dwa);
+    write_rows<WS::WB>(d_wb, row0, n, sm + nt * BP::o_dwb);
+  }
+  if (threadIdx.x == 0) bulk_store_drain();
+}
+
+// ------------------------------------------------------------ dispatch
+template <typename Kern>
+static int set_smem(Kern kern, int smem) {
+  if (smem <= 48 * 1024) return GSB_OK;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return check_launch("render (shared memory attribute)", 0);
+  return GSB_OK;
+}
+
+template <int MODE, int K, int P, int Q, int R, typename T>
+static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
+  using WS = WRows<MODE, K, P, Q, R>;
+  const int smem = WS::IN * kFuseThreads * 4;
+  const int grid = div_up(f.n, kFuseThreads);
+  int rc;
+  if (!backward) {
+    auto kern = k_render_preprocess<MODE, K, P, Q, R, T>;
+    if ((rc = set_smem(kern, smem))) return rc;
+    kern<<<grid, kFuseThreads, smem, st>>>(
+        f.n, f.gx, f.gy, f.cam, f.pws, f.rots, f.scales, f.alphas, (const T*)f.w0,
+        (const T*)f.wa, (const T*)f.wb, f.st.records, f.st.rects, f.st.dkeys, f.st.counts,
+        f.st.block_sums, f.st.stats, f.depths_out);
+    return check_launch("render_preprocess");
+  }
+  const bool geom = f.g_u != nullptr;
+  auto kern = geom ? k_render_backward_pre<MODE, K, P, Q, R, T, true>
+                   : k_render_backward_pre<MODE, K, P, Q, R, T, false>;
+  const int bsmem = (geom ? BwdPlan<MODE, K, P, Q, R, true>::floats
+                          : BwdPlan<MODE, K, P, Q, R, false>::floats) * kFuseThreads * 4;
+  if ((rc = set_smem(kern, bsmem))) return rc;
+  kern<<<grid, kFuseThreads, bsmem, st>>>(f.n, f.cam, f.pws, f.rots, f.scales, (const T*)f.w0,
+                                          (const T*)f.wa, (const T*)f.wb, f.g_feat, f.g_u,
+                                          f.g_conic, f.d_pws, f.d_rots, f.d_scales, f.d_w0,
+                                          f.d_wa, f.d_wb);
+  return check_launch("render_backward");
+}
+
+template <typename T>
+static int dispatch_fused(int mode, int K, int P, int Q, int R, const FusedArgs& f, bool bwd,
+                          cudaStream_t st) {
+  if (mode == GSB_WEIGHTS_FULL) {
+    switch (K) {
+      case 3: return launch_fused<GSB_WEIGHTS_FULL, 3, 0, 0, 0, T>(f, bwd, st);
+      case 4: return launch_fused<GSB_WEIGHTS_FULL, 4, 0, 0, 0, T>(f, bwd, st);
+      case 5: return launch_fused<GSB_WEIGHTS_FULL, 5, 0, 0, 0, T>(f, bwd, st);
+      case 6: return launch_fused<GSB_WEIGHTS_FULL, 6, 0, 0, 0, T>(f, bwd, st);
+      case 7: return launch_fused<GSB_WEIGHTS_FULL, 7, 0, 0, 0, T>(f, bwd, st);
+      case 8: return launch_fused<GSB_WEIGHTS_FULL, 8, 0, 0, 0, T>(f, bwd, st);
+      default: break;
+    }
+  } else {
+#define GSB_FL(KK, PP, QQ, RR)                   \
+  if (K == KK && P == PP && Q == QQ && R == RR) \
+    return launch_fused<GSB_WEIGHTS_LOWRANK, KK, PP, QQ, RR, T>(f, bwd, st);
+    GSB_FL(5, 5, 15, 1) GSB_FL(5, 5, 15, 2) GSB_FL(5, 5, 15, 3) GSB_FL(5, 5, 15, 4)
+    GSB_FL(3, 3, 15, 1) GSB_FL(4, 4, 15, 1) GSB_FL(6, 6, 15, 1) GSB_FL(6, 6, 15, 3)
+#undef GSB_FL
+  }
+  set_error("render: unsupported palette parameter shape (mode %d, K=%d, P=%d, Q=%d, rank=%d)",
+            mode, K, P, Q, R);
+  return GSB_ERR_UNSUPPORTED;
+}
+
+int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedArgs& f, bool bwd,
+                  cudaStream_t st) {
+  if (f.n == 0) return GSB_OK;
+  return dtype == GSB_DTYPE_BF16 ? dispatch_fused<__nv_bfloat16>(mode, K, P, Q, R, f, bwd, st)
+                                 : dispatch_fused<float>(mode, K, P, Q, R, f, bwd, st);
+}
+
+int fused_status(uint32_t* out, bool clear, cudaStream_t st) {
+  if (cudaMemcpyFromSymbolAsync(out, g_fused_status, sizeof(uint32_t), 0, cudaMemcpyDeviceToHost,
+                                st) != cudaSuccess)
+    return check_launch("device_status", 0);
+  if (clear) {
+    const uint32_t zero = 0;
+    if (cudaMemcpyToSymbolAsync(g_fused_status, &zero, sizeof(uint32_t), 0,
+                                cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return check_launch("device_status", 0);
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("device_status", 0);
+  return GSB_OK;
+}
+
+}  // namespace gsb

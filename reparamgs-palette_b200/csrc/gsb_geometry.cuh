@@ -266,6 +266,149 @@ __device__ __forceinline__ void sh_basis_grad(const float* dir, int nb, bool ref
   G[3 * 15 + 1] = 6.f * SH_C3_0 * x * y;
 }
 
+// Palette weights from full SH coefficients c[l*K + k] (band-major; nb
+// bands in {1,4,9,16}): acc_k = sum_l Y_l c[l*K + k], summed band by band as
+// the reference groups its sums (gsplatcu/kernel.cu:694-710).  `load(idx)`
+// returns coefficient idx as float.
+template <int K, typename Loader>
+__device__ __forceinline__ void sh_weights_full(Loader load, int nb, const float* Y, float* acc) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = Y[0] * load(k);
+  // band-by-band accumulation, as the reference groups its sums
+  if (nb > 1) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      acc[k] += Y[1] * load(K + k) + Y[2] * load(2 * K + k) + Y[3] * load(3 * K + k);
+    if (nb > 4) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        acc[k] += Y[4] * load(4 * K + k) + Y[5] * load(5 * K + k) + Y[6] * load(6 * K + k) +
+                  Y[7] * load(7 * K + k) + Y[8] * load(8 * K + k);
+      if (nb > 9) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          acc[k] += Y[9] * load(9 * K + k) + Y[10] * load(10 * K + k) +
+                    Y[11] * load(11 * K + k) + Y[12] * load(12 * K + k) +
+                    Y[13] * load(13 * K + k) + Y[14] * load(14 * K + k) +
+                    Y[15] * load(15 * K + k);
+      }
+    }
+  }
+}
+
+// Rank-R low-rank weights (sh2Weight_fast generalised, gsplatcu/kernel.cu:884-987):
+// w_k = C0 dc_k + sum_l C[g/Q][g%Q] Y_{l+1}, g = l*K + k, C = A B with
+// a = A [P,R] and b = B [R,Q] row-major.  Summation order fixed: each
+// coefficient over r, then over l, then added to the DC term.
+template <int K, int P, int Q, int R>
+__device__ __forceinline__ void lowrank_weights(const float* dc, const float* a, const float* b,
+                                                const float* Y, float* wk) {
+  constexpr int L = P * Q / K;
+#pragma unroll
+  for (int k = 0; k < K; ++k) wk[k] = SH_C0 * dc[k];
+  if (L > 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float acc = 0.f;
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        const int g = l * K + k, row = g / Q, col = g % Q;
+        float coef = a[row * R] * b[col];
+#pragma unroll
+        for (int r = 1; r < R; ++r) coef += a[row * R + r] * b[r * Q + col];
+        acc += coef * Y[l + 1];
+      }
+      wk[k] += acc;
+    }
+  }
+}
+
+// ------------------------------------------------------------ Jacobians
+// d Sigma_(rc) / d q_j and / d s_j for Sigma = M M^T, M = R(q) diag(s).
+__device__ __forceinline__ void cov3d_jacobians(float4 q, float3 s, const float* M,
+                                                const float* R, float* dq /*6x4*/,
+                                                float* ds /*6x3*/) {
+  const float w = q.x, x = q.y, y = q.z, z = q.w;
+  // dR_ab / dq_j (rows a*3+b)
+  const float dR[9][4] = {{0.f, 0.f, -4.f * y, -4.f * z},
+                          {-2.f * z, 2.f * y, 2.f * x, -2.f * w},
+                          {2.f * y, 2.f * z, 2.f * w, 2.f * x},
+                          {2.f * z, 2.f * y, 2.f * x, 2.f * w},
+                          {0.f, -4.f * x, 0.f, -4.f * z},
+                          {-2.f * x, -2.f * w, 2.f * z, 2.f * y},
+                          {-2.f * y, 2.f * z, -2.f * w, 2.f * x},
+                          {2.f * x, 2.f * w, 2.f * z, 2.f * y},
+                          {0.f, -4.f * x, -4.f * y, 0.f}};
+  const float sv[3] = {s.x, s.y, s.z};
+  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+  for (int u = 0; u < 6; ++u) {
+    const int r = sym[u][0], c = sym[u][1];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float acc = 0.f;
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        acc += (M[3 * c + b] * dR[3 * r + b][j] + M[3 * r + b] * dR[3 * c + b][j]) * sv[b];
+      dq[4 * u + j] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) ds[3 * u + j] = M[3 * c + j] * R[3 * r + j] + M[3 * r + j] * R[3 * c + j];
+  }
+}
+
+// Jacobians of cov2d = (Sigma'_00 + .3, Sigma'_01, Sigma'_11 + .3) w.r.t. the 6
+// unique entries of Sigma and the camera-space centre (clamp not
+// differentiated, as in the reference).  M = J Rcw.
+__device__ __forceinline__ void cov2d_jacobians(const float* cov3, const float* M, const float* Rcw,
+                                                float x, float y, float z, float fx, float fy,
+                                                float* d3 /*3x6*/, float* dp /*3x3*/) {
+  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  const int out[3][2] = {{0, 0}, {0, 1}, {1, 1}};
+#pragma unroll
+  for (int o = 0; o < 3; ++o)
+#pragma unroll
+    for (int u = 0; u < 6; ++u) {
+      const int a = out[o][0], b = out[o][1], k = sym[u][0], l = sym[u][1];
+      float v = M[3 * a + k] * M[3 * b + l];
+      if (k != l) v += M[3 * a + l] * M[3 * b + k];
+      d3[6 * o + u] = v;
+    }
+  const float S[9] = {cov3[0], cov3[1], cov3[2], cov3[1], cov3[3], cov3[4], cov3[2], cov3[4], cov3[5]};
+  float dm[3][6];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float sm0 = S[3 * c] * M[0] + S[3 * c + 1] * M[1] + S[3 * c + 2] * M[2];
+    const float sm1 = S[3 * c] * M[3] + S[3 * c + 1] * M[4] + S[3 * c + 2] * M[5];
+    dm[0][c] = 2.f * sm0;
+    dm[0][3 + c] = 0.f;
+    dm[1][c] = sm1;
+    dm[1][3 + c] = sm0;
+    dm[2][c] = 0.f;
+    dm[2][3 + c] = 2.f * sm1;
+  }
+  const float zi2 = 1.f / (z * z), zi3 = zi2 / z;
+  float dmp[6][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    dmp[c][0] = -fx * Rcw[6 + c] * zi2;
+    dmp[c][1] = 0.f;
+    dmp[c][2] = -fx * Rcw[c] * zi2 + 2.f * fx * Rcw[6 + c] * x * zi3;
+    dmp[3 + c][0] = 0.f;
+    dmp[3 + c][1] = -fy * Rcw[6 + c] * zi2;
+    dmp[3 + c][2] = -fy * Rcw[3 + c] * zi2 + 2.f * fy * Rcw[6 + c] * y * zi3;
+  }
+#pragma unroll
+  for (int o = 0; o < 3; ++o)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float acc = 0.f;
+#pragma unroll
+      for (int m = 0; m < 6; ++m) acc += dm[o][m] * dmp[m][j];
+      dp[3 * o + j] = acc;
+    }
+}
+
 // d dir / d pw = I/|d| - d d^T/|d|^3 (symmetric 3x3).
 __device__ __forceinline__ void dir_jacobian(const float* nd, float ninv, float* J) {
   const float n3 = ninv * ninv * ninv;

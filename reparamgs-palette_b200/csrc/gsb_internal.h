@@ -48,7 +48,8 @@ struct SplatState {
 };
 constexpr int kBinBlock = 256;      // Gaussians per binning block
 constexpr int kRadixBits = 9;                  // digit width of one radix pass
-constexpr int kRadixBins = 1 << kRadixBits;int record_vec4(int channels);
+constexpr int kRadixBins = 1 << kRadixBits;  // digits per pass
+int record_vec4(int channels);
 size_t splat_state_bytes(int64_t n, int channels, int H, int W);
 SplatState carve_state(void* base, int64_t n, int channels, int H, int W);
 
@@ -76,5 +77,28 @@ int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* r
                          const int32_t* gsid, const SplatState& s, const int32_t* contrib,
                          const float* final_tau, const float* dout, const float* dtau,
                          float* dfeat, float* dalpha, float* du, float* dconic, cudaStream_t st);
+
+
+// fused.cu -- per-Gaussian preprocess and its adjoint in one kernel each.
+struct CamArgs {
+  const float* R;  // device [3,3] Rcw
+  const float* t;  // device [3] tcw
+  const float* c;  // device [3] twc
+  float fx, fy, cx, cy, tanx, tany;
+};
+struct FusedArgs {
+  int64_t n;
+  uint32_t gx, gy;
+  CamArgs cam;
+  const float *pws, *rots, *scales, *alphas;
+  const void *w0, *wa, *wb;  // shs or dc; A; B (storage dtype)
+  SplatState st;             // forward: filled like gsb_splat_pack + count
+  float* depths_out;         // forward, may be null
+  const float *g_feat, *g_u, *g_conic;  // backward: screen-space gradients (g_u null: weights only)
+  float *d_pws, *d_rots, *d_scales, *d_w0, *d_wa, *d_wb;
+};
+int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedArgs& f, bool backward,
+                  cudaStream_t st);
+int fused_status(uint32_t* out, bool clear, cudaStream_t st);
 
 }  // namespace gsb

@@ -7,6 +7,7 @@
 #pragma once
 
 #include "gsb_common.cuh"
+#include "gsb_stage.cuh"
 
 namespace gsb {
 
@@ -79,6 +80,21 @@ __device__ __forceinline__ void fence_proxy_async_shared() {
 
 __device__ __forceinline__ bool aligned16(const void* p) {
   return ((uintptr_t)p & 15u) == 0;
+}
+
+// Copies the block's rows of one input array into shared memory: a bulk copy
+// when `bulk` (issued by thread 0, counted on `bar`), else a batched
+// per-thread copy.  Returns the bytes the bulk copy will deliver.
+template <int ROWLEN, typename T>
+__device__ __forceinline__ uint32_t stage_rows(const T* g, int64_t row0, int64_t n, float* s,
+                                               bool bulk, uint64_t* bar) {
+  if (bulk) {
+    const uint32_t bytes = (uint32_t)(blockDim.x * ROWLEN * sizeof(float));
+    if (threadIdx.x == 0) bulk_load(s, g + row0 * ROWLEN, bytes, bar);
+    return bytes;
+  }
+  stage_in_plain<ROWLEN>(g, row0, n, s);
+  return 0;
 }
 
 }  // namespace gsb

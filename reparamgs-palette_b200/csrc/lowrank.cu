@@ -41,21 +41,6 @@ struct LrSmem {
   static constexpr int bwd_floats = P * R + R * Q + LL + K + P * R + R * Q;
 };
 
-// Copies the block's rows of one input array into shared memory: a bulk copy
-// when `bulk` (issued by thread 0, counted on `bar`), else a batched
-// per-thread copy.  Returns the bytes the bulk copy will deliver.
-template <int ROWLEN, typename T>
-__device__ __forceinline__ uint32_t stage_rows(const T* g, int64_t row0, int64_t n, float* s,
-                                               bool bulk, uint64_t* bar) {
-  if (bulk) {
-    const uint32_t bytes = (uint32_t)(blockDim.x * ROWLEN * sizeof(float));
-    if (threadIdx.x == 0) bulk_load(s, g + row0 * ROWLEN, bytes, bar);
-    return bytes;
-  }
-  stage_in_plain<ROWLEN>(g, row0, n, s);
-  return 0;
-}
-
 template <int K, int P, int Q, int R, typename T>
 __global__ void __launch_bounds__(kLrThreads)
     k_lowrank_fixed(int64_t n, const T* __restrict__ dc, const T* __restrict__ A,
@@ -94,36 +79,18 @@ __global__ void __launch_bounds__(kLrThreads)
   }
   const int t = threadIdx.x;
   if (row0 + t < n) {
-    float wk[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) wk[k] = SH_C0 * s_dc[t * K + k];
+    float wk[K], Y[16];
+    Y[0] = SH_C0;
     if (L > 0) {
-      float a[PR], b[RQ];
-#pragma unroll
-      for (int j = 0; j < PR; ++j) a[j] = s_a[t * PR + j];
-#pragma unroll
-      for (int j = 0; j < RQ; ++j) b[j] = s_b[t * RQ + j];
-      float dir[3], Y[16];
+      float dir[3];
       const float3 pw = make_float3(s_p[t * 3], s_p[t * 3 + 1], s_p[t * 3 + 2]);
       const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
       view_direction(pw, cam, dir, nullptr, nullptr);
       sh_basis(dir, L + 1, Y);
 #pragma unroll
       for (int l = 0; l < L; ++l) s_y[t * S::LL + l] = Y[l + 1];
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        float acc = 0.f;
-#pragma unroll
-        for (int l = 0; l < L; ++l) {
-          const int g = l * K + k, row = g / Q, col = g % Q;
-          float coef = a[row * R] * b[col];
-#pragma unroll
-          for (int r = 1; r < R; ++r) coef += a[row * R + r] * b[r * Q + col];
-          acc += coef * Y[l + 1];
-        }
-        wk[k] += acc;
-      }
     }
+    lowrank_weights<K, P, Q, R>(s_dc + t * K, s_a + t * PR, s_b + t * RQ, Y, wk);
 #pragma unroll
     for (int k = 0; k < K; ++k) s_w[t * K + k] = wk[k];
   }

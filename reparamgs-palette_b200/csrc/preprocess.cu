@@ -51,39 +51,6 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// d Sigma_(rc) / d q_j and / d s_j for Sigma = M M^T, M = R(q) diag(s).
-__device__ __forceinline__ void cov3d_jacobians(float4 q, float3 s, const float* M,
-                                                const float* R, float* dq /*6x4*/,
-                                                float* ds /*6x3*/) {
-  const float w = q.x, x = q.y, y = q.z, z = q.w;
-  // dR_ab / dq_j (rows a*3+b)
-  const float dR[9][4] = {{0.f, 0.f, -4.f * y, -4.f * z},
-                          {-2.f * z, 2.f * y, 2.f * x, -2.f * w},
-                          {2.f * y, 2.f * z, 2.f * w, 2.f * x},
-                          {2.f * z, 2.f * y, 2.f * x, 2.f * w},
-                          {0.f, -4.f * x, 0.f, -4.f * z},
-                          {-2.f * x, -2.f * w, 2.f * z, 2.f * y},
-                          {-2.f * y, 2.f * z, -2.f * w, 2.f * x},
-                          {2.f * x, 2.f * w, 2.f * z, 2.f * y},
-                          {0.f, -4.f * x, -4.f * y, 0.f}};
-  const float sv[3] = {s.x, s.y, s.z};
-  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-#pragma unroll
-  for (int u = 0; u < 6; ++u) {
-    const int r = sym[u][0], c = sym[u][1];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      float acc = 0.f;
-#pragma unroll
-      for (int b = 0; b < 3; ++b)
-        acc += (M[3 * c + b] * dR[3 * r + b][j] + M[3 * r + b] * dR[3 * c + b][j]) * sv[b];
-      dq[4 * u + j] = acc;
-    }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) ds[3 * u + j] = M[3 * c + j] * R[3 * r + j] + M[3 * r + j] * R[3 * c + j];
-  }
-}
-
 // computeCov3D -- gsplatcu/kernel.cu:422-501.
 __global__ void __launch_bounds__(kThreads)
     k_cov3d(int64_t n, const float4* __restrict__ rots, const float* __restrict__ scales,
@@ -114,58 +81,6 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int k = 0; k < 18; ++k) ds[18 * i + k] = js[k];
   }
-}
-
-// Jacobians of cov2d = (Sigma'_00 + .3, Sigma'_01, Sigma'_11 + .3) w.r.t. the 6
-// unique entries of Sigma and the camera-space centre (clamp not
-// differentiated, as in the reference).  M = J Rcw.
-__device__ __forceinline__ void cov2d_jacobians(const float* cov3, const float* M, const float* Rcw,
-                                                float x, float y, float z, float fx, float fy,
-                                                float* d3 /*3x6*/, float* dp /*3x3*/) {
-  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-  const int out[3][2] = {{0, 0}, {0, 1}, {1, 1}};
-#pragma unroll
-  for (int o = 0; o < 3; ++o)
-#pragma unroll
-    for (int u = 0; u < 6; ++u) {
-      const int a = out[o][0], b = out[o][1], k = sym[u][0], l = sym[u][1];
-      float v = M[3 * a + k] * M[3 * b + l];
-      if (k != l) v += M[3 * a + l] * M[3 * b + k];
-      d3[6 * o + u] = v;
-    }
-  const float S[9] = {cov3[0], cov3[1], cov3[2], cov3[1], cov3[3], cov3[4], cov3[2], cov3[4], cov3[5]};
-  float dm[3][6];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const float sm0 = S[3 * c] * M[0] + S[3 * c + 1] * M[1] + S[3 * c + 2] * M[2];
-    const float sm1 = S[3 * c] * M[3] + S[3 * c + 1] * M[4] + S[3 * c + 2] * M[5];
-    dm[0][c] = 2.f * sm0;
-    dm[0][3 + c] = 0.f;
-    dm[1][c] = sm1;
-    dm[1][3 + c] = sm0;
-    dm[2][c] = 0.f;
-    dm[2][3 + c] = 2.f * sm1;
-  }
-  const float zi2 = 1.f / (z * z), zi3 = zi2 / z;
-  float dmp[6][3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    dmp[c][0] = -fx * Rcw[6 + c] * zi2;
-    dmp[c][1] = 0.f;
-    dmp[c][2] = -fx * Rcw[c] * zi2 + 2.f * fx * Rcw[6 + c] * x * zi3;
-    dmp[3 + c][0] = 0.f;
-    dmp[3 + c][1] = -fy * Rcw[6 + c] * zi2;
-    dmp[3 + c][2] = -fy * Rcw[3 + c] * zi2 + 2.f * fy * Rcw[6 + c] * y * zi3;
-  }
-#pragma unroll
-  for (int o = 0; o < 3; ++o)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float acc = 0.f;
-#pragma unroll
-      for (int m = 0; m < 6; ++m) acc += dm[o][m] * dmp[m][j];
-      dp[3 * o + j] = acc;
-    }
 }
 
 // computeCov2D -- gsplatcu/kernel.cu:508-611.
@@ -263,28 +178,7 @@ __global__ void __launch_bounds__(kThreads)
   }
   sh_basis(dir, nb, Y);
   float acc[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) acc[k] = Y[0] * ld(c, k);
-  // band-by-band accumulation, as the reference groups its sums
-  if (nb > 1) {
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      acc[k] += Y[1] * ld(c, K + k) + Y[2] * ld(c, 2 * K + k) + Y[3] * ld(c, 3 * K + k);
-    if (nb > 4) {
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-        acc[k] += Y[4] * ld(c, 4 * K + k) + Y[5] * ld(c, 5 * K + k) + Y[6] * ld(c, 6 * K + k) +
-                  Y[7] * ld(c, 7 * K + k) + Y[8] * ld(c, 8 * K + k);
-      if (nb > 9) {
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-          acc[k] += Y[9] * ld(c, 9 * K + k) + Y[10] * ld(c, 10 * K + k) +
-                    Y[11] * ld(c, 11 * K + k) + Y[12] * ld(c, 12 * K + k) +
-                    Y[13] * ld(c, 13 * K + k) + Y[14] * ld(c, 14 * K + k) +
-                    Y[15] * ld(c, 15 * K + k);
-      }
-    }
-  }
+  sh_weights_full<K>([&](int idx) { return ld(c, idx); }, nb, Y, acc);
 #pragma unroll
   for (int k = 0; k < K; ++k) feat[i * K + k] = acc[k];
   if (dshs) {

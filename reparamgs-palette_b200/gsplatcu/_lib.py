@@ -21,6 +21,8 @@ GSB_ERR_DEVICE_TIMEOUT = 5
 DTYPE_F32 = 0
 DTYPE_BF16 = 1
 MAX_CHANNELS = 8
+WEIGHTS_FULL = 0
+WEIGHTS_LOWRANK = 1
 
 _i64, _i32, _u32, _f32, _p, _sz = C.c_int64, C.c_int, C.c_uint32, C.c_float, C.c_void_p, C.c_size_t
 
@@ -54,6 +56,10 @@ _SIGS = {
     "gsb_palette_l1": (_i32, [_i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_splat_backward_packed": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p,
                                          _p, _p, _p, _p]),
+    "gsb_render_preprocess": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "gsb_render_backward_bytes": (_sz, [_i64, _i32]),
+    "gsb_render_backward": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
+                                   _p, _p, _p, _p, _p, _p, _p, _p]),
 }
 
 _lib = None
@@ -63,6 +69,20 @@ class SplatPlan(C.Structure):
     """gsb_splat_plan: sizes gsb_splat_counts reads back for the sort step."""
     _fields_ = [("patches", C.c_int64), ("max_depth_key", C.c_uint32),
                 ("reserved", C.c_uint32)]
+
+
+class Camera(C.Structure):
+    """gsb_camera: device pointers to Rcw [3,3], tcw [3], twc [3]; intrinsics."""
+    _fields_ = [("Rcw", C.c_void_p), ("tcw", C.c_void_p), ("twc", C.c_void_p),
+                ("fx", C.c_float), ("fy", C.c_float), ("cx", C.c_float), ("cy", C.c_float),
+                ("width", C.c_int), ("height", C.c_int)]
+
+
+class PaletteParams(C.Structure):
+    """gsb_palette_params: weight mode, storage dtype, shape and device pointers."""
+    _fields_ = [("mode", C.c_int), ("dtype", C.c_int), ("K", C.c_int), ("P", C.c_int),
+                ("Q", C.c_int), ("rank", C.c_int), ("w0", C.c_void_p), ("A", C.c_void_p),
+                ("B", C.c_void_p)]
 
 
 class GsplatError(RuntimeError):

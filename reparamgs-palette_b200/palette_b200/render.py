@@ -1,0 +1,158 @@
+"""Fused palette-weight rendering with the full adjoint.
+
+``render_palette(pws, rots, scales, alphas, cam, shs=... | dc=..., A=..., B=...)``
+renders one view and returns ``(layer [K,H,W], final_tau [H,W], depths [N])``.
+The forward runs the per-Gaussian work of project / computeCov3D /
+computeCov2D / sh2Weight(_fast) / inverseCov2D in one kernel and then the same
+binning and compositing as ``gsplatcu.splat_weight``; it computes what the
+reference operator sequence computes (gsplat/gsmodel.py:107-118, 155-170),
+with ``depths`` the reference's depths after its in-place updates
+(``depths > 0.2`` is the visibility mask ``WeightGSFunctionTest`` returns).
+
+Unlike the reference's backward, which only differentiates the weights, the
+backward here returns gradients for every input that requires one: means,
+rotations, scales, opacities and the weight parameters (full ``shs [N,16K]``
+or low-rank ``dc [N,K], A [N,P,r], B [N,r,Q]``), including the
+final-transmittance term when ``final_tau`` feeds the loss.  When no geometry
+input requires a gradient only the weight gradients are computed.  Weight
+parameters may be bfloat16 (FP32 arithmetic; gradients are returned in the
+parameter's dtype).
+"""
+import ctypes as C
+
+import torch
+
+from gsplatcu import _lib
+
+_F32 = torch.float32
+
+
+def camera_struct(cam):
+    """(gsb_camera, tensors to keep alive) for a camera-like object."""
+    Rcw = cam.Rcw.to(_F32).contiguous()
+    tcw = cam.tcw.to(_F32).contiguous().reshape(-1)
+    twc = cam.twc.to(_F32).contiguous().reshape(-1)
+    c = _lib.Camera(Rcw.data_ptr(), tcw.data_ptr(), twc.data_ptr(), float(cam.fx), float(cam.fy),
+                    float(cam.cx), float(cam.cy), int(cam.width), int(cam.height))
+    return c, (Rcw, tcw, twc)
+
+
+def _params(mode, K, P, Q, rank, w0, A, B):
+    return _lib.PaletteParams(mode, _lib.DTYPE_BF16 if w0.dtype == torch.bfloat16 else
+                              _lib.DTYPE_F32, K, P, Q, rank, w0.data_ptr(),
+                              A.data_ptr() if A is not None else None,
+                              B.data_ptr() if B is not None else None)
+
+
+def _check(name, t, dtypes=(_F32,)):
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype in dtypes):
+        raise TypeError(f"render_palette: {name} must be a CUDA tensor of dtype {dtypes}")
+    return t.contiguous()
+
+
+class _RenderPalette(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank):
+        dev = pws.device
+        n = int(pws.shape[0])
+        H, W = int(cam.height), int(cam.width)
+        L = _lib.lib()
+        camst, keep = camera_struct(cam)
+        params = _params(mode, K, P, Q, rank, w0, A, B)
+        with torch.cuda.device(dev):
+            st = _lib.stream_of(pws)
+            state = torch.empty(int(L.gsb_splat_state_bytes(n, K, H, W)), dtype=torch.uint8,
+                                device=dev)
+            depths = torch.empty((n,), dtype=_F32, device=dev)
+            _lib.call("render_palette", "gsb_render_preprocess", n, C.byref(camst), _lib.ptr(pws),
+                      _lib.ptr(rots), _lib.ptr(scales), _lib.ptr(alphas), C.byref(params),
+                      _lib.ptr(state), _lib.ptr(depths), st)
+            gx, gy = (W + 15) // 16, (H + 15) // 16
+            ranges = torch.empty((gx * gy, 2), dtype=torch.int32, device=dev)
+            layer = torch.empty((K, H, W), dtype=_F32, device=dev)
+            contrib = torch.empty((H, W), dtype=torch.int32, device=dev)
+            final_tau = torch.empty((H, W), dtype=_F32, device=dev)
+            plan = _lib.SplatPlan()
+            _lib.call("render_palette", "gsb_splat_counts", n, H, W, _lib.ptr(state),
+                      C.byref(plan), st)
+            M = int(plan.patches)
+            ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan)))),
+                             dtype=torch.uint8, device=dev)
+            gsid = torch.empty((M,), dtype=torch.int32, device=dev)
+            _lib.call("render_palette", "gsb_splat_sort", n, H, W, C.byref(plan), _lib.ptr(state),
+                      _lib.ptr(ws), _lib.ptr(gsid), _lib.ptr(ranges), st)
+            _lib.call("render_palette", "gsb_splat_draw", n, H, W, K, _lib.ptr(ranges),
+                      _lib.ptr(gsid), _lib.ptr(state), 0.0, _lib.ptr(layer), _lib.ptr(contrib),
+                      _lib.ptr(final_tau), st)
+        ctx.meta = (cam, mode, K, P, Q, rank)
+        ctx.save_for_backward(pws, rots, scales, alphas, w0, A, B, state, ranges, gsid, contrib,
+                              final_tau)
+        ctx.mark_non_differentiable(depths)
+        return layer, final_tau, depths
+
+    @staticmethod
+    def backward(ctx, dlayer, dtau, _ddepths):
+        cam, mode, K, P, Q, rank = ctx.meta
+        (pws, rots, scales, alphas, w0, A, B, state, ranges, gsid, contrib,
+         final_tau) = ctx.saved_tensors
+        dev = pws.device
+        n = int(pws.shape[0])
+        camst, _keep = camera_struct(cam)
+        params = _params(mode, K, P, Q, rank, w0, A, B)
+        L = _lib.lib()
+        if dlayer is None:
+            dlayer = torch.zeros((K,) + tuple(final_tau.shape), dtype=_F32, device=dev)
+        dlayer = dlayer.contiguous()
+        dtau = dtau.contiguous() if dtau is not None else None
+        # geometry gradients only when a geometry input needs one (the
+        # reference's own backward differentiates the weights alone)
+        geom = any(ctx.needs_input_grad[:4])
+        e = (lambda *shape: torch.empty(shape, dtype=_F32, device=dev)) if geom else \
+            (lambda *shape: None)
+        with torch.cuda.device(dev):
+            scratch = torch.empty(int(L.gsb_render_backward_bytes(n, K)), dtype=torch.uint8,
+                                  device=dev)
+            dpws, drots, dscales, dalphas = e(n, 3), e(n, 4), e(n, 3), e(n)
+            dw0 = torch.empty(tuple(w0.shape), dtype=_F32, device=dev)
+            dA = torch.empty(tuple(A.shape), dtype=_F32, device=dev) if A is not None else None
+            dB = torch.empty(tuple(B.shape), dtype=_F32, device=dev) if B is not None else None
+            _lib.call("render_palette.backward", "gsb_render_backward", n, C.byref(camst),
+                      _lib.ptr(pws), _lib.ptr(rots), _lib.ptr(scales), _lib.ptr(alphas),
+                      C.byref(params), _lib.ptr(state), _lib.ptr(ranges), _lib.ptr(gsid),
+                      _lib.ptr(contrib), _lib.ptr(final_tau), _lib.ptr(dlayer), _lib.ptr(dtau),
+                      _lib.ptr(scratch), _lib.ptr(dpws), _lib.ptr(drots), _lib.ptr(dscales),
+                      _lib.ptr(dalphas), _lib.ptr(dw0), _lib.ptr(dA), _lib.ptr(dB),
+                      _lib.stream_of(pws))
+        if dalphas is not None:
+            dalphas = dalphas.reshape(alphas.shape)
+        cast = lambda g, like: None if g is None else g.to(like.dtype)
+        return (dpws, drots, dscales, dalphas, cast(dw0, w0), cast(dA, A), cast(dB, B),
+                None, None, None, None, None, None)
+
+
+def render_palette(pws, rots, scales, alphas, cam, shs=None, dc=None, A=None, B=None, K=None):
+    """Render palette weights for one camera.  Pass ``shs [N,16K]`` (full SH
+    order 3) or the low-rank ``dc [N,K], A [N,P,r] (or [N,P]), B [N,r,Q] (or
+    [N,Q])``.  Returns ``(layer [K,H,W], final_tau [H,W], depths [N])``."""
+    pws, rots, scales = _check("pws", pws), _check("rots", rots), _check("scales", scales)
+    alphas = _check("alphas", alphas)
+    wt = (torch.float32, torch.bfloat16)
+    if shs is not None:
+        shs = _check("shs", shs, wt)
+        K = int(K) if K is not None else int(shs.shape[1]) // 16
+        if int(shs.shape[1]) != 16 * K:
+            raise ValueError("render_palette: shs must be [N, 16*K] (SH order 3)")
+        return _RenderPalette.apply(pws, rots, scales, alphas, shs, None, None, cam,
+                                    _lib.WEIGHTS_FULL, K, 0, 0, 0)
+    if dc is None or A is None or B is None:
+        raise ValueError("render_palette: pass shs, or dc, A and B")
+    dc, A, B = _check("dc", dc, wt), _check("A", A, wt), _check("B", B, wt)
+    if not (dc.dtype == A.dtype == B.dtype):
+        raise TypeError("render_palette: dc, A and B must share a dtype")
+    K = int(dc.shape[1])
+    if A.dim() == 2:
+        P, rank, Q = int(A.shape[1]), 1, int(B.shape[1])
+    else:
+        P, rank, Q = int(A.shape[1]), int(A.shape[2]), int(B.shape[2])
+    return _RenderPalette.apply(pws, rots, scales, alphas, dc, A, B, cam, _lib.WEIGHTS_LOWRANK,
+                                K, P, Q, rank)
