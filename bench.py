@@ -54,6 +54,11 @@ def parse():
     ap.add_argument("--rank", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="length of the palette-edit serving stream (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=400.0)
+    ap.add_argument("--serve-scale", type=float, default=1.0,
+                    help="scale of the resident scene sizes (1: 100k..3M)")
     return ap.parse_args()
 
 
@@ -314,6 +319,86 @@ def stage_breakdown(wl, reps=5):
         return out, dict(M=M, visible=visible, bytes_draw=bytes_draw, bytes_bwd=bytes_bwd)
 
 
+# ------------------------------------------------------------------ serving
+SERVE_SIZES = (100_000, 250_000, 500_000, 1_000_000, 2_000_000, 3_000_000)
+SERVE_RES = ((1280, 720), (1920, 1080), (3840, 2160))
+
+
+def serve_bench(a, device):
+    """Palette-edit serving (palette_b200.serve): 12 resident scenes of
+    100k..3M Gaussians (two of each size; one with full SH weights in FP32,
+    one with rank-3 low-rank factors in BF16), an open-loop Poisson stream of
+    requests (random scene, camera on a sphere of radius 6..10, resolution
+    720p / 1080p / 4K, the 3 chromatic palette anchors perturbed by
+    N(0, 0.15) clipped to [0, 1]).  Latency = arrival to image complete in
+    HBM, camera and palette copied from pinned host memory per request."""
+    from palette_b200.scene import look_at, sphere_poses, synthetic_scene, to_torch
+    from palette_b200.serve import PaletteServer, Request, Scene
+    rng = np.random.default_rng(a.seed + 7)
+    scenes, palettes = [], {}
+    for j, size in enumerate(SERVE_SIZES):
+        n = max(1000, int(size * a.serve_scale))
+        for form in ("fp32_full", "bf16_lowrank"):
+            sid = f"{form}_{n}"
+            if form == "fp32_full":
+                sc = synthetic_scene(n, seed=100 + j, mode="full")
+                st = to_torch(sc, device, torch.float32)
+                scenes.append(Scene(sid, st["pws"], st["rots"], st["scales"], st["alphas"],
+                                    shs=st["shs"]))
+            else:
+                sc = synthetic_scene(n, seed=200 + j, mode="lowrank", rank=3)
+                st = to_torch(sc, device, torch.bfloat16)
+                scenes.append(Scene(sid, st["pws"], st["rots"], st["scales"], st["alphas"],
+                                    dc=st["dc"], A=st["A"], B=st["B"]))
+            palettes[sid] = sc["palette"]
+            del sc, st
+    res = []
+    for W, H in SERVE_RES:
+        c = look_at((0, -8, 0), width=W, height=H, device="cpu")
+        res.append((W, H, c.fx, c.fy, c.cx, c.cy))
+    probes = [(c.Rcw.numpy(), c.tcw.numpy()) for c in
+              (look_at(e, device="cpu") for e in sphere_poses(8, 6.0, seed=3))]
+    free, _ = torch.cuda.mem_get_info(device)
+    srv = PaletteServer(hbm_budget=int(0.8 * free), slots=4, device=device, keep_images=False)
+    t0 = time.perf_counter()
+    for sc in scenes:
+        if not srv.admit_scene(sc, res, probes):
+            raise RuntimeError(f"serving: scene {sc.id} does not fit the HBM budget")
+    admit_s = time.perf_counter() - t0
+    nreq = max(1, int(a.serve_rate * a.serve_seconds))
+    eyes = sphere_poses(nreq, (6.0, 10.0), seed=a.seed + 11)
+    reqs = []
+    for i in range(nreq):
+        sc = scenes[int(rng.integers(len(scenes)))]
+        W, H, fx, fy, cx, cy = res[int(rng.integers(len(res)))]
+        cam = look_at(eyes[i], width=W, height=H, device="cpu")
+        pal = np.array(palettes[sc.id], np.float32)
+        pal[2:] = np.clip(pal[2:] + rng.normal(0, 0.15, pal[2:].shape), 0, 1)
+        reqs.append(Request(sc.id, cam.Rcw.numpy(), cam.tcw.numpy(), fx, fy, cx, cy, W, H, pal,
+                            tag=("bf16" if sc.id.startswith("bf16") else "fp32", W)))
+    t1 = time.perf_counter()
+    srv.prepare(reqs)
+    prep_s = time.perf_counter() - t1
+    st = srv.run_open_loop(reqs, rate=a.serve_rate, seed=a.seed)
+    lat = {}
+    for r in srv.done:
+        for key in (r.tag[0], f"{r.tag[1]}px"):
+            lat.setdefault(key, []).append((r.done - r.arrival) * 1000.0)
+    st["by_form"] = {k: dict(n=len(v), p50_ms=round(float(np.percentile(v, 50)), 3),
+                             p99_ms=round(float(np.percentile(v, 99)), 3))
+                     for k, v in sorted(lat.items())}
+    st.update(scenes=len(scenes), gaussians=int(sum(s.n for s in scenes)),
+              resident_gb=round(srv.resident_bytes() / 1e9, 2), slots=len(srv.slots),
+              graphs=srv.graph_captures, seconds=a.serve_seconds, admit_s=round(admit_s, 1),
+              capture_s=round(prep_s, 1),
+              latency="arrival to image complete in HBM; camera/palette H2D per request")
+    for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "frames_per_s"):
+        st[k] = round(st[k], 3)
+    del srv, scenes
+    torch.cuda.empty_cache()
+    return st
+
+
 # ----------------------------------------------------------- CPU baseline
 def cpu_step(wl, orc, stride):
     """One bounded sample of the step on the host cores (CPU oracle, FP32):
@@ -471,6 +556,8 @@ def run_b200(a):
                 peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s")
 
+    serving = serve_bench(a, device) if a.serve_seconds > 0 else None
+
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cb = cpu_baseline(wl, steps=8, warmup=1)
@@ -488,6 +575,7 @@ def run_b200(a):
                     fused_path=dict(iters_per_s=round(world * 1000.0 / fu_ms, 3),
                                     ms_per_step=round(fu_ms, 4), forward_ms=round(fu_fms, 4),
                                     frames_per_s=round(world * 1000.0 / fu_fms, 2)),
+                    serving=serving,
                     stages_ms={k: round(v, 4) for k, v in stages.items()},
                     patches=alg["M"])
         print(json.dumps(line), flush=True)

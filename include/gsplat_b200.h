@@ -49,6 +49,9 @@ int gsb_version(void);
  * up and the kernel returned without results.  Synchronises `stream`;
  * clears the word when `clear` is non-zero. */
 #define GSB_STATUS_BULK_TIMEOUT 1u
+/* Bits gsb_splat_sort_capacity writes to its status word. */
+#define GSB_STATUS_PATCH_OVERFLOW 2u     /* more patches than the capacity       */
+#define GSB_STATUS_DEPTH_KEY_OVERFLOW 4u /* a depth key above max_depth_key      */
 int gsb_device_status(uint32_t* status, int clear, void* stream);
 /* Number of kernels this library has launched in the process so far
  * (diagnostic; used to report how many of the library's kernels a timed
@@ -183,6 +186,24 @@ int gsb_splat_sort_static(int64_t n, int height, int width, const gsb_splat_plan
                           const void* state, int32_t* gsid_out, int32_t* ranges_out,
                           void* stream);
 
+/* Step 3 without the host read-back of step 2, for callers that keep the
+ * whole render on the device (CUDA-graph capture, serving): the sort is
+ * sized for `patch_capacity` patches and depth keys up to `max_depth_key`
+ * (uint32(depth*1000)); the true patch count stays on the device.  Needs
+ * `sort_ws` of gsb_splat_sort_capacity_bytes(...) bytes and gsid_out of
+ * patch_capacity entries.  *status (device memory) receives
+ * GSB_STATUS_PATCH_OVERFLOW / GSB_STATUS_DEPTH_KEY_OVERFLOW or 0; on an
+ * overflow every range is left empty (the image then shows nothing) and the
+ * caller re-renders with a larger capacity.  Without overflow the results
+ * equal gsb_splat_sort's.  No counterpart in the reference, which always
+ * reads the patch count back (gsplatcu/gausplat.cu:199-201). */
+size_t gsb_splat_sort_capacity_bytes(int64_t n, int height, int width, int64_t patch_capacity,
+                                     uint32_t max_depth_key);
+int gsb_splat_sort_capacity(int64_t n, int height, int width, int64_t patch_capacity,
+                            uint32_t max_depth_key, const void* state, void* sort_ws,
+                            int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
+                            void* stream);
+
 /* out [channels,H,W], contrib [H,W] (1-based index of the last blended
  * Gaussian in the tile list), final_tau [H,W].  Pixels of tiles without
  * patches are set to 0 / 0 / tau_init (0 for weights, 1 for colours, as
@@ -258,10 +279,16 @@ typedef struct gsb_palette_params {
   const void* w0; /* full: shs [n,16K]; low-rank: dc [n,K]               */
   const void* A;  /* low-rank: [n,P,rank]                                 */
   const void* B;  /* low-rank: [n,rank,Q]                                 */
+  const float* palette; /* NULL: records carry the K weights.  Else device
+                         * [K,3] RGB palette: records carry each Gaussian's
+                         * colour sum_k w_k palette[k] (3 channels; state of
+                         * gsb_splat_state_bytes(n, 3, H, W)), the palette-edit
+                         * render of gsplat/gsmodel.py:488-509 + 14-26. */
 } gsb_palette_params;
 
 /* pws [n,3], rots [n,4] (w,x,y,z), scales [n,3], alphas [n]; `state` of
- * gsb_splat_state_bytes(n, K, height, width) bytes, 256-byte aligned;
+ * gsb_splat_state_bytes(n, K (3 with a palette), height, width) bytes,
+ * 256-byte aligned;
  * depths_out [n] (may be NULL) receives the camera depth, or -1 for
  * Gaussians dropped by the depth, conic or tile tests (the reference's
  * depths after its in-place updates).  Supported shapes: full K in 3..8;

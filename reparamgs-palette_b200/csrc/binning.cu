@@ -203,6 +203,23 @@ __device__ __forceinline__ KT make_key(uint32_t tile, uint32_t dk, int dkey_bits
   return dkey_bits >= (int)(8 * sizeof(KT)) ? (KT)dk : (((KT)tile << dkey_bits) | (KT)dk);
 }
 
+// Patch count the sort kernels work on.  `mdev` null: the host-known count
+// M.  Otherwise (capacity path, no host read-back) M is a capacity and the
+// true count is the device total in mdev (stats words 0 and 3); a count
+// above the capacity, or a depth key wider than `dkey_bits`, is an overflow:
+// the kernels then stay inside the capacity and k_ranges leaves every range
+// empty, so nothing downstream reads the unsorted entries.
+__device__ __forceinline__ int64_t device_patches(int64_t M, const uint32_t* mdev) {
+  if (!mdev) return M;
+  const uint64_t m = (uint64_t)mdev[0] | ((uint64_t)mdev[3] << 32);
+  return m > (uint64_t)M ? M : (int64_t)m;
+}
+__device__ __forceinline__ bool capacity_overflow(int64_t M, const uint32_t* mdev, int dkey_bits) {
+  if (!mdev) return false;
+  const uint64_t m = (uint64_t)mdev[0] | ((uint64_t)mdev[3] << 32);
+  return m > (uint64_t)M || (dkey_bits < 32 && (mdev[1] >> dkey_bits) != 0u);
+}
+
 // ------------------------------------------------------------------ emit
 // Key emission (createKeys, gsplatcu/kernel.cu:96-124) done cooperatively by
 // each warp: the warp's 32 Gaussians own one contiguous run of patch slots,
@@ -213,7 +230,7 @@ __global__ void __launch_bounds__(kBinBlock)
     k_emit(int64_t n, uint32_t gx, int dkey_bits, const uint2* __restrict__ rects,
            const uint32_t* __restrict__ dkeys, const uint32_t* __restrict__ counts,
            const uint32_t* __restrict__ block_offs, KT* __restrict__ keys,
-           int32_t* __restrict__ vals) {
+           int32_t* __restrict__ vals, int64_t cap) {
   __shared__ uint32_t warp_tot[8];
   __shared__ uint32_t s_incl[8][32];
   __shared__ uint2 s_rect[8][32];
@@ -248,6 +265,7 @@ __global__ void __launch_bounds__(kBinBlock)
     const uint32_t ty = local / wdt, tx = local - ty * wdt;
     const uint32_t tile = (y0 + ty) * gx + (x0 + tx);
     const uint32_t slot = warp_start + p;
+    if ((int64_t)slot >= cap) break;  // capacity path overflow (flagged elsewhere)
     keys[slot] = make_key<KT>(tile, s_dk[w][L], dkey_bits);
     vals[slot] = (int32_t)(first + L);
   }
@@ -261,8 +279,9 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
 template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
     k_radix_upsweep(const KT* __restrict__ keys, int64_t M, int shift, uint32_t mask,
-                    uint32_t* __restrict__ hist, int64_t nblocks) {
+                    uint32_t* __restrict__ hist, int64_t nblocks, const uint32_t* __restrict__ mdev) {
   __shared__ uint32_t h[8][kRadixBins];
+  M = device_patches(M, mdev);
   const int w = threadIdx.x >> 5;
   for (int k = threadIdx.x; k < 8 * kRadixBins; k += kSortThreads) (&h[0][0])[k] = 0u;
   __syncthreads();
@@ -308,8 +327,11 @@ __global__ void __launch_bounds__(kSortThreads)
     k_radix_downsweep(const KT* __restrict__ kin, const int32_t* __restrict__ vin,
                       KT* __restrict__ kout, int32_t* __restrict__ vout, int64_t M, int shift,
                       uint32_t mask, const uint32_t* __restrict__ hist,
-                      const uint32_t* __restrict__ digit_tot, int64_t nblocks) {
+                      const uint32_t* __restrict__ digit_tot, int64_t nblocks,
+                      const uint32_t* __restrict__ mdev) {
   static_assert(kRadixBins == 2 * kSortThreads, "two digits per thread");
+  M = device_patches(M, mdev);
+  if ((int64_t)blockIdx.x * kSortTile >= M) return;  // whole block past the patches
   extern __shared__ __align__(16) unsigned char smem_raw[];
   KT* sk = (KT*)smem_raw;
   int32_t* sv = (int32_t*)(sk + kSortTile);
@@ -389,7 +411,9 @@ __global__ void __launch_bounds__(kSortThreads)
 // M == 1.  `ranges` is cleared beforehand.
 template <typename KT>
 __global__ void k_ranges(const KT* __restrict__ keys, int64_t M, int dkey_bits,
-                         int2* __restrict__ ranges) {
+                         int2* __restrict__ ranges, const uint32_t* __restrict__ mdev) {
+  if (capacity_overflow(M, mdev, dkey_bits)) return;
+  M = device_patches(M, mdev);
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= M) return;
   const uint32_t cur = key_tile(keys[p], dkey_bits);
@@ -402,6 +426,17 @@ __global__ void k_ranges(const KT* __restrict__ keys, int64_t M, int dkey_bits,
     ranges[prv].y = (int)p;
     ranges[cur].x = (int)p;
   }
+}
+
+// Overflow status of a capacity-path sort (bits GSB_STATUS_PATCH_OVERFLOW,
+// GSB_STATUS_DEPTH_KEY_OVERFLOW), written for the caller to read later.
+__global__ void k_capacity_status(int64_t cap, int dkey_bits, const uint32_t* __restrict__ stats,
+                                  uint32_t* __restrict__ status) {
+  const uint64_t m = (uint64_t)stats[0] | ((uint64_t)stats[3] << 32);
+  uint32_t v = 0;
+  if (m > (uint64_t)cap) v |= GSB_STATUS_PATCH_OVERFLOW;
+  if (dkey_bits < 32 && (stats[1] >> dkey_bits) != 0u) v |= GSB_STATUS_DEPTH_KEY_OVERFLOW;
+  *status = v;
 }
 
 // ------------------------------------------------------------ launchers
@@ -477,7 +512,8 @@ SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey) {
 
 template <typename KT>
 static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void* ws,
-                  int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st) {
+                  int32_t* gsid_out, int32_t* ranges_out, const uint32_t* mdev,
+                  cudaStream_t st) {
   char* b = (char*)ws;
   KT* ka = (KT*)(b + p.off_keys_a);
   KT* kb = (KT*)(b + p.off_keys_b);
@@ -488,7 +524,7 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
   const uint32_t gx = (uint32_t)div_up(W, kTile);
   k_emit<KT><<<(int)s.n_blocks, kBinBlock, 0, st>>>(n, gx, p.dkey_bits, s.rects, s.dkeys, s.counts,
                                                     s.block_sums, ka,
-                                                    p.passes == 0 ? gsid_out : va);
+                                                    p.passes == 0 ? gsid_out : va, p.M);
   int rc = check_launch("splat_sort (emit)");
   if (rc) return rc;
   const size_t smem =
@@ -506,10 +542,11 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
     const int bits = (p.key_bits - shift) < kRadixBits ? (p.key_bits - shift) : kRadixBits;
     const uint32_t mask = (1u << bits) - 1u;
     int32_t* vdst = (pass == p.passes - 1) ? gsid_out : vd;
-    k_radix_upsweep<KT><<<nbk, kSortThreads, 0, st>>>(ks, p.M, shift, mask, hist, p.n_sort_blocks);
+    k_radix_upsweep<KT><<<nbk, kSortThreads, 0, st>>>(ks, p.M, shift, mask, hist, p.n_sort_blocks,
+                                                      mdev);
     k_radix_scan<<<(int)mask + 1, 256, 0, st>>>(hist, p.n_sort_blocks, dtot);
     k_radix_downsweep<KT><<<nbk, kSortThreads, smem, st>>>(ks, vs, kd, vdst, p.M, shift, mask,
-                                                           hist, dtot, p.n_sort_blocks);
+                                                           hist, dtot, p.n_sort_blocks, mdev);
     rc = check_launch("splat_sort (radix pass)", 3);
     if (rc) return rc;
     KT* kt = ks;
@@ -519,7 +556,7 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
     vs = vd;
     vd = vt;
   }
-  k_ranges<KT><<<div_up(p.M, 256), 256, 0, st>>>(ks, p.M, p.dkey_bits, (int2*)ranges_out);
+  k_ranges<KT><<<div_up(p.M, 256), 256, 0, st>>>(ks, p.M, p.dkey_bits, (int2*)ranges_out, mdev);
   return check_launch("splat_sort (ranges)");
 }
 
@@ -529,8 +566,21 @@ int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
   if (cudaMemsetAsync(ranges_out, 0, (size_t)p.n_tiles * 2 * sizeof(int32_t), st) != cudaSuccess)
     return check_launch("splat_sort (memset)", 0);
   if (p.M == 0) return GSB_OK;
-  return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, st)
-                : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, st);
+  return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, nullptr, st)
+                : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, nullptr, st);
+}
+
+int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
+                         void* ws, int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
+                         cudaStream_t st) {
+  (void)H;
+  if (cudaMemsetAsync(ranges_out, 0, (size_t)p.n_tiles * 2 * sizeof(int32_t), st) != cudaSuccess)
+    return check_launch("splat_sort_capacity (memset)", 0);
+  k_capacity_status<<<1, 1, 0, st>>>(p.M, p.dkey_bits, s.stats, status);
+  int rc = check_launch("splat_sort_capacity (status)");
+  if (rc || p.M == 0 || n == 0) return rc;
+  return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, s.stats, st)
+                : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, s.stats, st);
 }
 
 }  // namespace gsb

@@ -262,6 +262,29 @@ GSB_API int gsb_splat_sort(int64_t n, int height, int width, const gsb_splat_pla
   return launch_sort(p, n, height, width, s, sort_ws, gsid_out, ranges_out, ST(stream));
 }
 
+GSB_API size_t gsb_splat_sort_capacity_bytes(int64_t n, int height, int width,
+                                             int64_t patch_capacity, uint32_t max_depth_key) {
+  if (n < 0 || height < 0 || width < 0 || patch_capacity < 0) return 0;
+  return make_sort_plan(n, height, width, patch_capacity, max_depth_key).bytes_total;
+}
+
+GSB_API int gsb_splat_sort_capacity(int64_t n, int height, int width, int64_t patch_capacity,
+                                    uint32_t max_depth_key, const void* state, void* sort_ws,
+                                    int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
+                                    void* stream) {
+  int rc = check_image("splat_sort_capacity", n, height, width, 1);
+  if (rc) return rc;
+  GSB_CHECK_ARG(patch_capacity >= 0 && patch_capacity < (int64_t)INT32_MAX,
+                "splat_sort_capacity: capacity out of range");
+  GSB_CHECK_ARG(state && ranges_out && status, "splat_sort_capacity: null pointer");
+  GSB_CHECK_ARG(patch_capacity == 0 || (sort_ws && gsid_out),
+                "splat_sort_capacity: null workspace/output");
+  const SortPlan p = make_sort_plan(n, height, width, patch_capacity, max_depth_key);
+  const SplatState s = carve_state((void*)state, n, 1, height, width);
+  return launch_sort_capacity(p, n, height, width, s, sort_ws, gsid_out, ranges_out, status,
+                              ST(stream));
+}
+
 GSB_API int gsb_splat_draw(int64_t n, int height, int width, int channels, const int32_t* ranges,
                            const int32_t* gsid, const void* state, float tau_init, float* out,
                            int32_t* contrib, float* final_tau, void* stream) {
@@ -373,7 +396,8 @@ GSB_API int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float*
   GSB_CHECK_ARG(state && ((uintptr_t)state & 255) == 0,
                 "render_preprocess: state must be 256-byte aligned");
   GSB_CHECK_ARG(n == 0 || (pws && rots && scales && alphas), "render_preprocess: null input");
-  const SplatState s = carve_state(state, n, params->K, cam->height, cam->width);
+  const SplatState s =
+      carve_state(state, n, params->palette ? 3 : params->K, cam->height, cam->width);
   if (cudaMemsetAsync(s.stats, 0, 16 * sizeof(uint32_t), ST(stream)) != cudaSuccess ||
       cudaMemsetAsync(s.block_sums, 0, (size_t)(s.n_blocks > 0 ? s.n_blocks : 1) * 4,
                       ST(stream)) != cudaSuccess)
@@ -392,6 +416,7 @@ GSB_API int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float*
   f.wb = params->B;
   f.st = s;
   f.depths_out = depths_out;
+  f.palette = params->palette;
   rc = launch_render(params->mode, params->dtype, params->K, params->P, params->Q, params->rank, f,
                      false, ST(stream));
   if (rc) return rc;
@@ -424,6 +449,7 @@ GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* p
   const bool geom = dpws || drots || dscales || dalphas;
   GSB_CHECK_ARG(!geom || (dpws && drots && dscales && dalphas),
                 "render_backward: pass all of dpws, drots, dscales, dalphas or none");
+  GSB_CHECK_ARG(!params->palette, "render_backward: the palette-colour render has no adjoint here");
   const int K = params->K;
   const SplatState s = carve_state((void*)state, n, K, cam->height, cam->width);
   float* g_feat = (float*)scratch;

@@ -128,9 +128,14 @@ __device__ __forceinline__ void weights_of(const float* w0, const float* wa, con
 }
 
 // ------------------------------------------------------------- forward
-template <int MODE, int K, int P, int Q, int R, typename T>
+// COL: the record carries the Gaussian's palette colour sum_k w_k pal[k]
+// (3 channels) instead of its K weights -- the palette-edit render, which
+// the reference gets by baking the palette into RGB SH coefficients and
+// rendering those (gsplat/gsmodel.py:488-509, 14-26).
+template <int MODE, int K, int P, int Q, int R, typename T, bool COL>
 __global__ void __launch_bounds__(kFuseThreads)
     k_render_preprocess(int64_t n, uint32_t gx, uint32_t gy, CamArgs cam,
+                        const float* __restrict__ pal,
                         const float* __restrict__ pws, const float* __restrict__ rots,
                         const float* __restrict__ scales, const float* __restrict__ alphas,
                         const T* __restrict__ w0, const T* __restrict__ wa,
@@ -139,10 +144,14 @@ __global__ void __launch_bounds__(kFuseThreads)
                         uint32_t* __restrict__ counts, uint32_t* __restrict__ block_sums,
                         uint32_t* __restrict__ stats, float* __restrict__ depths_out) {
   using WS = WRows<MODE, K, P, Q, R>;
-  constexpr int V = RecordLayout<K>::kVec4;
+  constexpr int V = RecordLayout<COL ? 3 : K>::kVec4;
   extern __shared__ __align__(16) float sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t warp_tot[kFuseThreads / 32];
+  __shared__ float s_pal[COL ? 3 * K : 1];
+  if constexpr (COL) {
+    if (threadIdx.x < 3 * K) s_pal[threadIdx.x] = pal[threadIdx.x];
+  }
   const int nt = blockDim.x, t = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
   const bool staged = stage_params<MODE, K, P, Q, R, T>(n, row0, pws, rots, scales, alphas, w0,
@@ -177,8 +186,18 @@ __global__ void __launch_bounds__(kFuseThreads)
           weights_of<MODE, K, P, Q, R>(S.w0 + t * WS::W0, S.wa + t * WS::WA, S.wb + t * WS::WB,
                                        Y, w);
           record_head(p.ux, p.uy, conic[0], conic[1], conic[2], S.al[t], f);
+          if constexpr (COL) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) f[11 + k] = w[k];
+            for (int c = 0; c < 3; ++c) {
+              float acc = 0.f;
+#pragma unroll
+              for (int k = 0; k < K; ++k) acc += w[k] * s_pal[3 * k + c];
+              f[11 + c] = acc;
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) f[11 + k] = w[k];
+          }
           float4* rec = records + i * V;
 #pragma unroll
           for (int v = 0; v < V; ++v)
@@ -485,10 +504,11 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   const int grid = div_up(f.n, kFuseThreads);
   int rc;
   if (!backward) {
-    auto kern = k_render_preprocess<MODE, K, P, Q, R, T>;
+    auto kern = f.palette ? k_render_preprocess<MODE, K, P, Q, R, T, true>
+                          : k_render_preprocess<MODE, K, P, Q, R, T, false>;
     if ((rc = set_smem(kern, smem))) return rc;
     kern<<<grid, kFuseThreads, smem, st>>>(
-        f.n, f.gx, f.gy, f.cam, f.pws, f.rots, f.scales, f.alphas, (const T*)f.w0,
+        f.n, f.gx, f.gy, f.cam, f.palette, f.pws, f.rots, f.scales, f.alphas, (const T*)f.w0,
         (const T*)f.wa, (const T*)f.wb, f.st.records, f.st.rects, f.st.dkeys, f.st.counts,
         f.st.block_sums, f.st.stats, f.depths_out);
     return check_launch("render_preprocess");

@@ -68,6 +68,11 @@ struct SortPlan {
 SortPlan make_sort_plan(int64_t n, int H, int W, int64_t M, uint32_t max_dkey);
 int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s, void* ws,
                 int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st);
+// Capacity path: p.M is a patch capacity, the true count stays on the device
+// (s.stats); `status` (device) receives the overflow bits.  No host sync.
+int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
+                         void* ws, int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
+                         cudaStream_t st);
 
 // raster.cu
 int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, const int32_t* gsid,
@@ -94,6 +99,7 @@ struct FusedArgs {
   const void *w0, *wa, *wb;  // shs or dc; A; B (storage dtype)
   SplatState st;             // forward: filled like gsb_splat_pack + count
   float* depths_out;         // forward, may be null
+  const float* palette;      // forward, may be null: [K,3] -> colour records
   const float *g_feat, *g_u, *g_conic;  // backward: screen-space gradients (g_u null: weights only)
   float *d_pws, *d_rots, *d_scales, *d_w0, *d_wa, *d_wb;
 };

@@ -74,6 +74,44 @@ __device__ __forceinline__ bool box_overlaps_rect(float4 box, int wx, int wy, in
          box.z <= (float)(wy + ey);
 }
 
+// Second, exact stage of the warp's record test: can the record's cut
+// ellipse d^T Q d <= cut reach the pixel block [x0,x1] x [y0,y1] at all?
+// The minimum of the quadratic over the (continuous) block is 0 when the
+// centre lies inside, else it is attained on one of the four edges, where it
+// is a clamped 1-D quadratic minimum.  The record is dropped only when that
+// minimum exceeds the cut inflated exactly as the support box is (rounding of
+// the FP32 quadratic form grows with the conic's condition number): every
+// pixel of the block would then fail the per-pixel test maha <= cut, so the
+// results do not change.  Degenerate or ill-conditioned conics always pass
+// (their support box is unbounded too).
+__device__ __forceinline__ bool ellipse_meets_block(float4 v1, float4 v2, float x0, float y0,
+                                                    float x1, float y1) {
+  const float ux = v1.x, uy = v1.y, qa = v1.z, qb = v1.w, qc = v2.x, cut = v2.y;
+  if (!(isfinite(ux) && isfinite(uy)) || (ux >= x0 && ux <= x1 && uy >= y0 && uy <= y1))
+    return true;
+  const float det = qa * qc - qb * qb;
+  const float kappa = (qa + qc) * (qa + qc) / det;
+  if (!(det > 0.f && qa > 0.f && qc > 0.f && kappa < 1e5f)) return true;
+  const float c2 = cut * (1.f + 4e-6f * kappa) + 1e-3f;
+  const float ia = 1.f / qa, ic = 1.f / qc;
+  float m = INFINITY;
+  // vertical edges x = x0, x1: d_x fixed, d_y free in [uy - y1, uy - y0]
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const float dx = ux - (e ? x1 : x0);
+    const float dy = fminf(uy - y0, fmaxf(uy - y1, -qb * dx * ic));
+    m = fminf(m, qa * dx * dx + dy * (2.f * qb * dx + qc * dy));
+  }
+  // horizontal edges y = y0, y1
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const float dy = uy - (e ? y1 : y0);
+    const float dx = fminf(ux - x0, fmaxf(ux - x1, -qb * dy * ia));
+    m = fminf(m, qc * dy * dy + dx * (2.f * qb * dy + qa * dx));
+  }
+  return !(m > c2);
+}
+
 template <int K>
 __device__ __forceinline__ void load_feats(const float4* srec, int j, float v2w, float* f) {
   f[0] = v2w;
@@ -112,7 +150,10 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4)
     if (!__all_sync(0xffffffffu, done)) {
       for (int s = 0; s < cnt; s += 32) {
         const int j = s + (threadIdx.x & 31);
-        const bool ov = j < cnt && box_overlaps_rect(srec[j], wx, wy, 7, 3);
+        bool ov = j < cnt && box_overlaps_rect(srec[j], wx, wy, 7, 3);
+        if (ov)
+          ov = ellipse_meets_block(srec[kBatch + j], srec[2 * kBatch + j], (float)wx, (float)wy,
+                                   (float)(wx + 7), (float)(wy + 3));
         unsigned mask = __ballot_sync(0xffffffffu, ov);
         while (mask) {
           const int jj = s + __ffs(mask) - 1;
@@ -291,7 +332,10 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 6)
     for (int s_hi = hi; s_hi > 0; s_hi -= 32) {
       const int s_lo = max(0, s_hi - 32);
       const int j = s_lo + lane;
-      const bool ov = j < s_hi && box_overlaps_rect(srec[j], pp.wx, pp.wy, 7, 7);
+      bool ov = j < s_hi && box_overlaps_rect(srec[j], pp.wx, pp.wy, 7, 7);
+      if (ov)
+        ov = ellipse_meets_block(srec[kBatch + j], srec[2 * kBatch + j], (float)pp.wx,
+                                 (float)pp.wy, (float)(pp.wx + 7), (float)(pp.wy + 7));
       unsigned mask = __ballot_sync(0xffffffffu, ov);
       while (mask) {
         const int msb = 31 - __clz(mask);

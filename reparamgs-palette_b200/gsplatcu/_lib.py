@@ -18,6 +18,9 @@ GSB_ERR_CUDA = 2
 GSB_ERR_UNSUPPORTED = 3
 GSB_ERR_CAPACITY = 4
 GSB_ERR_DEVICE_TIMEOUT = 5
+STATUS_BULK_TIMEOUT = 1
+STATUS_PATCH_OVERFLOW = 2
+STATUS_DEPTH_KEY_OVERFLOW = 4
 DTYPE_F32 = 0
 DTYPE_BF16 = 1
 MAX_CHANNELS = 8
@@ -48,6 +51,8 @@ _SIGS = {
     "gsb_splat_counts": (_i32, [_i64, _i32, _i32, _p, _p, _p]),
     "gsb_splat_sort_bytes": (_sz, [_i64, _i32, _i32, _p]),
     "gsb_splat_sort": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p, _p]),
+    "gsb_splat_sort_capacity_bytes": (_sz, [_i64, _i32, _i32, _i64, _u32]),
+    "gsb_splat_sort_capacity": (_i32, [_i64, _i32, _i32, _i64, _u32, _p, _p, _p, _p, _p, _p]),
     "gsb_splat_sort_static_max_bytes": (_sz, []),
     "gsb_splat_sort_static": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p]),
     "gsb_splat_draw": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _f32, _p, _p, _p, _p]),
@@ -82,7 +87,7 @@ class PaletteParams(C.Structure):
     """gsb_palette_params: weight mode, storage dtype, shape and device pointers."""
     _fields_ = [("mode", C.c_int), ("dtype", C.c_int), ("K", C.c_int), ("P", C.c_int),
                 ("Q", C.c_int), ("rank", C.c_int), ("w0", C.c_void_p), ("A", C.c_void_p),
-                ("B", C.c_void_p)]
+                ("B", C.c_void_p), ("palette", C.c_void_p)]
 
 
 class GsplatError(RuntimeError):

@@ -1,0 +1,137 @@
+#!/usr/bin/env python
+"""Precision of the B200 path against the FP64 oracle: FP32 and BF16 storage.
+
+Scene: 3M Gaussians drawn as the benchmark scenes, full palette weights
+[N,16,5] at SH order 3.  For each of `--poses` seeded poses on a sphere of
+radius 8 and each resolution, the fused forward (palette_b200.render) runs
+with the weights stored in FP32 and in BF16 (all arithmetic FP32); the CPU
+oracle renders the same view in FP64 from the FP32 parameters (the BF16 error
+therefore includes the storage rounding).  The FP64 composite covers every
+`--tile-stride`-th tile (tiles are independent given the tile lists), and the
+errors are taken over those tiles: max / mean abs error of the K-channel
+weight image and of the palette colour image, and PSNR (peak 1).  Gradients:
+for the first `--grad-poses` poses, every parameter group's relative error
+||g - g64|| / ||g64|| of the full adjoint against the oracle's FP64 chain
+rule, with dL/dlayer random on the sampled tiles and zero elsewhere.
+
+Not collected by pytest (it is a report, minutes of CPU time): run it on a
+GPU box and keep the printed JSON.
+
+    python tests/precision_report.py [--gaussians 3000000] [--poses 32] [--tile-stride 8]
+"""
+import argparse
+import json
+import math
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+for p in (ROOT, os.path.join(ROOT, "reparamgs-palette_b200"), HERE):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+
+def sampled_lists(orc, pre32, H, W, stride):
+    b = orc.bin_gaussians(pre32["us"], pre32["areas"].copy(), pre32["depths"].copy(), H, W)
+    ranges = b["ranges"].copy()
+    keep = np.zeros(len(ranges), bool)
+    keep[::stride] = True
+    ranges[~keep] = 0
+    gx = (W + 15) // 16
+    mask = np.zeros((H, W), bool)
+    for t in np.flatnonzero(keep):
+        ty, tx = divmod(int(t), gx)
+        mask[ty * 16:(ty + 1) * 16, tx * 16:(tx + 1) * 16] = True
+    return (ranges, b["gsid"]), mask
+
+
+def stats(a, b, mask):
+    d = np.abs((a - b)[..., mask])
+    mse = float(np.mean(d * d))
+    return dict(max_abs=float(d.max()), mean_abs=float(d.mean()),
+                p9999_abs=float(np.quantile(d, 0.9999)), frac_over_1e5=float(np.mean(d > 1e-5)),
+                psnr=float("inf") if mse == 0 else 10 * math.log10(1.0 / mse))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gaussians", type=int, default=3_000_000)
+    ap.add_argument("--poses", type=int, default=32)
+    ap.add_argument("--grad-poses", type=int, default=2)
+    ap.add_argument("--tile-stride", type=int, default=8)
+    ap.add_argument("--resolutions", default="3840x2160,1920x1080")
+    a = ap.parse_args()
+    from oracle import oracle as orc
+    from palette_b200.render import render_palette
+    from palette_b200.scene import look_at, sphere_poses, synthetic_scene, to_torch
+    orc.set_threads(os.cpu_count() or 1)
+    sc = synthetic_scene(a.gaussians, seed=2, mode="full")
+    K = 5
+    st32 = to_torch(sc, "cuda", torch.float32)
+    st16 = to_torch(sc, "cuda", torch.bfloat16)
+    pal = sc["palette"].astype(np.float64)
+    f64 = {k: sc[k].astype(np.float64) for k in ("pws", "rots", "scales", "alphas", "shs")}
+    res = [tuple(int(v) for v in r.split("x")) for r in a.resolutions.split(",")]
+    report = dict(gaussians=a.gaussians, poses=a.poses, tile_stride=a.tile_stride,
+                  host_threads=orc.get_threads(), resolutions={}, gradients=[])
+    t0 = time.time()
+    for W, H in res:
+        rows = {"fp32": [], "bf16": []}
+        for pi, eye in enumerate(sphere_poses(a.poses, 8.0, seed=2)):
+            cam = look_at(eye, width=W, height=H, device="cuda")
+            twc = cam.twc.detach().double().cpu().numpy()
+            pre32 = orc.preprocess(sc["pws"], sc["rots"], sc["scales"], cam, np.float32)
+            lists, mask = sampled_lists(orc, pre32, H, W, a.tile_stride)
+            w64, = orc.sh2feat(f64["shs"], f64["pws"], twc, K, False, np.float64, ref_quirk=False)
+            o = orc.render_weights(f64["pws"], f64["rots"], f64["scales"], f64["alphas"], w64, cam,
+                                   np.float64, lists=lists)
+            img64 = np.einsum("kc,khw->chw", pal, o["layer"])
+            for name, st in (("fp32", st32), ("bf16", st16)):
+                with torch.no_grad():
+                    layer, _, _ = render_palette(st["pws"], st["rots"], st["scales"], st["alphas"],
+                                                 cam, shs=st["shs"])
+                L = layer.double().cpu().numpy()
+                img = np.einsum("kc,khw->chw", pal, L)
+                rows[name].append(dict(layer=stats(L, o["layer"], mask), image=stats(img, img64, mask)))
+            if pi < a.grad_poses and (W, H) == res[-1]:
+                rng = np.random.default_rng(pi)
+                dout = rng.standard_normal((K, H, W)) * mask
+                g64 = orc.render_weights_backward(f64["pws"], f64["rots"], f64["scales"],
+                                                  f64["alphas"], cam, twc, K, shs=f64["shs"],
+                                                  lists=lists, dout=dout)
+                pairs = dict(pws="dpws", rots="drots", scales="dscales", alphas="dalphas",
+                             shs="dshs")
+                for name, st in (("fp32", st32), ("bf16", st16)):
+                    leaves = {k: st[k].detach().clone().requires_grad_(True) for k in pairs}
+                    layer, _, _ = render_palette(leaves["pws"], leaves["rots"], leaves["scales"],
+                                                 leaves["alphas"], cam, shs=leaves["shs"])
+                    layer.backward(torch.from_numpy(dout.astype(np.float32)).cuda())
+                    rel = {}
+                    for k, gk in pairs.items():
+                        g = leaves[k].grad.double().cpu().numpy().reshape(len(g64[gk]), -1)
+                        r = g64[gk].reshape(len(g), -1)
+                        rel[k] = float(np.linalg.norm(g - r) / max(np.linalg.norm(r), 1e-300))
+                    report["gradients"].append(dict(storage=name, width=W, height=H, pose=pi,
+                                                    rel_err=rel))
+        summ = {}
+        for name, rs in rows.items():
+            summ[name] = {
+                part: dict(max_abs=max(r[part]["max_abs"] for r in rs),
+                           mean_abs=float(np.mean([r[part]["mean_abs"] for r in rs])),
+                           p9999_abs=max(r[part]["p9999_abs"] for r in rs),
+                           frac_over_1e5=float(np.mean([r[part]["frac_over_1e5"] for r in rs])),
+                           psnr_min=min(r[part]["psnr"] for r in rs),
+                           psnr_mean=float(np.mean([r[part]["psnr"] for r in rs])))
+                for part in ("layer", "image")}
+        report["resolutions"][f"{W}x{H}"] = summ
+    report["wall_s"] = round(time.time() - t0, 1)
+    print(json.dumps(report, indent=1))
+
+
+if __name__ == "__main__":
+    main()
