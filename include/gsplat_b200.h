@@ -191,8 +191,9 @@ int gsb_splat_sort_static(int64_t n, int height, int width, const gsb_splat_plan
  * sized for `patch_capacity` patches and depth keys up to `max_depth_key`
  * (uint32(depth*1000)); the true patch count stays on the device.  Needs
  * `sort_ws` of gsb_splat_sort_capacity_bytes(...) bytes and gsid_out of
- * patch_capacity entries.  *status (device memory) receives
- * GSB_STATUS_PATCH_OVERFLOW / GSB_STATUS_DEPTH_KEY_OVERFLOW or 0; on an
+ * patch_capacity entries.  status (device uint32[3]) receives the overflow
+ * bits GSB_STATUS_PATCH_OVERFLOW / GSB_STATUS_DEPTH_KEY_OVERFLOW (or 0) and
+ * the true patch count (low, high word); on an
  * overflow every range is left empty (the image then shows nothing) and the
  * caller re-renders with a larger capacity.  Without overflow the results
  * equal gsb_splat_sort's.  No counterpart in the reference, which always

@@ -436,7 +436,9 @@ __global__ void k_capacity_status(int64_t cap, int dkey_bits, const uint32_t* __
   uint32_t v = 0;
   if (m > (uint64_t)cap) v |= GSB_STATUS_PATCH_OVERFLOW;
   if (dkey_bits < 32 && (stats[1] >> dkey_bits) != 0u) v |= GSB_STATUS_DEPTH_KEY_OVERFLOW;
-  *status = v;
+  status[0] = v;
+  status[1] = stats[0];  // the patch count, low and high words
+  status[2] = stats[3];
 }
 
 // ------------------------------------------------------------ launchers

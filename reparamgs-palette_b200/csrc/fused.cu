@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kFuseThreads)
                         uint32_t* __restrict__ stats, float* __restrict__ depths_out) {
   using WS = WRows<MODE, K, P, Q, R>;
   constexpr int V = RecordLayout<COL ? 3 : K>::kVec4;
+  static_assert(WS::IN >= 4 * V, "the record span reuses the input staging area");
   extern __shared__ __align__(16) float sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t warp_tot[kFuseThreads / 32];
@@ -159,6 +160,7 @@ __global__ void __launch_bounds__(kFuseThreads)
   const Staged<MODE, K, P, Q, R> S(sm);
   const int64_t i = row0 + t;
   uint32_t cnt = 0, dk = 0;
+  float f[4 * V];  // this Gaussian's record (kept until the block writes its records)
   if (staged && i < n) {
     const CamRegs cr = load_cam(cam);
     float depth_out = kBadDepth;
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(kFuseThreads)
           depth_out = p.z;
           dk = __float2uint_rz(p.z * 1000);
           rects[i] = make_uint2(r.x0 | (r.y0 << 16), r.x1 | (r.y1 << 16));
-          float dir[3], Y[16], w[K], f[20];
+          float dir[3], Y[16], w[K];
           view_direction(pw, make_float3(cr.c[0], cr.c[1], cr.c[2]), dir, nullptr, nullptr);
           sh_basis(dir, WS::L + 1, Y);
           weights_of<MODE, K, P, Q, R>(S.w0 + t * WS::W0, S.wa + t * WS::WA, S.wb + t * WS::WB,
@@ -198,10 +200,6 @@ __global__ void __launch_bounds__(kFuseThreads)
 #pragma unroll
             for (int k = 0; k < K; ++k) f[11 + k] = w[k];
           }
-          float4* rec = records + i * V;
-#pragma unroll
-          for (int v = 0; v < V; ++v)
-            rec[v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
         }
       }
     }
@@ -222,11 +220,31 @@ __global__ void __launch_bounds__(kFuseThreads)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane == 0 && m) atomicMax(stats + 1, m);
-  __syncthreads();
+  __syncthreads();  // every thread is done with the staged inputs from here on
   if (t == 0) {  // block_sums count blocks of kBinBlock Gaussians (zeroed by the caller)
     uint32_t tot = 0;
     for (int k = 0; k < nt / 32; ++k) tot += warp_tot[k];
     if (tot) atomicAdd(block_sums + row0 / kBinBlock, tot);
+  }
+  // records: assembled over the input staging area, written as one span (the
+  // rows of Gaussians without patches are never read)
+  float4* s_rec = reinterpret_cast<float4*>(sm);
+  if (cnt > 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      s_rec[t * V + v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
+  }
+  const int64_t rows = min((int64_t)nt, n - row0);
+  if (rows == nt && aligned16(records + row0 * V)) {
+    fence_proxy_async_shared();
+    __syncthreads();
+    if (t == 0) {
+      bulk_store(records + row0 * V, s_rec, (uint32_t)(nt * V * 16));
+      bulk_store_drain();
+    }
+  } else {
+    __syncthreads();
+    for (int j = t; j < rows * V; j += nt) records[row0 * V + j] = s_rec[j];
   }
 }
 

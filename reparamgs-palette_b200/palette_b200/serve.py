@@ -135,8 +135,8 @@ class _Slot:
         self.tcw = torch.zeros((3,), dtype=_F32, device=device)
         self.twc = torch.zeros((3,), dtype=_F32, device=device)
         self.palette = torch.zeros((K_max, 3), dtype=_F32, device=device)
-        self.status = torch.zeros((1,), dtype=torch.int32, device=device)
-        self.status_host = torch.zeros((1,), dtype=torch.int32).pin_memory()
+        self.status = torch.zeros((4,), dtype=torch.int32, device=device)
+        self.status_host = torch.zeros((4,), dtype=torch.int32).pin_memory()
         self.sizes = dict(state=0, sort=0, gsid=0, tiles=0, pixels=0)
         self.buf = {}
         self.graphs = {}

@@ -106,7 +106,7 @@ def test_capacity_sort_matches_exact_sort_and_flags_overflow(cuda_ok):
     r_ref = torch.empty((tiles, 2), dtype=torch.int32, device="cuda")
     _lib.call("t", "gsb_splat_sort", n, H, W, C.byref(plan), _lib.ptr(state), _lib.ptr(ws),
               _lib.ptr(g_ref), _lib.ptr(r_ref), None)
-    status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    status = torch.full((4,), -1, dtype=torch.int32, device="cuda")
     for cap, dkey in ((M, MAX_DEPTH_KEY), (3 * M + 5000, MAX_DEPTH_KEY), (M, (1 << 30))):
         ws2 = torch.empty(int(L.gsb_splat_sort_capacity_bytes(n, H, W, cap, dkey)),
                           dtype=torch.uint8, device="cuda")
@@ -114,7 +114,7 @@ def test_capacity_sort_matches_exact_sort_and_flags_overflow(cuda_ok):
         r = torch.full((tiles, 2), -3, dtype=torch.int32, device="cuda")
         _lib.call("t", "gsb_splat_sort_capacity", n, H, W, cap, dkey, _lib.ptr(state),
                   _lib.ptr(ws2), _lib.ptr(g), _lib.ptr(r), _lib.ptr(status), None)
-        assert int(status.item()) == 0
+        assert int(status[0]) == 0 and int(status[1]) == M and int(status[2]) == 0
         assert torch.equal(g[:M], g_ref) and torch.equal(r, r_ref)
     # overflow: capacity below the patch count, and depth keys wider than allowed
     for cap, dkey, bit in ((M // 2, MAX_DEPTH_KEY, _lib.STATUS_PATCH_OVERFLOW),
@@ -125,7 +125,7 @@ def test_capacity_sort_matches_exact_sort_and_flags_overflow(cuda_ok):
         r = torch.full((tiles, 2), -3, dtype=torch.int32, device="cuda")
         _lib.call("t", "gsb_splat_sort_capacity", n, H, W, cap, dkey, _lib.ptr(state),
                   _lib.ptr(ws2), _lib.ptr(g), _lib.ptr(r), _lib.ptr(status), None)
-        assert int(status.item()) & bit
+        assert int(status[0]) & bit
         assert torch.count_nonzero(r) == 0
 
 
