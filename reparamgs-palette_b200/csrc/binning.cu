@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(kBinBlock)
            bool bin, float4* __restrict__ records, uint2* __restrict__ rects,
            uint32_t* __restrict__ dkeys, uint32_t* __restrict__ counts,
            uint32_t* __restrict__ block_sums, uint32_t* __restrict__ stats) {
+  pdl_wait();
   __shared__ uint32_t warp_tot[8];
   const int64_t i = (int64_t)blockIdx.x * kBinBlock + threadIdx.x;
   uint32_t cnt = 0, dk = 0;
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(kBinBlock)
 // total M (low/high words) into stats[0] / stats[3].
 __global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__ sums, int64_t nb,
                                                           uint32_t* __restrict__ stats) {
+  pdl_wait();
   __shared__ uint32_t warp_tot[32];
   __shared__ unsigned long long carry;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -231,6 +233,7 @@ __global__ void __launch_bounds__(kBinBlock)
            const uint32_t* __restrict__ dkeys, const uint32_t* __restrict__ counts,
            const uint32_t* __restrict__ block_offs, KT* __restrict__ keys,
            int32_t* __restrict__ vals, int64_t cap) {
+  pdl_wait();
   __shared__ uint32_t warp_tot[8];
   __shared__ uint32_t s_incl[8][32];
   __shared__ uint2 s_rect[8][32];
@@ -280,6 +283,7 @@ template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
     k_radix_upsweep(const KT* __restrict__ keys, int64_t M, int shift, uint32_t mask,
                     uint32_t* __restrict__ hist, int64_t nblocks, const uint32_t* __restrict__ mdev) {
+  pdl_wait();
   __shared__ uint32_t h[8][kRadixBins];
   M = device_patches(M, mdev);
   const int w = threadIdx.x >> 5;
@@ -303,6 +307,7 @@ __global__ void __launch_bounds__(kSortThreads)
 // One block per digit: exclusive scan of that digit's per-block counts.
 __global__ void __launch_bounds__(256)
     k_radix_scan(uint32_t* __restrict__ hist, int64_t nblocks, uint32_t* __restrict__ digit_tot) {
+  pdl_wait();
   __shared__ uint32_t warp_tot[8];
   uint32_t* row = hist + (int64_t)blockIdx.x * nblocks;
   uint32_t carry = 0;
@@ -329,6 +334,7 @@ __global__ void __launch_bounds__(kSortThreads)
                       uint32_t mask, const uint32_t* __restrict__ hist,
                       const uint32_t* __restrict__ digit_tot, int64_t nblocks,
                       const uint32_t* __restrict__ mdev) {
+  pdl_wait();
   static_assert(kRadixBins == 2 * kSortThreads, "two digits per thread");
   M = device_patches(M, mdev);
   if ((int64_t)blockIdx.x * kSortTile >= M) return;  // whole block past the patches
@@ -412,6 +418,7 @@ __global__ void __launch_bounds__(kSortThreads)
 template <typename KT>
 __global__ void k_ranges(const KT* __restrict__ keys, int64_t M, int dkey_bits,
                          int2* __restrict__ ranges, const uint32_t* __restrict__ mdev) {
+  pdl_wait();
   if (capacity_overflow(M, mdev, dkey_bits)) return;
   M = device_patches(M, mdev);
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -432,6 +439,7 @@ __global__ void k_ranges(const KT* __restrict__ keys, int64_t M, int dkey_bits,
 // GSB_STATUS_DEPTH_KEY_OVERFLOW), written for the caller to read later.
 __global__ void k_capacity_status(int64_t cap, int dkey_bits, const uint32_t* __restrict__ stats,
                                   uint32_t* __restrict__ status) {
+  pdl_wait();
   const uint64_t m = (uint64_t)stats[0] | ((uint64_t)stats[3] << 32);
   uint32_t v = 0;
   if (m > (uint64_t)cap) v |= GSB_STATUS_PATCH_OVERFLOW;
@@ -446,10 +454,9 @@ template <typename T>
 static void pack_t(int64_t n, uint32_t gx, uint32_t gy, int C, const float* us, const float* cinv,
                    const float* alphas, const void* feats, float* depths, int32_t* areas, bool bin,
                    const SplatState& s, cudaStream_t st) {
-  k_pack<T><<<(int)s.n_blocks, kBinBlock, 0, st>>>(n, gx, gy, C, s.rec_vec4, us, cinv, alphas,
-                                                   (const T*)feats, depths, areas, bin, s.records,
-                                                   s.rects, s.dkeys, s.counts, s.block_sums,
-                                                   s.stats);
+  launch_pdl(k_pack<T>, dim3((unsigned)s.n_blocks), dim3(kBinBlock), 0, st, n, gx, gy, C,
+             s.rec_vec4, us, cinv, alphas, (const T*)feats, depths, areas, bin, s.records, s.rects,
+             s.dkeys, s.counts, s.block_sums, s.stats);
 }
 
 int launch_pack(int64_t n, int H, int W, int channels, const float* us, const float* cinv,
@@ -468,7 +475,7 @@ int launch_pack(int64_t n, int H, int W, int channels, const float* us, const fl
 
 int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st) {
   if (n == 0) return GSB_OK;
-  k_scan_block_sums<<<1, 1024, 0, st>>>(s.block_sums, s.n_blocks, s.stats);
+  launch_pdl(k_scan_block_sums, dim3(1), dim3(1024), 0, st, s.block_sums, s.n_blocks, s.stats);
   return check_launch("splat_scan");
 }
 
@@ -524,9 +531,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
   uint32_t* hist = (uint32_t*)(b + p.off_hist);
   uint32_t* dtot = (uint32_t*)(b + p.off_digit_tot);
   const uint32_t gx = (uint32_t)div_up(W, kTile);
-  k_emit<KT><<<(int)s.n_blocks, kBinBlock, 0, st>>>(n, gx, p.dkey_bits, s.rects, s.dkeys, s.counts,
-                                                    s.block_sums, ka,
-                                                    p.passes == 0 ? gsid_out : va, p.M);
+  launch_pdl(k_emit<KT>, dim3((unsigned)s.n_blocks), dim3(kBinBlock), 0, st, n, gx, p.dkey_bits,
+             s.rects, s.dkeys, s.counts, s.block_sums, ka, p.passes == 0 ? gsid_out : va, p.M);
   int rc = check_launch("splat_sort (emit)");
   if (rc) return rc;
   const size_t smem =
@@ -544,11 +550,12 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
     const int bits = (p.key_bits - shift) < kRadixBits ? (p.key_bits - shift) : kRadixBits;
     const uint32_t mask = (1u << bits) - 1u;
     int32_t* vdst = (pass == p.passes - 1) ? gsid_out : vd;
-    k_radix_upsweep<KT><<<nbk, kSortThreads, 0, st>>>(ks, p.M, shift, mask, hist, p.n_sort_blocks,
-                                                      mdev);
-    k_radix_scan<<<(int)mask + 1, 256, 0, st>>>(hist, p.n_sort_blocks, dtot);
-    k_radix_downsweep<KT><<<nbk, kSortThreads, smem, st>>>(ks, vs, kd, vdst, p.M, shift, mask,
-                                                           hist, dtot, p.n_sort_blocks, mdev);
+    launch_pdl(k_radix_upsweep<KT>, dim3(nbk), dim3(kSortThreads), 0, st, (const KT*)ks, p.M,
+               shift, mask, hist, p.n_sort_blocks, mdev);
+    launch_pdl(k_radix_scan, dim3(mask + 1), dim3(256), 0, st, hist, p.n_sort_blocks, dtot);
+    launch_pdl(k_radix_downsweep<KT>, dim3(nbk), dim3(kSortThreads), smem, st, (const KT*)ks,
+               (const int32_t*)vs, kd, vdst, p.M, shift, mask, (const uint32_t*)hist,
+               (const uint32_t*)dtot, p.n_sort_blocks, mdev);
     rc = check_launch("splat_sort (radix pass)", 3);
     if (rc) return rc;
     KT* kt = ks;
@@ -558,7 +565,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
     vs = vd;
     vd = vt;
   }
-  k_ranges<KT><<<div_up(p.M, 256), 256, 0, st>>>(ks, p.M, p.dkey_bits, (int2*)ranges_out, mdev);
+  launch_pdl(k_ranges<KT>, dim3((unsigned)div_up(p.M, 256)), dim3(256), 0, st, (const KT*)ks, p.M,
+             p.dkey_bits, (int2*)ranges_out, mdev);
   return check_launch("splat_sort (ranges)");
 }
 

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kFuseThreads)
                         uint2* __restrict__ rects, uint32_t* __restrict__ dkeys,
                         uint32_t* __restrict__ counts, uint32_t* __restrict__ block_sums,
                         uint32_t* __restrict__ stats, float* __restrict__ depths_out) {
+  pdl_wait();
   using WS = WRows<MODE, K, P, Q, R>;
   constexpr int V = RecordLayout<COL ? 3 : K>::kVec4;
   static_assert(WS::IN >= 4 * V, "the record span reuses the input staging area");
@@ -335,6 +336,7 @@ __global__ void __launch_bounds__(kFuseThreads)
                           float* __restrict__ d_pws, float* __restrict__ d_rots,
                           float* __restrict__ d_scales, float* __restrict__ d_w0,
                           float* __restrict__ d_wa, float* __restrict__ d_wb) {
+  pdl_wait();
   using WS = WRows<MODE, K, P, Q, R>;
   using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
   constexpr int L = WS::L;
@@ -525,10 +527,10 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
     auto kern = f.palette ? k_render_preprocess<MODE, K, P, Q, R, T, true>
                           : k_render_preprocess<MODE, K, P, Q, R, T, false>;
     if ((rc = set_smem(kern, smem))) return rc;
-    kern<<<grid, kFuseThreads, smem, st>>>(
-        f.n, f.gx, f.gy, f.cam, f.palette, f.pws, f.rots, f.scales, f.alphas, (const T*)f.w0,
-        (const T*)f.wa, (const T*)f.wb, f.st.records, f.st.rects, f.st.dkeys, f.st.counts,
-        f.st.block_sums, f.st.stats, f.depths_out);
+    launch_pdl(kern, dim3(grid), dim3(kFuseThreads), smem, st, f.n, f.gx, f.gy, f.cam, f.palette,
+               f.pws, f.rots, f.scales, f.alphas, (const T*)f.w0, (const T*)f.wa, (const T*)f.wb,
+               f.st.records, f.st.rects, f.st.dkeys, f.st.counts, f.st.block_sums, f.st.stats,
+               f.depths_out);
     return check_launch("render_preprocess");
   }
   const bool geom = f.g_u != nullptr;
@@ -537,10 +539,9 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   const int bsmem = (geom ? BwdPlan<MODE, K, P, Q, R, true>::floats
                           : BwdPlan<MODE, K, P, Q, R, false>::floats) * kFuseThreads * 4;
   if ((rc = set_smem(kern, bsmem))) return rc;
-  kern<<<grid, kFuseThreads, bsmem, st>>>(f.n, f.cam, f.pws, f.rots, f.scales, (const T*)f.w0,
-                                          (const T*)f.wa, (const T*)f.wb, f.g_feat, f.g_u,
-                                          f.g_conic, f.d_pws, f.d_rots, f.d_scales, f.d_w0,
-                                          f.d_wa, f.d_wb);
+  launch_pdl(kern, dim3(grid), dim3(kFuseThreads), bsmem, st, f.n, f.cam, f.pws, f.rots,
+             f.scales, (const T*)f.w0, (const T*)f.wa, (const T*)f.wb, f.g_feat, f.g_u, f.g_conic,
+             f.d_pws, f.d_rots, f.d_scales, f.d_w0, f.d_wa, f.d_wb);
   return check_launch("render_backward");
 }
 

@@ -76,6 +76,30 @@ void set_error(const char* fmt, ...);
 // converts a launch error into GSB_ERR_CUDA with a message.
 int check_launch(const char* what, int launches = 1);
 
+// Programmatic dependent launch: a kernel launched with launch_pdl may be
+// scheduled while the previous kernel on its stream is still finishing, which
+// hides the launch gap between the short kernels of one render.  Every kernel
+// that can be launched this way calls pdl_wait() before it touches global
+// memory; the wait returns once the previous kernel has completed and its
+// writes are visible (without the launch attribute it returns at once).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 }  // namespace gsb
 
 #define GSB_CHECK_ARG(cond, ...)        \

@@ -17,6 +17,7 @@ __global__ void __launch_bounds__(kLossThreads)
     k_palette_l1(int64_t hw, const float* __restrict__ layer, const float* __restrict__ palette,
                  const float* __restrict__ target, float scale, float* __restrict__ image,
                  float* __restrict__ loss, float* __restrict__ dlayer, float* __restrict__ dpal) {
+  pdl_wait();
   constexpr int KC = 3 * K;
   __shared__ float sP[KC];
   __shared__ float red[kLossThreads / 32][KC + 1];
@@ -91,8 +92,8 @@ int launch_palette_l1(int K, int H, int W, const float* layer, const float* pale
   switch (K) {
 #define GSB_K(KK)                                                                                 \
   case KK:                                                                                        \
-    k_palette_l1<KK><<<grid, kLossThreads, 0, st>>>(hw, layer, palette, target, scale, image, loss, \
-                                                    dlayer, dpal);                                \
+    launch_pdl(k_palette_l1<KK>, dim3(grid), dim3(kLossThreads), 0, st, hw, layer, palette,      \
+               target, scale, image, loss, dlayer, dpal);                                        \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K

@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4)
     k_draw(int H, int W, int gx, const int2* __restrict__ ranges, const int32_t* __restrict__ gsid,
            const float4* __restrict__ records, float tau_init, float* __restrict__ out,
            int32_t* __restrict__ contrib, float* __restrict__ final_tau) {
+  pdl_wait();
   constexpr int V = RecordLayout<K>::kVec4;
   __shared__ float4 srec[V * kBatch];
   int wx, wy, px, py;
@@ -286,6 +287,7 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 6)
                     const float* __restrict__ dout, const float* __restrict__ dtau,
                     float* __restrict__ dfeat, float* __restrict__ dalpha,
                     float* __restrict__ du, float* __restrict__ dconic) {
+  pdl_wait();
   constexpr int V = RecordLayout<K>::kVec4;
   constexpr int NREAL = GEOM ? K + 6 : K;
   constexpr int NV = Pow2<NREAL>::value;
@@ -402,8 +404,8 @@ int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, co
   switch (channels) {
 #define GSB_K(KK)                                                                           \
   case KK:                                                                                  \
-    k_draw<KK><<<tiles, kDrawFwdThreads, 0, st>>>(H, W, gx, rg, gsid, s.records, tau_init, out, \
-                                               contrib, final_tau);                         \
+    launch_pdl(k_draw<KK>, dim3(tiles), dim3(kDrawFwdThreads), 0, st, H, W, gx, rg, gsid,       \
+               (const float4*)s.records, tau_init, out, contrib, final_tau);                   \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K
@@ -418,15 +420,11 @@ static void draw_bwd_k(int tiles, int H, int W, int gx, const int2* rg, const in
                        const float* dtau, float* dfeat, float* dalpha, float* du, float* dq,
                        cudaStream_t st) {
   const bool geom = dalpha != nullptr;
-  if (geom && dtau)
-    k_draw_backward<K, true, true><<<tiles, kDrawThreads, 0, st>>>(
-        H, W, gx, rg, gsid, rec, contrib, ft, dout, dtau, dfeat, dalpha, du, dq);
-  else if (geom)
-    k_draw_backward<K, true, false><<<tiles, kDrawThreads, 0, st>>>(
-        H, W, gx, rg, gsid, rec, contrib, ft, dout, dtau, dfeat, dalpha, du, dq);
-  else
-    k_draw_backward<K, false, false><<<tiles, kDrawThreads, 0, st>>>(
-        H, W, gx, rg, gsid, rec, contrib, ft, dout, dtau, dfeat, dalpha, du, dq);
+  auto kern = (geom && dtau) ? k_draw_backward<K, true, true>
+              : geom         ? k_draw_backward<K, true, false>
+                             : k_draw_backward<K, false, false>;
+  launch_pdl(kern, dim3(tiles), dim3(kDrawThreads), 0, st, H, W, gx, rg, gsid, rec, contrib, ft,
+             dout, dtau, dfeat, dalpha, du, dq);
 }
 
 int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* ranges,
