@@ -200,6 +200,13 @@ int gsb_splat_sort_static(int64_t n, int height, int width, const gsb_splat_plan
  * reads the patch count back (gsplatcu/gausplat.cu:199-201). */
 size_t gsb_splat_sort_capacity_bytes(int64_t n, int height, int width, int64_t patch_capacity,
                                      uint32_t max_depth_key);
+/* Writes only the status words of gsb_splat_sort_capacity (overflow bits and
+ * the true patch count, status = device uint32[3]) for `state`, so that a
+ * caller can copy them to the host and learn the patch count while the sort
+ * and compositing already run. */
+int gsb_splat_patch_status(int64_t n, int height, int width, int64_t patch_capacity,
+                           uint32_t max_depth_key, const void* state, uint32_t* status,
+                           void* stream);
 int gsb_splat_sort_capacity(int64_t n, int height, int width, int64_t patch_capacity,
                             uint32_t max_depth_key, const void* state, void* sort_ws,
                             int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,

@@ -580,6 +580,13 @@ int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
                 : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, nullptr, st);
 }
 
+int launch_patch_status(const SortPlan& p, const SplatState& s, uint32_t* status,
+                        cudaStream_t st) {
+  launch_pdl(k_capacity_status, dim3(1), dim3(1), 0, st, p.M, p.dkey_bits,
+             (const uint32_t*)s.stats, status);
+  return check_launch("splat_patch_status");
+}
+
 int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
                          void* ws, int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
                          cudaStream_t st) {

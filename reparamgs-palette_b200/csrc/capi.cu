@@ -268,6 +268,17 @@ GSB_API size_t gsb_splat_sort_capacity_bytes(int64_t n, int height, int width,
   return make_sort_plan(n, height, width, patch_capacity, max_depth_key).bytes_total;
 }
 
+GSB_API int gsb_splat_patch_status(int64_t n, int height, int width, int64_t patch_capacity,
+                                   uint32_t max_depth_key, const void* state, uint32_t* status,
+                                   void* stream) {
+  int rc = check_image("splat_patch_status", n, height, width, 1);
+  if (rc) return rc;
+  GSB_CHECK_ARG(state && status, "splat_patch_status: null pointer");
+  const SortPlan p = make_sort_plan(n, height, width, patch_capacity, max_depth_key);
+  const SplatState s = carve_state((void*)state, n, 1, height, width);
+  return launch_patch_status(p, s, status, ST(stream));
+}
+
 GSB_API int gsb_splat_sort_capacity(int64_t n, int height, int width, int64_t patch_capacity,
                                     uint32_t max_depth_key, const void* state, void* sort_ws,
                                     int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,

@@ -70,6 +70,8 @@ int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
                 int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st);
 // Capacity path: p.M is a patch capacity, the true count stays on the device
 // (s.stats); `status` (device) receives the overflow bits.  No host sync.
+int launch_patch_status(const SortPlan& p, const SplatState& s, uint32_t* status,
+                        cudaStream_t st);
 int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const SplatState& s,
                          void* ws, int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
                          cudaStream_t st);

@@ -233,6 +233,54 @@ def sh2Weight_fast_B(shs_A, shs_B, Ylm_stored, dloss_dw, num_palette, Q):
 
 
 # --------------------------------------------------------------- splatting
+# Per (Gaussian count, image size): patch capacity (1.25x the largest count
+# seen, plus slack) and depth-key bound for the overlapped read-back below.
+_CAPACITY = {}
+
+
+def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_init, dev, st):
+    """Tile sort and compositing of a packed `state`; returns the tile lists
+    (gsid, exactly the patch count long).  The reference reads the patch
+    count back before it sorts (gsplatcu/gausplat.cu:199-201), and so does
+    the first render of each size here.  Later renders of that size enqueue
+    the sort -- sized by the stored capacity -- and the compositing at once,
+    and read the count back while they run; if the count or a depth key
+    exceeded the capacity, those kernels left every range empty and the tile
+    lists are sorted and composited again exactly (results identical)."""
+    L = _lib.lib()
+    key = (n, H, W)
+    if key in _CAPACITY:
+        cap, dkey = _CAPACITY[key]
+        status = torch.empty((4,), dtype=torch.int32, device=dev)
+        host = torch.empty((4,), dtype=torch.int32, pin_memory=True)
+        call(op, "gsb_splat_patch_status", n, H, W, cap, dkey, ptr(state), ptr(status), st)
+        host.copy_(status, non_blocking=True)
+        counted = torch.cuda.Event()
+        counted.record(torch.cuda.current_stream(dev))
+        ws = torch.empty(max(1, int(L.gsb_splat_sort_capacity_bytes(n, H, W, cap, dkey))),
+                         dtype=torch.uint8, device=dev)
+        full = torch.empty((max(1, cap),), dtype=torch.int32, device=dev)
+        call(op, "gsb_splat_sort_capacity", n, H, W, cap, dkey, ptr(state), ptr(ws), ptr(full),
+             ptr(ranges), ptr(status), st)
+        call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(full), ptr(state),
+             float(tau_init), ptr(out), ptr(contrib), ptr(final_tau), st)
+        counted.synchronize()
+        if int(host[0]) == 0:
+            return full[:int(host[1]) | (int(host[2]) << 32)]
+    plan = _lib.SplatPlan()
+    call(op, "gsb_splat_counts", n, H, W, ptr(state), C.byref(plan), st)
+    M = int(plan.patches)
+    ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan)))),
+                     dtype=torch.uint8, device=dev)
+    gsid = torch.empty((M,), dtype=torch.int32, device=dev)
+    call(op, "gsb_splat_sort", n, H, W, C.byref(plan), ptr(state), ptr(ws), ptr(gsid), ptr(ranges),
+         st)
+    call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(gsid), ptr(state), float(tau_init),
+         ptr(out), ptr(contrib), ptr(final_tau), st)
+    _CAPACITY[key] = (int(M * 1.25) + 4096, (1 << int(plan.max_depth_key).bit_length()) - 1)
+    return gsid
+
+
 def _splat_forward(op, H, W, C_, us, cinv2ds, alphas, depths, feats, areas, tau_init):
     us, cinv = _cuda(op, "us", us), _cuda(op, "cinv2ds", cinv2ds)
     alphas = _cuda(op, "alphas", alphas)
@@ -255,16 +303,8 @@ def _splat_forward(op, H, W, C_, us, cinv2ds, alphas, depths, feats, areas, tau_
         out = torch.empty((C_, H, W), dtype=_F32, device=dev)
         contrib = torch.empty((H, W), dtype=torch.int32, device=dev)
         final_tau = torch.empty((H, W), dtype=_F32, device=dev)
-        plan = _lib.SplatPlan()
-        call(op, "gsb_splat_counts", n, H, W, ptr(state), C.byref(plan), st)
-        M = int(plan.patches)
-        ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan)))),
-                         dtype=torch.uint8, device=dev)
-        gsid = torch.empty((M,), dtype=torch.int32, device=dev)
-        call(op, "gsb_splat_sort", n, H, W, C.byref(plan), ptr(state), ptr(ws), ptr(gsid),
-             ptr(ranges), st)
-        call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(gsid), ptr(state), float(tau_init),
-             ptr(out), ptr(contrib), ptr(final_tau), st)
+        gsid = _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_init,
+                              dev, st)
     return [out, contrib, final_tau, ranges, gsid]
 
 

@@ -53,6 +53,7 @@ _SIGS = {
     "gsb_splat_sort": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p, _p]),
     "gsb_splat_sort_capacity_bytes": (_sz, [_i64, _i32, _i32, _i64, _u32]),
     "gsb_splat_sort_capacity": (_i32, [_i64, _i32, _i32, _i64, _u32, _p, _p, _p, _p, _p, _p]),
+    "gsb_splat_patch_status": (_i32, [_i64, _i32, _i32, _i64, _u32, _p, _p, _p]),
     "gsb_splat_sort_static_max_bytes": (_sz, []),
     "gsb_splat_sort_static": (_i32, [_i64, _i32, _i32, _p, _p, _p, _p, _p]),
     "gsb_splat_draw": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _f32, _p, _p, _p, _p]),

@@ -22,7 +22,7 @@ import ctypes as C
 
 import torch
 
-from gsplatcu import _lib
+from gsplatcu import _lib, _sort_and_draw
 
 _F32 = torch.float32
 
@@ -72,18 +72,8 @@ class _RenderPalette(torch.autograd.Function):
             layer = torch.empty((K, H, W), dtype=_F32, device=dev)
             contrib = torch.empty((H, W), dtype=torch.int32, device=dev)
             final_tau = torch.empty((H, W), dtype=_F32, device=dev)
-            plan = _lib.SplatPlan()
-            _lib.call("render_palette", "gsb_splat_counts", n, H, W, _lib.ptr(state),
-                      C.byref(plan), st)
-            M = int(plan.patches)
-            ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan)))),
-                             dtype=torch.uint8, device=dev)
-            gsid = torch.empty((M,), dtype=torch.int32, device=dev)
-            _lib.call("render_palette", "gsb_splat_sort", n, H, W, C.byref(plan), _lib.ptr(state),
-                      _lib.ptr(ws), _lib.ptr(gsid), _lib.ptr(ranges), st)
-            _lib.call("render_palette", "gsb_splat_draw", n, H, W, K, _lib.ptr(ranges),
-                      _lib.ptr(gsid), _lib.ptr(state), 0.0, _lib.ptr(layer), _lib.ptr(contrib),
-                      _lib.ptr(final_tau), st)
+            gsid = _sort_and_draw("render_palette", n, H, W, K, state, ranges, layer, contrib,
+                                  final_tau, 0.0, dev, st)
         ctx.meta = (cam, mode, K, P, Q, rank)
         ctx.save_for_backward(pws, rots, scales, alphas, w0, A, B, state, ranges, gsid, contrib,
                               final_tau)

@@ -8,7 +8,8 @@ reference build (oracle/_ref, compiled from its sources by oracle/build_ref.py)
 and once through this build's gsplatcu, on identical synthetic inputs, plus
 this build's fused path (palette_b200.render.render_palette, weights-only
 backward) on the same scene.  Device time per iteration by CUDA events
-(median of several repeats, after warm-up).  Not collected by pytest: run it
+(median of 10 repeats after warm-up, then the median over 3 rounds in which
+the implementations alternate, after 2 s of GPU load to settle the clocks).  Not collected by pytest: run it
 on a GPU box and keep the printed JSON.
 
     python tests/perf_reference_gpu.py [--gaussians 1000000] [--width 1920] [--height 1080]
@@ -73,12 +74,30 @@ def timed(fn, reps=10, warm=3):
     return statistics.median(ts)
 
 
+def burn(seconds=2.0):
+    """Keep the GPU busy so that its clocks have ramped up before timing."""
+    a = torch.randn((4096, 4096), device="cuda")
+    t = torch.cuda.Event(enable_timing=True)
+    s = torch.cuda.Event(enable_timing=True)
+    s.record()
+    while True:
+        for _ in range(20):
+            a = a @ a
+            a = a / a.norm()
+        t.record()
+        torch.cuda.synchronize()
+        if s.elapsed_time(t) > seconds * 1000:
+            return
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gaussians", type=int, default=1_000_000)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--rounds", type=int, default=3,
+                    help="alternating rounds; each figure is the median over rounds")
     a = ap.parse_args()
     import gsplatcu as ours
     from oracle.build_ref import load_ref
@@ -96,14 +115,6 @@ def main():
         if mode == "lowrank":  # the reference's rank-1 shapes
             st["A"], st["B"] = st["A"][:, :, 0].contiguous(), st["B"][:, 0, :].contiguous()
         dlayer = torch.rand((5, a.height, a.width), device="cuda")
-        row = {}
-        for name, g in (("reference", ref), ("b200_ops", ours)):
-            row[name + "_forward"] = timed(lambda: forward(g, st, cam, mode), a.reps)
-
-            def fb():
-                saved, _ = forward(g, st, cam, mode)
-                backward(g, st, cam, mode, saved, dlayer)
-            row[name + "_fwd_bwd"] = timed(fb, a.reps)
         wn = dict(shs=st["shs"]) if mode == "full" else dict(dc=st["dc"], A=st["A"], B=st["B"])
         leaves = {k: v.detach().clone().requires_grad_(True) for k, v in wn.items()}
 
@@ -112,14 +123,31 @@ def main():
                                          **leaves)
             if bwd:
                 layer.backward(dlayer)
-        with torch.no_grad():
-            row["b200_fused_forward"] = timed(lambda: fused(False), a.reps)
-        row["b200_fused_fwd_bwd"] = timed(lambda: fused(True), a.reps)
+
+        burn()
+        rounds = []
+        for _ in range(a.rounds):  # alternate the implementations within each round
+            row = {}
+            for name, g in (("reference", ref), ("b200_ops", ours)):
+                row[name + "_forward"] = timed(lambda: forward(g, st, cam, mode), a.reps)
+
+                def fb():
+                    saved, _ = forward(g, st, cam, mode)
+                    backward(g, st, cam, mode, saved, dlayer)
+                row[name + "_fwd_bwd"] = timed(fb, a.reps)
+            with torch.no_grad():
+                row["b200_fused_forward"] = timed(lambda: fused(False), a.reps)
+            row["b200_fused_fwd_bwd"] = timed(lambda: fused(True), a.reps)
+            rounds.append(row)
+        row = {k: statistics.median(r[k] for r in rounds) for k in rounds[0]}
+        row["reference_forward_range"] = [min(r["reference_forward"] for r in rounds),
+                                          max(r["reference_forward"] for r in rounds)]
         for k in ("forward", "fwd_bwd"):
             row[f"speedup_ops_{k}"] = row[f"reference_{k}"] / row[f"b200_ops_{k}"]
             row[f"speedup_fused_{k}"] = row[f"reference_{k}"] / row[f"b200_fused_{k}"]
         out["cases"][mode + ("" if mode == "full" else "_rank1")] = {
-            k: round(v, 4) for k, v in row.items()}
+            k: (round(v, 4) if not isinstance(v, list) else [round(x, 4) for x in v])
+            for k, v in row.items()}
     print(json.dumps(out, indent=1))
 
 

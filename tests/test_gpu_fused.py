@@ -236,3 +236,18 @@ def test_fused_weight_gradients_match_reference_backward(cuda_ok, rank):
     (ref_layer * g).sum().backward()
     for k in ("dc", "A", "B"):
         assert rel_err(leaf[k].grad, ref_in[k].grad) < 1e-5, k
+
+
+def test_fused_forward_overlapped_count_and_overflow(cuda_ok):
+    """Repeated renders of one size enqueue the sort before the patch count is
+    read back; a view with more patches than the stored capacity is redone
+    exactly.  All match the operator sequence."""
+    sc, st, cam_far = _setup("full", 0, torch.float32, n=15000, W=160, H=96, eye=(0.0, -14.0, 0.0))
+    cam_near = look_at((0.0, -5.0, 0.5), width=160, height=96, device="cuda")
+    gsc._CAPACITY.pop((15000, 96, 160), None)
+    for cam in (cam_far, cam_far, cam_near, cam_near):
+        ref = forward_ops(gsc, st, cam, "full")
+        (layer, ft, depths), _ = _render(st, cam, "full")
+        assert max_abs(layer, ref["layer"]) < IMG_TOL and max_abs(ft, ref["final_tau"]) < IMG_TOL
+        assert torch.equal(depths, ref["depths"].reshape(-1))
+    assert gsc._CAPACITY[(15000, 96, 160)][0] >= int(ref["gsid"].numel())

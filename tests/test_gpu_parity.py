@@ -321,3 +321,29 @@ def test_sort_long_lists_and_ties_bitexact(cuda_ok, crowd):
     assert np.array_equal(np_of(d_g), dd) and np.array_equal(np_of(a_g), aa)
     counts = b["ranges"][:, 1] - b["ranges"][:, 0]
     assert counts.max() >= crowd
+
+
+def test_splat_weight_overlapped_count_and_overflow_bitexact(cuda_ok):
+    """After the first render of a size, the sort and compositing are enqueued
+    before the patch count is read back (capacity from earlier renders); a
+    view needing more patches is sorted and composited again exactly.  Every
+    render's lists, ranges, in-place updates and image equal the oracle's."""
+    n, W, H = 12000, 144, 112
+    sc, st = _scene(n, seed=77)
+    gsc._CAPACITY.pop((n, H, W), None)
+    for eye in ((0.0, -15.0, 0.0), (1.0, -14.0, 0.5), (0.0, -5.0, 0.5), (0.5, -5.5, 0.0)):
+        cam = _cam(W, H, eye)
+        pre = _gpu_pre(st, cam)
+        w, = gsc.sh2Weight(st["shs"], st["pws"], cam.twc, False, 5)
+        ref = _oracle_splat(H, W, 5, {k: v.clone() for k, v in pre.items()}, st["alphas"], w, 0.0)
+        layer, contrib, ft, ranges, gsid = gsc.splat_weight(H, W, 5, pre["us"], pre["cinv"],
+                                                            st["alphas"], pre["depths"], w,
+                                                            pre["areas"])
+        assert (n, H, W) in gsc._CAPACITY
+        assert np.array_equal(np_of(gsid), ref["b"]["gsid"])
+        assert np.array_equal(np_of(ranges), ref["b"]["ranges"])
+        assert np.array_equal(np_of(pre["depths"]), ref["depths"])
+        assert np.array_equal(np_of(pre["areas"]), ref["areas"])
+        same = np_of(contrib) == ref["contrib"]
+        assert same.mean() > 1 - 1e-4
+        assert max_abs(np_of(layer)[:, same], ref["out"][:, same]) < IMG_TOL
