@@ -26,7 +26,7 @@
 
 namespace gsb {
 
-constexpr int kFuseThreads = 128;
+constexpr int kFuseThreads = 64;
 static __device__ uint32_t g_fused_status;
 
 // Row lengths of the colour-parameter arrays (floats per Gaussian).

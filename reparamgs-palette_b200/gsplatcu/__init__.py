@@ -23,6 +23,7 @@ torch CUDA stream without device synchronisation, except ``splat_weight`` /
 reference does).
 """
 import ctypes as C
+import threading
 
 import torch
 
@@ -236,6 +237,19 @@ def sh2Weight_fast_B(shs_A, shs_B, Ylm_stored, dloss_dw, num_palette, Q):
 # Per (Gaussian count, image size): patch capacity (1.25x the largest count
 # seen, plus slack) and depth-key bound for the overlapped read-back below.
 _CAPACITY = {}
+_READBACK = {}
+
+
+def _readback_buffers(dev):
+    """(device status words, pinned host copy, event) of the calling thread on
+    `dev`; the host copy is read before the thread renders again."""
+    key = (dev, threading.get_ident())
+    b = _READBACK.get(key)
+    if b is None:
+        b = (torch.empty((4,), dtype=torch.int32, device=dev),
+             torch.empty((4,), dtype=torch.int32, pin_memory=True), torch.cuda.Event())
+        _READBACK[key] = b
+    return b
 
 
 def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_init, dev, st):
@@ -251,11 +265,9 @@ def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_
     key = (n, H, W)
     if key in _CAPACITY:
         cap, dkey = _CAPACITY[key]
-        status = torch.empty((4,), dtype=torch.int32, device=dev)
-        host = torch.empty((4,), dtype=torch.int32, pin_memory=True)
+        status, host, counted = _readback_buffers(dev)
         call(op, "gsb_splat_patch_status", n, H, W, cap, dkey, ptr(state), ptr(status), st)
         host.copy_(status, non_blocking=True)
-        counted = torch.cuda.Event()
         counted.record(torch.cuda.current_stream(dev))
         ws = torch.empty(max(1, int(L.gsb_splat_sort_capacity_bytes(n, H, W, cap, dkey))),
                          dtype=torch.uint8, device=dev)

@@ -27,11 +27,13 @@ from gsplatcu import _lib, _sort_and_draw
 _F32 = torch.float32
 
 
+def _f32c(t):
+    return t if t.dtype == _F32 and t.is_contiguous() else t.to(_F32).contiguous()
+
+
 def camera_struct(cam):
     """(gsb_camera, tensors to keep alive) for a camera-like object."""
-    Rcw = cam.Rcw.to(_F32).contiguous()
-    tcw = cam.tcw.to(_F32).contiguous().reshape(-1)
-    twc = cam.twc.to(_F32).contiguous().reshape(-1)
+    Rcw, tcw, twc = _f32c(cam.Rcw), _f32c(cam.tcw), _f32c(cam.twc)
     c = _lib.Camera(Rcw.data_ptr(), tcw.data_ptr(), twc.data_ptr(), float(cam.fx), float(cam.fy),
                     float(cam.cx), float(cam.cy), int(cam.width), int(cam.height))
     return c, (Rcw, tcw, twc)
