@@ -258,6 +258,24 @@ int gsb_palette_l1(int K, int height, int width, const float* layer, const float
                    const float* target, float* image, float* loss, float* dlayer,
                    float* dpalette, void* stream);
 
+/* The finetune step's loss on the rendered weights (finetune.py:356-389, the
+ * target by gsplat/gsmodel.py:219-285), one pass over the image: the
+ * barycentric target W of the colour image `target` [3,H,W] in the palette
+ * {black, white, chroma [chroma_count,3]} (optionally clamped to >= 0 and
+ * renormalised, `clamp`), then loss[0] = loss[1] + loss[2] with
+ * loss[1] = mean((layer - W)^2) (GSB_LOSS_MSE) or mean|layer - W| (GSB_LOSS_L1)
+ * over the K = chroma_count + 2 channels, loss[2] = lambda_pos *
+ * mean(relu(-layer)).  dlayer [K,H,W] (overwritten) and dchroma
+ * [chroma_count,3] (overwritten) are the loss gradients, the latter through
+ * the target; target_weights [K,H,W] receives W.  Outputs other than loss may
+ * be NULL. */
+#define GSB_LOSS_MSE 0
+#define GSB_LOSS_L1 1
+int gsb_palette_geo_loss(int chroma_count, int height, int width, const float* layer,
+                         const float* target, const float* chroma, int clamp, int kind,
+                         float lambda_pos, float* target_weights, float* loss, float* dlayer,
+                         float* dchroma, void* stream);
+
 /* ============================================================ fused path
  * One view of the palette-weight rasterizer with the per-Gaussian work of
  * project / computeCov3D / computeCov2D / sh2Weight(_fast) / inverseCov2D /

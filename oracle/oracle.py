@@ -360,3 +360,133 @@ def render_weights_backward(pws, rots, scales, alphas, cam, twc, K, shs=None, lo
         out["dA"] = np.einsum("npq,nrq->npr", dC, B3).reshape(A.shape)
         out["dB"] = np.einsum("npq,npr->nrq", dC, A3).reshape(B.shape)
     return out
+
+
+# ------------------------------------------------------------- loss side
+def _softplus(x):
+    return np.where(x > 20.0, x, np.log1p(np.exp(np.minimum(x, 20.0))))
+
+
+def _sigmoid(x):
+    return 1.0 / (1.0 + np.exp(-x))
+
+
+def palette_geo_loss(layer, target, chroma, clamp=True, lambda_pos=0.5, kind="mse", tau=1e-9,
+                     eps=1e-12):
+    """The finetune step's loss on the rendered palette weights (finetune.py:
+    356-389 with gsplat/gsmodel.py:219-285 for the target), in FP64:
+
+      W_bary = barycentric target of the colour image `target` [3,H,W] in the
+               palette {black, white, chroma [Kc,3]}: for each tetrahedron
+               (black, white, c_i, c_{i+1}) the barycentric coordinates of the
+               pixel colour, their softplus-normalised projection's
+               reconstruction error, and a softmax over the tetrahedra (tau)
+               weighting the raw coordinates;
+      clamp:   W_bary <- max(W_bary, 0) / max(sum_k max(W_bary, 0), 1e-8);
+      loss   = mean((layer - W_bary)^2) (kind "mse") or mean(|layer - W_bary|)
+               ("l1"), plus lambda_pos * mean(relu(-layer)).
+
+    Returns dict(loss, target_weights [K,H,W], dlayer [K,H,W], dchroma [Kc,3])
+    with the gradients of the loss (the target depends on the palette)."""
+    layer = np.asarray(layer, np.float64)
+    C = np.asarray(target, np.float64).reshape(3, -1).T  # [N,3]
+    P = np.asarray(chroma, np.float64)
+    Kc = P.shape[0]
+    K = Kc + 2
+    N = C.shape[0]
+    Wt = layer.reshape(K, -1).T  # [N,K]
+    e = np.ones(3)
+    raws, errs, cache = [], [], []
+    for i in range(Kc):
+        j = (i + 1) % Kc
+        A = np.stack([e, P[i], P[j]], axis=1)  # columns: white-black, P_i, P_j
+        a = A
+        det = (a[0, 0] * (a[1, 1] * a[2, 2] - a[1, 2] * a[2, 1])
+               - a[0, 1] * (a[1, 0] * a[2, 2] - a[1, 2] * a[2, 0])
+               + a[0, 2] * (a[1, 0] * a[2, 1] - a[1, 1] * a[2, 0]))
+        adj = np.array([
+            [a[1, 1] * a[2, 2] - a[1, 2] * a[2, 1], -(a[0, 1] * a[2, 2] - a[0, 2] * a[2, 1]),
+             a[0, 1] * a[1, 2] - a[0, 2] * a[1, 1]],
+            [-(a[1, 0] * a[2, 2] - a[1, 2] * a[2, 0]), a[0, 0] * a[2, 2] - a[0, 2] * a[2, 0],
+             -(a[0, 0] * a[1, 2] - a[0, 2] * a[1, 0])],
+            [a[1, 0] * a[2, 1] - a[1, 1] * a[2, 0], -(a[0, 0] * a[2, 1] - a[0, 1] * a[2, 0]),
+             a[0, 0] * a[1, 1] - a[0, 1] * a[1, 0]]])
+        dinv = 1.0 / (det + eps)
+        co = (C @ adj.T) * dinv  # [N,3]: beta, gamma, delta
+        beta, gamma, delta = co[:, 0], co[:, 1], co[:, 2]
+        alpha = 1.0 - beta - gamma - delta
+        raw = np.zeros((N, K))
+        raw[:, 0] = alpha
+        raw[:, 1] = beta
+        raw[:, i + 2] += gamma
+        raw[:, j + 2] += delta
+        x = np.stack([alpha, beta, gamma, delta], 1)
+        sp = _softplus(x)
+        den = sp.sum(1) + eps
+        pr = sp / den[:, None]
+        recon = pr[:, 1:2] * e + pr[:, 2:3] * P[i] + pr[:, 3:4] * P[j]
+        err = ((recon - C) ** 2).sum(1)
+        raws.append(raw)
+        errs.append(err)
+        cache.append((i, j, A, co, x, sp, den, pr, recon))
+    E = np.stack(errs, 1)  # [N,Kc]
+    lg = -E / tau
+    lg = lg - lg.max(1, keepdims=True)
+    pe = np.exp(lg)
+    probs = pe / pe.sum(1, keepdims=True)
+    R = np.stack(raws, 1)  # [N,Kc,K]
+    Wb = (probs[:, :, None] * R).sum(1)  # [N,K]
+    if clamp:
+        m = np.maximum(Wb, 0.0)
+        s_raw = m.sum(1)
+        s = np.maximum(s_raw, 1e-8)
+        Wc = m / s[:, None]
+    else:
+        Wc = Wb
+    diff = Wt - Wc
+    n_el = K * N
+    if kind == "mse":
+        loss = (diff ** 2).sum() / n_el
+        g = 2.0 * diff / n_el
+    else:
+        loss = np.abs(diff).sum() / n_el
+        g = np.sign(diff) / n_el
+    loss += lambda_pos * np.maximum(-Wt, 0.0).sum() / n_el
+    dWt = g + lambda_pos * np.where(Wt < 0, -1.0, 0.0) / n_el
+    gW = -g  # dL / d (clamped) target
+    if clamp:
+        gm = np.where(s_raw[:, None] > 1e-8,
+                      gW / s[:, None] - (gW * m).sum(1, keepdims=True) / (s * s)[:, None],
+                      gW / s[:, None])
+        gWb = gm * (Wb > 0)
+    else:
+        gWb = gW
+    # W = sum_i probs_i raw_i
+    graw = probs[:, :, None] * gWb[:, None, :]  # [N,Kc,K]
+    gprob = (R * gWb[:, None, :]).sum(2)  # [N,Kc]
+    glog = probs * (gprob - (probs * gprob).sum(1, keepdims=True))
+    gerr = -glog / tau
+    dP = np.zeros_like(P)
+    for (i, j, A, co, x, sp, den, pr, recon), ii in zip(cache, range(Kc)):
+        gr = graw[:, ii, :]
+        g_alpha, g_beta = gr[:, 0], gr[:, 1]
+        g_gamma, g_delta = gr[:, i + 2], gr[:, j + 2]
+        # error path: err = |recon - C|^2
+        ge = gerr[:, ii]
+        grec = 2.0 * (recon - C) * ge[:, None]  # [N,3]
+        dP[i] += (grec * pr[:, 2:3]).sum(0)
+        dP[j] += (grec * pr[:, 3:4]).sum(0)
+        gpr = np.stack([np.zeros(N), grec.sum(1), (grec * P[i]).sum(1), (grec * P[j]).sum(1)], 1)
+        gsp = gpr / den[:, None] - (gpr * sp).sum(1, keepdims=True) / (den * den)[:, None]
+        gx = gsp * np.where(x > 20.0, 1.0, _sigmoid(np.minimum(x, 20.0)))
+        g_alpha = g_alpha + gx[:, 0]
+        g_beta = g_beta + gx[:, 1]
+        g_gamma = g_gamma + gx[:, 2]
+        g_delta = g_delta + gx[:, 3]
+        gco = np.stack([g_beta - g_alpha, g_gamma - g_alpha, g_delta - g_alpha], 1)  # [N,3]
+        # coords = A^-1 C: d coords = -A^-1 (dA) coords, dA columns 1, 2 = dP_i, dP_j
+        Ainv_T_g = gco @ np.linalg.inv(A)  # rows: (A^-T g)^T
+        dP[i] -= (Ainv_T_g * co[:, 1:2]).sum(0)
+        dP[j] -= (Ainv_T_g * co[:, 2:3]).sum(0)
+    return dict(loss=float(loss), target_weights=Wc.T.reshape(layer.shape),
+                dlayer=dWt.T.reshape(layer.shape), dchroma=dP)

@@ -364,6 +364,23 @@ GSB_API int gsb_palette_l1(int K, int height, int width, const float* layer,
                            ST(stream));
 }
 
+GSB_API int gsb_palette_geo_loss(int chroma_count, int height, int width, const float* layer,
+                                 const float* target, const float* chroma, int clamp, int kind,
+                                 float lambda_pos, float* target_weights, float* loss,
+                                 float* dlayer, float* dchroma, void* stream) {
+  GSB_CHECK_ARG(chroma_count >= 2 && chroma_count <= GSB_MAX_CHANNELS - 2,
+                "palette_geo_loss: chromatic palette size must be in [2, %d]",
+                GSB_MAX_CHANNELS - 2);
+  GSB_CHECK_ARG(height >= 0 && width >= 0, "palette_geo_loss: negative image size");
+  GSB_CHECK_ARG(kind == GSB_LOSS_MSE || kind == GSB_LOSS_L1, "palette_geo_loss: bad loss kind");
+  GSB_CHECK_ARG(chroma && loss, "palette_geo_loss: null pointer");
+  GSB_CHECK_ARG(((int64_t)height * width == 0) || (layer && target),
+                "palette_geo_loss: null input");
+  return launch_palette_geo_loss(chroma_count, height, width, layer, target, chroma, clamp != 0,
+                                 kind, lambda_pos, target_weights, loss, dlayer, dchroma,
+                                 ST(stream));
+}
+
 // ------------------------------------------------------------- fused path
 static int check_params(const char* op, int64_t n, const gsb_palette_params* p) {
   GSB_CHECK_ARG(p, "%s: null palette parameters", op);

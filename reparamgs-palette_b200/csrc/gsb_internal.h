@@ -33,6 +33,10 @@ int lowrank_status(uint32_t* out, bool clear, cudaStream_t st);
 int launch_palette_l1(int K, int H, int W, const float* layer, const float* palette,
                       const float* target, float* image, float* loss, float* dlayer, float* dpal,
                       cudaStream_t st);
+int launch_palette_geo_loss(int KC, int H, int W, const float* layer, const float* target,
+                            const float* chroma, int clamp, int kind, float lambda_pos,
+                            float* wbary, float* loss, float* dlayer, float* dchroma,
+                            cudaStream_t st);
 
 // binning.cu -- per-Gaussian binning state carved out of one caller buffer.
 struct SplatState {

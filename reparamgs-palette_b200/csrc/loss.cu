@@ -102,4 +102,304 @@ int launch_palette_l1(int K, int H, int W, const float* layer, const float* pale
   return check_launch("palette_l1");
 }
 
+
+// ------------------------------------------------- palette-weight loss
+// The finetune step's loss on the rendered weights (finetune.py:356-389),
+// per pixel, with the barycentric target of gsplat/gsmodel.py:219-285
+// recomputed in the same pass (it depends on the palette, which is being
+// learnt):
+//   for each tetrahedron i (black, white, c_i, c_{i+1}): coords
+//     (beta, gamma, delta) = adj(A_i) C / (det A_i + 1e-12), A_i = [1, c_i, c_{i+1}],
+//     alpha = 1 - beta - gamma - delta; a softplus-normalised projection of
+//     (alpha, beta, gamma, delta) reconstructs the colour with error err_i;
+//   W = sum_i softmax(-err / 1e-9)_i raw_i (raw_i: the coords on their channels);
+//   optional clamp: W <- max(W, 0) / max(sum max(W, 0), 1e-8);
+//   loss = mean over the K x H x W values of (layer - W)^2 (MSE) or |layer - W|
+//   (L1), plus lambda_pos * mean(relu(-layer)).
+// Gradients: d/d layer per pixel, and d/d palette through the target (the
+// raw coordinates' dependence on A_i, and the softmax term, which is exactly
+// zero unless two tetrahedra's errors tie to within ~1e-7).
+constexpr float kBaryTau = 1e-9f, kBaryEps = 1e-12f;
+
+template <int KC>
+struct TetraConst {
+  float adj[9], dinv, ainv[9];  // ainv = A^-1 (for the adjoint)
+  int i, j;
+};
+
+__device__ __forceinline__ float softplus_f(float x) { return x > 20.f ? x : log1pf(expf(x)); }
+__device__ __forceinline__ float softplus_grad(float x) {
+  return x > 20.f ? 1.f : 1.f / (1.f + expf(-x));
+}
+
+// Forward of one tetrahedron: coords x[4] = (alpha, beta, gamma, delta),
+// softplus values, normaliser, projection and reconstruction error.
+template <int KC>
+__device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const float* Pi,
+                                               const float* Pj, const float* C, float* x, float* sp,
+                                               float& den, float* pr, float* rec) {
+  float co[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    co[r] = (T.adj[3 * r] * C[0] + T.adj[3 * r + 1] * C[1] + T.adj[3 * r + 2] * C[2]) * T.dinv;
+  x[1] = co[0];
+  x[2] = co[1];
+  x[3] = co[2];
+  x[0] = 1.f - co[0] - co[1] - co[2];
+  den = kBaryEps;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    sp[k] = softplus_f(x[k]);
+    den += sp[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) pr[k] = sp[k] / den;
+  float err = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    rec[c] = pr[1] + pr[2] * Pi[c] + pr[3] * Pj[c];
+    const float d = rec[c] - C[c];
+    err += d * d;
+  }
+  return err;
+}
+
+template <int KC>
+__global__ void __launch_bounds__(kLossThreads, 2)
+    k_palette_geo_loss(int64_t hw, const float* __restrict__ layer,
+                       const float* __restrict__ target, const float* __restrict__ chroma,
+                       int clamp, int kind, float lambda_pos, float inv_n,
+                       float* __restrict__ wbary, float* __restrict__ loss,
+                       float* __restrict__ dlayer, float* __restrict__ dchroma) {
+  pdl_wait();
+  constexpr int K = KC + 2;
+  __shared__ TetraConst<KC> s_t[KC];
+  __shared__ float s_p[KC][3];
+  __shared__ float red[kLossThreads / 32][3 * KC + 2];
+  if (threadIdx.x < 3 * KC) s_p[threadIdx.x / 3][threadIdx.x % 3] = chroma[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x < KC) {
+    const int i = threadIdx.x, j = (i + 1) % KC;
+    TetraConst<KC> T;
+    T.i = i;
+    T.j = j;
+    float a[9];  // A = [1 | c_i | c_j] by columns, row-major
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      a[3 * r] = 1.f;
+      a[3 * r + 1] = s_p[i][r];
+      a[3 * r + 2] = s_p[j][r];
+    }
+    const float det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                      a[2] * (a[3] * a[7] - a[4] * a[6]);
+    T.adj[0] = a[4] * a[8] - a[5] * a[7];
+    T.adj[1] = -(a[1] * a[8] - a[2] * a[7]);
+    T.adj[2] = a[1] * a[5] - a[2] * a[4];
+    T.adj[3] = -(a[3] * a[8] - a[5] * a[6]);
+    T.adj[4] = a[0] * a[8] - a[2] * a[6];
+    T.adj[5] = -(a[0] * a[5] - a[2] * a[3]);
+    T.adj[6] = a[3] * a[7] - a[4] * a[6];
+    T.adj[7] = -(a[0] * a[7] - a[1] * a[6]);
+    T.adj[8] = a[0] * a[4] - a[1] * a[3];
+    T.dinv = 1.f / (det + kBaryEps);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) T.ainv[k] = T.adj[k] / det;
+    s_t[i] = T;
+  }
+  __syncthreads();
+  float dP[KC][3];
+#pragma unroll
+  for (int i = 0; i < KC; ++i) dP[i][0] = dP[i][1] = dP[i][2] = 0.f;
+  float lgeo = 0.f, lpos = 0.f;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < hw;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const float C[3] = {target[p], target[hw + p], target[2 * hw + p]};
+    float err[KC];
+#pragma unroll
+    for (int i = 0; i < KC; ++i) {
+      float x[4], sp[4], den, pr[4], rec[3];
+      err[i] = tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, x, sp, den, pr, rec);
+    }
+    // softmax over the tetrahedra of -err / tau (shifted by the maximum)
+    float lmax = -INFINITY;
+#pragma unroll
+    for (int i = 0; i < KC; ++i) lmax = fmaxf(lmax, -err[i] / kBaryTau);
+    float prob[KC], psum = 0.f;
+#pragma unroll
+    for (int i = 0; i < KC; ++i) {
+      prob[i] = expf(-err[i] / kBaryTau - lmax);
+      psum += prob[i];
+    }
+    float Wb[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) Wb[k] = 0.f;
+#pragma unroll
+    for (int i = 0; i < KC; ++i) {
+      prob[i] /= psum;
+      float x[4], sp[4], den, pr[4], rec[3];
+      tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, x, sp, den, pr, rec);
+      Wb[0] += prob[i] * x[0];
+      Wb[1] += prob[i] * x[1];
+      Wb[i + 2] += prob[i] * x[2];
+      Wb[(i + 1) % KC + 2] += prob[i] * x[3];
+    }
+    float Wc[K], m[K], s_raw = 0.f, s = 1.f;
+    if (clamp) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        m[k] = fmaxf(Wb[k], 0.f);
+        s_raw += m[k];
+      }
+      s = fmaxf(s_raw, 1e-8f);
+#pragma unroll
+      for (int k = 0; k < K; ++k) Wc[k] = m[k] / s;
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) Wc[k] = Wb[k];
+    }
+    float gW[K];  // d loss / d target
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float wt = layer[k * hw + p];
+      const float d = wt - Wc[k];
+      float g;
+      if (kind == 0) {
+        lgeo += d * d;
+        g = 2.f * d * inv_n;
+      } else {
+        lgeo += fabsf(d);
+        g = (d > 0.f ? 1.f : d < 0.f ? -1.f : 0.f) * inv_n;
+      }
+      lpos += fmaxf(-wt, 0.f);
+      if (dlayer) dlayer[k * hw + p] = g + (wt < 0.f ? -lambda_pos * inv_n : 0.f);
+      if (wbary) wbary[k * hw + p] = Wc[k];
+      gW[k] = -g;
+    }
+    if (!dchroma) continue;
+    // through the clamp and renormalisation
+    float gWb[K];
+    if (clamp) {
+      float gm_dot = 0.f;
+#pragma unroll
+      for (int k = 0; k < K; ++k) gm_dot += gW[k] * m[k];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const float gm = s_raw > 1e-8f ? gW[k] / s - gm_dot / (s * s) : gW[k] / s;
+        gWb[k] = Wb[k] > 0.f ? gm : 0.f;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) gWb[k] = gW[k];
+    }
+    // W = sum_i prob_i raw_i: raw path and softmax path
+    float gprob[KC], gdot = 0.f;
+#pragma unroll
+    for (int i = 0; i < KC; ++i) {
+      float x[4], sp[4], den, pr[4], rec[3];
+      tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, x, sp, den, pr, rec);
+      gprob[i] = x[0] * gWb[0] + x[1] * gWb[1] + x[2] * gWb[i + 2] + x[3] * gWb[(i + 1) % KC + 2];
+      gdot += prob[i] * gprob[i];
+    }
+#pragma unroll
+    for (int i = 0; i < KC; ++i) {
+      const float gerr = -prob[i] * (gprob[i] - gdot) / kBaryTau;
+      if (prob[i] == 0.f && gerr == 0.f) continue;  // contributes nothing
+      const TetraConst<KC>& T = s_t[i];
+      const int ti = i, tj = (i + 1) % KC;
+      const float* Pi = s_p[ti];
+      const float* Pj = s_p[tj];
+      float x[4], sp[4], den, pr[4], rec[3];
+      tetra_forward<KC>(T, Pi, Pj, C, x, sp, den, pr, rec);
+      float gx[4] = {prob[i] * gWb[0], prob[i] * gWb[1], prob[i] * gWb[ti + 2],
+                     prob[i] * gWb[tj + 2]};
+      if (gerr != 0.f) {  // error path: err = |rec - C|^2
+        float grec[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) grec[c] = 2.f * (rec[c] - C[c]) * gerr;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          dP[ti][c] += grec[c] * pr[2];
+          dP[tj][c] += grec[c] * pr[3];
+        }
+        const float gpr[4] = {0.f, grec[0] + grec[1] + grec[2],
+                              grec[0] * Pi[0] + grec[1] * Pi[1] + grec[2] * Pi[2],
+                              grec[0] * Pj[0] + grec[1] * Pj[1] + grec[2] * Pj[2]};
+        const float gps = (gpr[0] * sp[0] + gpr[1] * sp[1] + gpr[2] * sp[2] + gpr[3] * sp[3]) /
+                          (den * den);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gx[k] += (gpr[k] / den - gps) * softplus_grad(x[k]);
+      }
+      // coords (beta, gamma, delta) = A^-1 C; alpha = 1 - sum
+      const float gco[3] = {gx[1] - gx[0], gx[2] - gx[0], gx[3] - gx[0]};
+      float v[3];  // A^-T gco
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        v[c] = T.ainv[c] * gco[0] + T.ainv[3 + c] * gco[1] + T.ainv[6 + c] * gco[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dP[ti][c] -= v[c] * x[2];
+        dP[tj][c] -= v[c] * x[3];
+      }
+    }
+  }
+  // block reduction: dchroma (3 KC values), geo and pos loss sums
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float vals[3 * KC + 2];
+#pragma unroll
+  for (int i = 0; i < KC; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vals[3 * i + c] = dP[i][c];
+  vals[3 * KC] = lgeo;
+  vals[3 * KC + 1] = lpos;
+#pragma unroll
+  for (int k = 0; k < 3 * KC + 2; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vals[k] += __shfl_xor_sync(0xffffffffu, vals[k], o);
+    if (lane == 0) red[w][k] = vals[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3 * KC + 2) {
+    float t = 0.f;
+#pragma unroll
+    for (int k = 0; k < kLossThreads / 32; ++k) t += red[k][threadIdx.x];
+    if (threadIdx.x < 3 * KC) {
+      if (dchroma) atomicAdd(dchroma + threadIdx.x, t);
+    } else if (threadIdx.x == 3 * KC) {
+      atomicAdd(loss + 1, t * inv_n);
+      atomicAdd(loss, t * inv_n);
+    } else {
+      atomicAdd(loss + 2, t * lambda_pos * inv_n);
+      atomicAdd(loss, t * lambda_pos * inv_n);
+    }
+  }
+}
+
+int launch_palette_geo_loss(int KC, int H, int W, const float* layer, const float* target,
+                            const float* chroma, int clamp, int kind, float lambda_pos,
+                            float* wbary, float* loss, float* dlayer, float* dchroma,
+                            cudaStream_t st) {
+  const int64_t hw = (int64_t)H * W;
+  if (cudaMemsetAsync(loss, 0, sizeof(float) * 3, st) != cudaSuccess ||
+      (dchroma && cudaMemsetAsync(dchroma, 0, sizeof(float) * 3 * KC, st) != cudaSuccess))
+    return check_launch("palette_geo_loss (memset)", 0);
+  if (hw == 0) return GSB_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t need = (hw + kLossThreads - 1) / kLossThreads;
+  const int grid = (int)std::min<int64_t>(need, (int64_t)sms * 4);
+  const float inv_n = 1.f / (float)((int64_t)(KC + 2) * hw);
+  switch (KC) {
+#define GSB_KC(KK)                                                                                \
+  case KK:                                                                                        \
+    launch_pdl(k_palette_geo_loss<KK>, dim3(grid), dim3(kLossThreads), 0, st, hw, layer, target, \
+               chroma, clamp, kind, lambda_pos, inv_n, wbary, loss, dlayer, dchroma);           \
+    break;
+    GSB_KC(2) GSB_KC(3) GSB_KC(4) GSB_KC(5) GSB_KC(6)
+#undef GSB_KC
+    default: return GSB_ERR_INVALID_ARGUMENT;
+  }
+  return check_launch("palette_geo_loss");
+}
+
 }  // namespace gsb

@@ -25,6 +25,8 @@ DTYPE_F32 = 0
 DTYPE_BF16 = 1
 MAX_CHANNELS = 8
 WEIGHTS_FULL = 0
+LOSS_MSE = 0
+LOSS_L1 = 1
 WEIGHTS_LOWRANK = 1
 
 _i64, _i32, _u32, _f32, _p, _sz = C.c_int64, C.c_int, C.c_uint32, C.c_float, C.c_void_p, C.c_size_t
@@ -60,6 +62,8 @@ _SIGS = {
     "gsb_splat_backward": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _i32, _p, _p, _p, _p,
                                   _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_palette_l1": (_i32, [_i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "gsb_palette_geo_loss": (_i32, [_i32, _i32, _i32, _p, _p, _p, _i32, _i32, _f32, _p, _p, _p,
+                                    _p, _p]),
     "gsb_splat_backward_packed": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p,
                                          _p, _p, _p, _p]),
     "gsb_render_preprocess": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p]),

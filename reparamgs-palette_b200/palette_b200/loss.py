@@ -1,5 +1,13 @@
 """Fused loss-side operators.
 
+``palette_geo_loss(layer, chroma, target, clamp, lambda_pos, kind)`` is the
+finetune step's loss on the rendered palette weights (finetune.py:356-389):
+the barycentric target of the colour image in the palette {black, white,
+chroma} (gsplat/gsmodel.py:219-285), optionally clamped to non-negative and
+renormalised, then MSE (or L1) against the weights plus ``lambda_pos *
+mean(relu(-layer))``.  One kernel computes the loss and both gradients
+(the target depends on the learnt palette).
+
 ``palette_l1_loss(layer, palette, target)`` composites the palette colour
 image ``image[c] = sum_k palette[k][c] * layer[k]`` and returns
 ``mean(|image - target|)``; its forward pass also produces the adjoint w.r.t.
@@ -57,3 +65,57 @@ def palette_image(layer, palette):
                   _lib.ptr(zero), _lib.ptr(image), _lib.ptr(loss), None, None,
                   _lib.stream_of(layer))
     return image
+
+
+class PaletteGeoLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, layer, chroma, target, clamp, lambda_pos, kind):
+        if not (layer.is_cuda and layer.dtype == torch.float32):
+            raise TypeError("palette_geo_loss: layer must be a CUDA float32 tensor [K,H,W]")
+        layer = layer.contiguous()
+        chroma = chroma.detach().to(torch.float32).contiguous()
+        target = target.to(torch.float32).contiguous()
+        K, H, W = (int(x) for x in layer.shape)
+        Kc = int(chroma.shape[0])
+        if tuple(chroma.shape) != (Kc, 3) or K != Kc + 2 or tuple(target.shape) != (3, H, W):
+            raise ValueError("palette_geo_loss: layer must be [Kc+2,H,W], chroma [Kc,3] and "
+                             "target [3,H,W]")
+        loss = torch.empty((3,), dtype=torch.float32, device=layer.device)
+        dlayer = torch.empty_like(layer)
+        dchroma = torch.empty((Kc, 3), dtype=torch.float32, device=layer.device)
+        code = {"mse": _lib.LOSS_MSE, "l1": _lib.LOSS_L1}[kind]
+        with torch.cuda.device(layer.device):
+            _lib.call("palette_geo_loss", "gsb_palette_geo_loss", Kc, H, W, _lib.ptr(layer),
+                      _lib.ptr(target), _lib.ptr(chroma), int(bool(clamp)), code,
+                      float(lambda_pos), None, _lib.ptr(loss), _lib.ptr(dlayer),
+                      _lib.ptr(dchroma), _lib.stream_of(layer))
+        ctx.save_for_backward(dlayer, dchroma)
+        return loss[0]
+
+    @staticmethod
+    def backward(ctx, g):
+        dlayer, dchroma = ctx.saved_tensors
+        return dlayer * g, dchroma * g, None, None, None, None
+
+
+def palette_geo_loss(layer, chroma, target, clamp=False, lambda_pos=0.5, kind="mse"):
+    """Loss of rendered palette weights `layer` [Kc+2,H,W] against the
+    barycentric target of `target` [3,H,W] in {black, white, chroma [Kc,3]}."""
+    return PaletteGeoLoss.apply(layer, chroma, target, clamp, lambda_pos, kind)
+
+
+def barycentric_target(target, chroma, clamp=False):
+    """The (optionally clamped and renormalised) barycentric weights
+    [Kc+2,H,W] of the colour image `target` (no gradient)."""
+    chroma = chroma.detach().to(torch.float32).contiguous()
+    target = target.to(torch.float32).contiguous()
+    Kc = int(chroma.shape[0])
+    H, W = int(target.shape[1]), int(target.shape[2])
+    out = torch.empty((Kc + 2, H, W), dtype=torch.float32, device=target.device)
+    zero = torch.zeros_like(out)
+    loss = torch.empty((3,), dtype=torch.float32, device=target.device)
+    with torch.cuda.device(target.device):
+        _lib.call("barycentric_target", "gsb_palette_geo_loss", Kc, H, W, _lib.ptr(zero),
+                  _lib.ptr(target), _lib.ptr(chroma), int(bool(clamp)), _lib.LOSS_MSE, 0.0,
+                  _lib.ptr(out), _lib.ptr(loss), None, None, _lib.stream_of(target))
+    return out

@@ -84,3 +84,30 @@ def test_weight_function_test_gradients(cuda_ok):
     dw = _oracle_grads(st, sc, cam, w, G)
     expect = (dw[:, None, :] * np_of(dshs)[:, 0, :, None]).reshape(6000, -1)  # [N,16,K] outer
     assert rel_err(shs.grad, expect) < 1e-4
+
+
+@pytest.mark.parametrize("clamp,kind", [(False, "mse"), (True, "mse"), (True, "l1")])
+def test_palette_geo_loss_matches_oracle(cuda_ok, clamp, kind):
+    """The finetune loss kernel (barycentric target + MSE/L1 + negative-weight
+    penalty) against the FP64 oracle: loss, target weights, and both
+    gradients (weights; chromatic palette through the target)."""
+    from oracle import oracle as orc
+    from palette_b200.loss import barycentric_target, palette_geo_loss
+    g = torch.Generator().manual_seed(11)
+    H, W = 96, 128
+    chroma = torch.tensor([[0.85, 0.2, 0.15], [0.2, 0.75, 0.3], [0.25, 0.2, 0.85]]) + \
+        0.03 * torch.randn((3, 3), generator=g)
+    target = torch.rand((3, H, W), generator=g) * 0.9 + 0.05
+    layer = torch.randn((5, H, W), generator=g) * 0.3 + 0.2
+    ref = orc.palette_geo_loss(layer.double().numpy(), target.double().numpy(),
+                               chroma.double().numpy(), clamp=clamp, kind=kind)
+    L = layer.cuda().requires_grad_(True)
+    P = chroma.cuda().requires_grad_(True)
+    loss = palette_geo_loss(L, P, target.cuda(), clamp=clamp, lambda_pos=0.5, kind=kind)
+    loss.backward()
+    assert abs(float(loss) - ref["loss"]) < 1e-5 * max(1.0, abs(ref["loss"]))
+    wb = barycentric_target(target.cuda(), chroma.cuda(), clamp=clamp)
+    same = np.abs(np_of(wb) - ref["target_weights"]).max(axis=0) < 1e-4
+    assert same.mean() > 0.999  # pixels on a tetrahedron boundary may pick the other one
+    assert rel_err(L.grad, ref["dlayer"]) < 1e-4
+    assert rel_err(P.grad, ref["dchroma"]) < 1e-3
