@@ -6,10 +6,13 @@ path (WeightGSFunctionFast, gsplat/gsmodel.py:151-200) over 1,000,000
 synthetic Gaussians at 1920x1080 with rank-3 factors A [N,5,3], B [N,3,15]
 (P=5, Q=15, K=5, SH order 3, FP32 storage): forward through the gsplatcu
 operators (project, computeCov3D, computeCov2D, sh2Weight_fast, inverseCov2D,
-splat_weight), colour image = palette^T . layer and its L1 loss against a seeded random
-target (one fused kernel, palette_b200.loss), backward (splat_weight_B, sh2Weight_fast_B, dc and palette
-gradients).  `value` is whole-job fwd+bwd iterations per second with the
-scene resident in HBM; `frames_per_s` is the forward alone.
+splat_weight), the finetune loss (finetune.py:356-389) against a seeded random
+target image -- L1 between the rendered weights and the target's barycentric
+weights in the palette, clamped to non-negative and renormalised, plus
+0.5 * mean(relu(-weights)) (one fused kernel, palette_b200.loss) -- and the
+backward (splat_weight_B, sh2Weight_fast_B; dc, A, B and palette gradients).
+`value` is whole-job fwd+bwd iterations per second with the scene resident
+in HBM; `frames_per_s` is the forward alone.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -39,6 +42,10 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 METRIC = "1080p frames/s & fwd+bwd iters/s at 1M Gaussians; p50/p99 palette-edit latency"
+# The finetune step's loss on the rendered weights (finetune.py:356-389): L1
+# against the barycentric target of the target image in the palette, clamped
+# to non-negative and renormalised, plus the negative-weight penalty.
+LOSS = dict(clamp=True, lambda_pos=0.5, kind="l1")
 SAMPLE_TILE_STRIDE = 8  # CPU baseline composites every 8th tile and scales
 
 
@@ -71,7 +78,7 @@ def make_workload(a, device):
     wl = dict(sc=sc, cam=cam, K=5, Q=15, pws=t(sc["pws"]), rots=t(sc["rots"]),
               scales=t(sc["scales"]), alphas=t(sc["alphas"]),
               dc=t(sc["dc"]).requires_grad_(), A=t(sc["A"]).requires_grad_(),
-              B=t(sc["B"]).requires_grad_(), palette=t(sc["palette"]).requires_grad_())
+              B=t(sc["B"]).requires_grad_(), chroma=t(sc["palette"][2:]).requires_grad_())
     g = torch.Generator(device="cpu").manual_seed(a.seed)
     target = torch.rand((3, a.height, a.width), generator=g)
     wl["target_host"] = target.pin_memory() if device.type == "cuda" else target
@@ -83,14 +90,14 @@ def make_workload(a, device):
 
 def step(wl, cam=None, target=None, backward=True):
     from palette_b200.autograd import WeightGSFunctionFast
-    from palette_b200.loss import palette_l1_loss
+    from palette_b200.loss import palette_geo_loss
     cam = cam or wl["cam"]
     target = wl["target"] if target is None else target
-    for p in (wl["dc"], wl["A"], wl["B"], wl["palette"]):
+    for p in (wl["dc"], wl["A"], wl["B"], wl["chroma"]):
         p.grad = None
     layer, _ = WeightGSFunctionFast.apply(wl["pws"], wl["dc"], wl["A"], wl["B"], wl["alphas"],
                                           wl["scales"], wl["rots"], cam, wl["K"], wl["Q"])
-    loss = palette_l1_loss(layer, wl["palette"], target)
+    loss = palette_geo_loss(layer, wl["chroma"], target, **LOSS)
     if backward:
         loss.backward()
     return loss
@@ -100,13 +107,13 @@ def step_fused(wl, backward=True):
     """The same step through the fused render path (palette_b200.render): one
     preprocess kernel instead of five operators; weights-only backward, as
     the reference's backward (only dc, A, B and the palette need gradients)."""
-    from palette_b200.loss import palette_l1_loss
+    from palette_b200.loss import palette_geo_loss
     from palette_b200.render import render_palette
-    for p in (wl["dc"], wl["A"], wl["B"], wl["palette"]):
+    for p in (wl["dc"], wl["A"], wl["B"], wl["chroma"]):
         p.grad = None
     layer, _, _ = render_palette(wl["pws"], wl["rots"], wl["scales"], wl["alphas"], wl["cam"],
                                  dc=wl["dc"], A=wl["A"], B=wl["B"])
-    loss = palette_l1_loss(layer, wl["palette"], wl["target"])
+    loss = palette_geo_loss(layer, wl["chroma"], wl["target"], **LOSS)
     if backward:
         loss.backward()
     return loss
@@ -401,9 +408,9 @@ def serve_bench(a, device):
 
 # ----------------------------------------------------------- CPU baseline
 def cpu_step(wl, orc, stride):
-    """One bounded sample of the step on the host cores (CPU oracle, FP32):
-    full preprocess and binning of all Gaussians; forward and adjoint
-    compositing of every `stride`-th tile.  Returns extrapolated seconds for
+    """One bounded sample of the step on the host cores (CPU oracle, FP32;
+    the loss in FP64): full preprocess and binning of all Gaussians; forward
+    compositing, loss and adjoint compositing of every `stride`-th tile.  Returns extrapolated seconds for
     one full step and the sample's own seconds."""
     sc, cam, K, Q = wl["sc"], wl["cam"], wl["K"], wl["Q"]
     H, W = cam.height, cam.width
@@ -417,10 +424,17 @@ def cpu_step(wl, orc, stride):
     keep[::stride] = True
     ranges[~keep] = 0
     out, contrib, ft = orc.draw(H, W, K, ranges, b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w, 0.0)
-    pal = sc["palette"]
-    img = np.einsum("kc,khw->chw", pal, out)
-    dimg = np.sign(img - wl["target_host"].numpy()) / img.size
-    dlayer = np.einsum("kc,chw->khw", pal, dimg).astype(np.float32)
+    # the loss and its gradients on the composited tiles' pixels
+    gx = (W + 15) // 16
+    mask = np.zeros((H, W), bool)
+    for t in np.flatnonzero(keep):
+        ty, tx = divmod(int(t), gx)
+        mask[ty * 16:(ty + 1) * 16, tx * 16:(tx + 1) * 16] = True
+    tgt = wl["target_host"].numpy()
+    lo = orc.palette_geo_loss(out[:, mask][:, None, :], tgt[:, mask][:, None, :],
+                              sc["palette"][2:], **LOSS)
+    dlayer = np.zeros_like(out)
+    dlayer[:, mask] = lo["dlayer"][:, 0, :]
     g = orc.draw_backward(H, W, K, ranges, b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w, ft,
                           contrib, dlayer)
     t2 = time.perf_counter()
@@ -472,7 +486,8 @@ def run_reference(a):
 def config(a):
     return dict(workload=(f"palette-weight finetune step, low-rank fused path: {a.gaussians} "
                           f"Gaussians, {a.width}x{a.height}, rank-{a.rank} factors P=5 Q=15, K=5, "
-                          "SH order 3, FP32 storage, L1 loss on palette colour image"),
+                          "SH order 3, FP32 storage, L1 loss against the clamped and renormalised "
+                          "barycentric palette target + 0.5 negative-weight penalty"),
                 gaussians=a.gaussians, width=a.width, height=a.height, rank=a.rank,
                 parallelism="replicas" if a.gpus > 1 else "single-gpu",
                 l2="inputs larger than L2 (scene parameters ~%d MB > 126 MB L2)"

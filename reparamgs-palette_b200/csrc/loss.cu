@@ -120,6 +120,7 @@ int launch_palette_l1(int K, int H, int W, const float* layer, const float* pale
 // raw coordinates' dependence on A_i, and the softmax term, which is exactly
 // zero unless two tetrahedra's errors tie to within ~1e-7).
 constexpr float kBaryTau = 1e-9f, kBaryEps = 1e-12f;
+constexpr int kGeoThreads = 128;  // ~140 registers per thread: 3 blocks per SM
 
 template <int KC>
 struct TetraConst {
@@ -127,7 +128,12 @@ struct TetraConst {
   int i, j;
 };
 
-__device__ __forceinline__ float softplus_f(float x) { return x > 20.f ? x : log1pf(expf(x)); }
+// The softplus values only rank the tetrahedra by reconstruction error (the
+// target weights are the exact coordinates), so the fast exp/log intrinsics
+// are used; they can change the choice only between near-tied tetrahedra.
+__device__ __forceinline__ float softplus_f(float x) {
+  return x > 20.f ? x : __logf(1.f + __expf(x));
+}
 __device__ __forceinline__ float softplus_grad(float x) {
   return x > 20.f ? 1.f : 1.f / (1.f + expf(-x));
 }
@@ -152,8 +158,9 @@ __device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const fl
     sp[k] = softplus_f(x[k]);
     den += sp[k];
   }
+  const float rden = 1.f / den;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) pr[k] = sp[k] / den;
+  for (int k = 0; k < 4; ++k) pr[k] = sp[k] * rden;
   float err = 0.f;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -165,7 +172,7 @@ __device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const fl
 }
 
 template <int KC>
-__global__ void __launch_bounds__(kLossThreads, 2)
+__global__ void __launch_bounds__(kGeoThreads)
     k_palette_geo_loss(int64_t hw, const float* __restrict__ layer,
                        const float* __restrict__ target, const float* __restrict__ chroma,
                        int clamp, int kind, float lambda_pos, float inv_n,
@@ -175,7 +182,7 @@ __global__ void __launch_bounds__(kLossThreads, 2)
   constexpr int K = KC + 2;
   __shared__ TetraConst<KC> s_t[KC];
   __shared__ float s_p[KC][3];
-  __shared__ float red[kLossThreads / 32][3 * KC + 2];
+  __shared__ float red[kGeoThreads / 32][3 * KC + 2];
   if (threadIdx.x < 3 * KC) s_p[threadIdx.x / 3][threadIdx.x % 3] = chroma[threadIdx.x];
   __syncthreads();
   if (threadIdx.x < KC) {
@@ -214,34 +221,33 @@ __global__ void __launch_bounds__(kLossThreads, 2)
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < hw;
        p += (int64_t)gridDim.x * blockDim.x) {
     const float C[3] = {target[p], target[hw + p], target[2 * hw + p]};
-    float err[KC];
+    float err[KC], xs[KC][4];  // per tetrahedron: error and coordinates
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
-      float x[4], sp[4], den, pr[4], rec[3];
-      err[i] = tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, x, sp, den, pr, rec);
+      float sp[4], den, pr[4], rec[3];
+      err[i] = tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, xs[i], sp, den, pr, rec);
     }
     // softmax over the tetrahedra of -err / tau (shifted by the maximum)
-    float lmax = -INFINITY;
+    float emin = INFINITY;
 #pragma unroll
-    for (int i = 0; i < KC; ++i) lmax = fmaxf(lmax, -err[i] / kBaryTau);
+    for (int i = 0; i < KC; ++i) emin = fminf(emin, err[i]);
     float prob[KC], psum = 0.f;
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
-      prob[i] = expf(-err[i] / kBaryTau - lmax);
+      prob[i] = expf((emin - err[i]) * (1.f / kBaryTau));
       psum += prob[i];
     }
+    const float rpsum = 1.f / psum;
     float Wb[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) Wb[k] = 0.f;
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
-      prob[i] /= psum;
-      float x[4], sp[4], den, pr[4], rec[3];
-      tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, x, sp, den, pr, rec);
-      Wb[0] += prob[i] * x[0];
-      Wb[1] += prob[i] * x[1];
-      Wb[i + 2] += prob[i] * x[2];
-      Wb[(i + 1) % KC + 2] += prob[i] * x[3];
+      prob[i] *= rpsum;
+      Wb[0] += prob[i] * xs[i][0];
+      Wb[1] += prob[i] * xs[i][1];
+      Wb[i + 2] += prob[i] * xs[i][2];
+      Wb[(i + 1) % KC + 2] += prob[i] * xs[i][3];
     }
     float Wc[K], m[K], s_raw = 0.f, s = 1.f;
     if (clamp) {
@@ -251,8 +257,9 @@ __global__ void __launch_bounds__(kLossThreads, 2)
         s_raw += m[k];
       }
       s = fmaxf(s_raw, 1e-8f);
+      const float rs = 1.f / s;
 #pragma unroll
-      for (int k = 0; k < K; ++k) Wc[k] = m[k] / s;
+      for (int k = 0; k < K; ++k) Wc[k] = m[k] * rs;
     } else {
 #pragma unroll
       for (int k = 0; k < K; ++k) Wc[k] = Wb[k];
@@ -282,9 +289,10 @@ __global__ void __launch_bounds__(kLossThreads, 2)
       float gm_dot = 0.f;
 #pragma unroll
       for (int k = 0; k < K; ++k) gm_dot += gW[k] * m[k];
+      const float rs = 1.f / s, corr = s_raw > 1e-8f ? gm_dot * rs * rs : 0.f;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        const float gm = s_raw > 1e-8f ? gW[k] / s - gm_dot / (s * s) : gW[k] / s;
+        const float gm = gW[k] * rs - corr;
         gWb[k] = Wb[k] > 0.f ? gm : 0.f;
       }
     } else {
@@ -295,24 +303,24 @@ __global__ void __launch_bounds__(kLossThreads, 2)
     float gprob[KC], gdot = 0.f;
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
-      float x[4], sp[4], den, pr[4], rec[3];
-      tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, x, sp, den, pr, rec);
+      const float* x = xs[i];
       gprob[i] = x[0] * gWb[0] + x[1] * gWb[1] + x[2] * gWb[i + 2] + x[3] * gWb[(i + 1) % KC + 2];
       gdot += prob[i] * gprob[i];
     }
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
-      const float gerr = -prob[i] * (gprob[i] - gdot) / kBaryTau;
+      const float gerr = -prob[i] * (gprob[i] - gdot) * (1.f / kBaryTau);
       if (prob[i] == 0.f && gerr == 0.f) continue;  // contributes nothing
       const TetraConst<KC>& T = s_t[i];
       const int ti = i, tj = (i + 1) % KC;
       const float* Pi = s_p[ti];
       const float* Pj = s_p[tj];
-      float x[4], sp[4], den, pr[4], rec[3];
-      tetra_forward<KC>(T, Pi, Pj, C, x, sp, den, pr, rec);
+      const float* x = xs[i];
       float gx[4] = {prob[i] * gWb[0], prob[i] * gWb[1], prob[i] * gWb[ti + 2],
                      prob[i] * gWb[tj + 2]};
-      if (gerr != 0.f) {  // error path: err = |rec - C|^2
+      if (gerr != 0.f) {  // error path (near-ties only): err = |rec - C|^2
+        float xr[4], sp[4], den, pr[4], rec[3];
+        tetra_forward<KC>(T, Pi, Pj, C, xr, sp, den, pr, rec);
         float grec[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) grec[c] = 2.f * (rec[c] - C[c]) * gerr;
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(kLossThreads, 2)
         const float gps = (gpr[0] * sp[0] + gpr[1] * sp[1] + gpr[2] * sp[2] + gpr[3] * sp[3]) /
                           (den * den);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) gx[k] += (gpr[k] / den - gps) * softplus_grad(x[k]);
+        for (int k = 0; k < 4; ++k) gx[k] += (gpr[k] / den - gps) * softplus_grad(xr[k]);
       }
       // coords (beta, gamma, delta) = A^-1 C; alpha = 1 - sum
       const float gco[3] = {gx[1] - gx[0], gx[2] - gx[0], gx[3] - gx[0]};
@@ -361,7 +369,7 @@ __global__ void __launch_bounds__(kLossThreads, 2)
   if (threadIdx.x < 3 * KC + 2) {
     float t = 0.f;
 #pragma unroll
-    for (int k = 0; k < kLossThreads / 32; ++k) t += red[k][threadIdx.x];
+    for (int k = 0; k < kGeoThreads / 32; ++k) t += red[k][threadIdx.x];
     if (threadIdx.x < 3 * KC) {
       if (dchroma) atomicAdd(dchroma + threadIdx.x, t);
     } else if (threadIdx.x == 3 * KC) {
@@ -386,13 +394,13 @@ int launch_palette_geo_loss(int KC, int H, int W, const float* layer, const floa
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t need = (hw + kLossThreads - 1) / kLossThreads;
-  const int grid = (int)std::min<int64_t>(need, (int64_t)sms * 4);
+  const int64_t need = (hw + kGeoThreads - 1) / kGeoThreads;
+  const int grid = (int)std::min<int64_t>(need, (int64_t)sms * 12);
   const float inv_n = 1.f / (float)((int64_t)(KC + 2) * hw);
   switch (KC) {
 #define GSB_KC(KK)                                                                                \
   case KK:                                                                                        \
-    launch_pdl(k_palette_geo_loss<KK>, dim3(grid), dim3(kLossThreads), 0, st, hw, layer, target, \
+    launch_pdl(k_palette_geo_loss<KK>, dim3(grid), dim3(kGeoThreads), 0, st, hw, layer, target, \
                chroma, clamp, kind, lambda_pos, inv_n, wbary, loss, dlayer, dchroma);           \
     break;
     GSB_KC(2) GSB_KC(3) GSB_KC(4) GSB_KC(5) GSB_KC(6)
