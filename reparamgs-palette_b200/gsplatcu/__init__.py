@@ -397,6 +397,25 @@ def splat_color_B(height, width, us, cinv2ds, alphas, depths, colors, contrib, f
     return [du, dq, da, dfeat]
 
 
+# The stage-1 extension of the same project (vanilla_3dgs/gsplatcu/ext.cpp:71-77)
+# names its colour splat `splat` / `splatB`; the backward also takes the
+# gradient of the final transmittance (vanilla_3dgs/gsplatcu/gausplat.cu:114-160),
+# which is how its training drives transparent regions empty
+# (vanilla_3dgs/gsplat/gsmodel.py:27-75).
+def splat(height, width, us, cinv2ds, alphas, depths, colors, areas):
+    """vanilla_3dgs/gsplatcu/gausplat.cu:24-112 -> [image [3,H,W], contrib, final_tau, ranges,
+    gsid] (final_tau of empty tiles is 1), as splat_color."""
+    return splat_color(height, width, us, cinv2ds, alphas, depths, colors, areas)
+
+
+def splatB(height, width, us, cinv2ds, alphas, depths, colors, contrib, final_tau,
+           patch_range_per_tile, gsid_per_patch, dloss_dgammas, dloss_dfinal_taus):
+    """vanilla_3dgs/gsplatcu/gausplat.cu:114-160 -> [dloss_dus [N,1,2], dloss_dcinv2ds [N,1,3],
+    dloss_dalphas [N,1,1], dloss_dcolors [N,1,3]], including the final-transmittance term."""
+    return splat_color_B(height, width, us, cinv2ds, alphas, depths, colors, contrib, final_tau,
+                         patch_range_per_tile, gsid_per_patch, dloss_dgammas, dloss_dfinal_taus)
+
+
 def lab2rgb(lab_image):
     """gsplatcu/gausplat.cu:623-641: [3,H,W] CIE Lab (L in [0,1]) -> sRGB [3,H,W]."""
     op = "lab2rgb"

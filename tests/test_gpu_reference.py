@@ -153,3 +153,35 @@ def test_jacobian_outputs_vs_reference(ref):
     ms = gsc.sh2Weight(st["shs"], st["pws"], cam.twc, True, 5)
     rs = ref.sh2Weight(st["shs"], st["pws"], cam.twc, True, 5)
     assert rel_err(ms[2], rs[2]) < 1e-5  # includes the reference's d Y_9 / d y form
+
+
+def test_vanilla_splat_and_final_tau_adjoint_vs_stage1_reference(cuda_ok):
+    """splat / splatB against the stage-1 extension (vanilla_3dgs/gsplatcu,
+    built from its sources by oracle/build_ref.py), whose backward carries the
+    final-transmittance gradient: lists, contributors and ranges bit-exact,
+    image and final T within 1e-5, gradients within 1e-4 relative."""
+    from oracle.build_ref import load_vanilla_ref
+    van = load_vanilla_ref()
+    if van is None:
+        pytest.skip("stage-1 reference build oracle/_ref/vanilla is not present")
+    n, W, H = 30000, 320, 240
+    st, cam = _setup(n, W, H, seed=6)
+    us, pcs, d = van.project(st["pws"], cam.Rcw, cam.tcw, cam.fx, cam.fy, cam.cx, cam.cy, False)
+    c3, = van.computeCov3D(st["rots"], st["scales"], d, False)
+    c2, = van.computeCov2D(c3, pcs, cam.Rcw, d, cam.fx, cam.fy, cam.width, cam.height, False)
+    col, = van.sh2Color(st["shs"][:, :48].contiguous(), st["pws"], cam.twc, False)
+    cinv, areas = van.inverseCov2D(c2, d, False)
+    dA, aA, dB, aB = d.clone(), areas.clone(), d.clone(), areas.clone()
+    ra = van.splat(H, W, us, cinv, st["alphas"], dA, col, aA)
+    ma = gsc.splat(H, W, us, cinv, st["alphas"], dB, col, aB)
+    for i in (1, 3, 4):
+        assert torch.equal(ma[i], ra[i])
+    assert torch.equal(dA, dB) and torch.equal(aA, aB)
+    assert max_abs(ma[0], ra[0]) <= 1e-5 and max_abs(ma[2], ra[2]) <= 1e-5
+    g = torch.randn((3, H, W), device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    gT = torch.randn((H, W), device="cuda", generator=torch.Generator("cuda").manual_seed(2))
+    gm = gsc.splatB(H, W, us, cinv, st["alphas"], dB, col, ma[1], ma[2], ma[3], ma[4], g, gT)
+    gr = van.splatB(H, W, us, cinv, st["alphas"], dA, col, ra[1], ra[2], ra[3], ra[4], g, gT)
+    for x, y, name in zip(gm, gr, ("dus", "dcinv", "dalphas", "dcolors")):
+        assert x.shape == y.shape, name
+        assert rel_err(x, y) < 1e-4, name
