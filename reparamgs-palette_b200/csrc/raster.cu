@@ -280,7 +280,7 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
 // (vanilla_3dgs/gsplatcu/kernel.cu:912-919).  As in the reference, the 0.99
 // clamp and max(0, .) are not differentiated.
 template <int K, bool GEOM, bool DTAU>
-__global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 6)
+__global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
     k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
                     const int32_t* __restrict__ gsid, const float4* __restrict__ records,
                     const int32_t* __restrict__ contrib, const float* __restrict__ final_tau,
