@@ -347,3 +347,45 @@ def test_splat_weight_overlapped_count_and_overflow_bitexact(cuda_ok):
         same = np_of(contrib) == ref["contrib"]
         assert same.mean() > 1 - 1e-4
         assert max_abs(np_of(layer)[:, same], ref["out"][:, same]) < IMG_TOL
+
+
+def test_backward_reuses_forward_records_only_when_inputs_unchanged(cuda_ok):
+    """splat_weight_B takes the forward's packed records when it is handed the
+    same, unmodified tensors; the result matches a fresh pack (up to the order
+    of the float atomics that sum a Gaussian's gradient over tiles), and an
+    input modified in place since the forward forces the fresh pack."""
+    n, W, H, eye = CASES[1]
+    sc, st = _scene(n, seed=44)
+    cam = _cam(W, H, eye)
+    pre = _gpu_pre(st, cam)
+    w, = gsc.sh2Weight(st["shs"], st["pws"], cam.twc, False, 5)
+    g = torch.randn((5, H, W), device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+
+    def fwd_bwd(release):
+        out = gsc.splat_weight(H, W, 5, pre["us"], pre["cinv"], st["alphas"], pre["depths"], w,
+                               pre["areas"].clone())
+        if release:
+            gsc.release_packed()
+        else:
+            assert len(gsc._PACKED) >= 1
+        dW, = gsc.splat_weight_B(H, W, 5, pre["us"], pre["cinv"], st["alphas"], pre["depths"], w,
+                                 *out[1:], g)
+        return out, dW
+
+    _, reused = fwd_bwd(release=False)
+    _, fresh = fwd_bwd(release=True)
+    assert rel_err(reused[:, 0], np_of(fresh[:, 0]).astype(np.float64)) < 1e-6
+    # modify the opacities in place after the forward: the cached records hold
+    # the old ones, so the backward must pack again (a fresh pack of the same
+    # call, with the cache emptied, is the expected answer)
+    out = gsc.splat_weight(H, W, 5, pre["us"], pre["cinv"], st["alphas"], pre["depths"], w,
+                           pre["areas"].clone())
+    alphas = st["alphas"]
+    alphas.mul_(0.5)
+    dW, = gsc.splat_weight_B(H, W, 5, pre["us"], pre["cinv"], alphas, pre["depths"], w,
+                             *out[1:], g)
+    gsc.release_packed()
+    dW2, = gsc.splat_weight_B(H, W, 5, pre["us"], pre["cinv"], alphas, pre["depths"], w,
+                              *out[1:], g)
+    assert rel_err(dW[:, 0], np_of(dW2[:, 0]).astype(np.float64)) < 1e-6
+    assert rel_err(dW[:, 0], np_of(fresh[:, 0]).astype(np.float64)) > 0.05
