@@ -12,7 +12,10 @@ weights in the palette, clamped to non-negative and renormalised, plus
 0.5 * mean(relu(-weights)) (one fused kernel, palette_b200.loss) -- and the
 backward (splat_weight_B, sh2Weight_fast_B; dc, A, B and palette gradients).
 `value` is whole-job fwd+bwd iterations per second with the scene resident
-in HBM; `frames_per_s` is the forward alone.
+in HBM; `frames_per_s` is the forward alone.  `multiview` is the
+differentiation workload on the same scene: steps of 8 views at 1920x1080
+from BF16 rank-3 factors, loss 0.8 L1 + 0.2 (1 - SSIM) + 0.5 mean(relu(-W))
+per view (fused render + fused loss kernel).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -117,6 +120,48 @@ def step_fused(wl, backward=True):
     if backward:
         loss.backward()
     return loss
+
+
+VIEWS = 8  # views per step of the multi-view finetune leg
+
+
+def make_views(wl, a, device):
+    """The multi-view leg's inputs: the scene's low-rank factors in BF16, a
+    learnt palette, VIEWS cameras on a sphere of radius 8 and one seeded
+    random target image per view."""
+    from palette_b200.scene import look_at, sphere_poses
+    sc = wl["sc"]
+    bf = lambda x: torch.from_numpy(x).to(device, torch.bfloat16).contiguous().requires_grad_()
+    g = torch.Generator(device="cpu").manual_seed(a.seed + 1)
+    return dict(dc=bf(sc["dc"]), A=bf(sc["A"]), B=bf(sc["B"]),
+                palette=torch.from_numpy(sc["palette"]).to(device).requires_grad_(),
+                cams=[look_at(e, width=a.width, height=a.height, device=device)
+                      for e in sphere_poses(VIEWS, 8.0, seed=a.seed)],
+                targets=[torch.rand((3, a.height, a.width), generator=g).to(device)
+                         for _ in range(VIEWS)])
+
+
+def step_views(wl, mv, backward=True):
+    """One step of the multi-view finetune workload: VIEWS views rendered
+    through the fused path from BF16 rank-3 factors (FP32 arithmetic), each
+    with 0.8 L1 + 0.2 (1 - SSIM) of its palette colour image against its
+    target plus 0.5 mean(relu(-weights)) (one fused kernel per view,
+    palette_b200.loss.palette_l1_ssim_loss), averaged over the views; the
+    backward gives dc, A, B (BF16) and palette gradients."""
+    from palette_b200.loss import palette_l1_ssim_loss
+    from palette_b200.render import render_palette
+    for p in (mv["dc"], mv["A"], mv["B"], mv["palette"]):
+        p.grad = None
+    total = None
+    for cam, tgt in zip(mv["cams"], mv["targets"]):
+        layer, _, _ = render_palette(wl["pws"], wl["rots"], wl["scales"], wl["alphas"], cam,
+                                     dc=mv["dc"], A=mv["A"], B=mv["B"])
+        loss = palette_l1_ssim_loss(layer, mv["palette"], tgt, lambda_ssim=0.2, lambda_pos=0.5)
+        total = loss if total is None else total + loss
+    total = total / len(mv["cams"])
+    if backward:
+        total.backward()
+    return total
 
 
 # ------------------------------------------------------------------- clocks
@@ -317,6 +362,10 @@ def stage_breakdown(wl, reps=5):
             _lib.ptr(state), _lib.ptr(ranges), _lib.ptr(gsid), _lib.ptr(contrib), _lib.ptr(ft),
             _lib.ptr(g), None, _lib.ptr(scratch), None, None, None, None, _lib.ptr(gdc),
             _lib.ptr(gA), _lib.ptr(gB), sp), reps, st) / reps
+        from palette_b200.loss import palette_l1_ssim_loss
+        pal = torch.from_numpy(wl["sc"]["palette"]).to(us.device)
+        out["l1_ssim_loss"] = timed(lambda: palette_l1_ssim_loss(layer, pal, wl["target"]),
+                                    reps, st) / reps
         visible = int((d > 0.2).sum())
         pix = H * W
         # algorithmic bytes: per patch 48 B record + 4 B id; per pixel K*4 + 8 B out;
@@ -559,6 +608,14 @@ def run_b200(a):
         fu_fms = allreduce_max(timed(lambda: step_fused(wl, backward=False), a.steps, stream),
                                world, device) / a.steps
 
+    # the multi-view finetune leg (8 views per step, BF16 factors, L1 + SSIM)
+    mv = make_views(wl, a, device)
+    for _ in range(3):
+        step_views(wl, mv)
+    mv_reps = max(2, a.steps // 4)
+    mv_ms = allreduce_max(timed(lambda: step_views(wl, mv), mv_reps, stream), world, device) / mv_reps
+    del mv
+
     stages, alg = stage_breakdown(wl)
     dom = max(("draw", "draw_backward"), key=lambda k: stages[k])
     dom_bytes = alg["bytes_draw"] if dom == "draw" else alg["bytes_bwd"]
@@ -590,6 +647,11 @@ def run_b200(a):
                     fused_path=dict(iters_per_s=round(world * 1000.0 / fu_ms, 3),
                                     ms_per_step=round(fu_ms, 4), forward_ms=round(fu_fms, 4),
                                     frames_per_s=round(world * 1000.0 / fu_fms, 2)),
+                    multiview=dict(views_per_step=VIEWS, storage="bf16 dc/A/B, FP32 arithmetic",
+                                   loss="0.8 L1 + 0.2 (1 - SSIM) + 0.5 mean(relu(-W))",
+                                   steps=mv_reps, ms_per_step=round(mv_ms, 4),
+                                   iters_per_s=round(world * 1000.0 / mv_ms, 3),
+                                   views_per_s=round(world * VIEWS * 1000.0 / mv_ms, 2)),
                     serving=serving,
                     stages_ms={k: round(v, 4) for k, v in stages.items()},
                     patches=alg["M"])

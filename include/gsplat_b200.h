@@ -276,6 +276,23 @@ int gsb_palette_geo_loss(int chroma_count, int height, int width, const float* l
                          float lambda_pos, float* target_weights, float* loss, float* dlayer,
                          float* dchroma, void* stream);
 
+/* The differentiation workload's loss, one launch (plus a one-block init): the
+ * colour image img_c = sum_k palette[k][c] layer_k and
+ *   loss[0] = (1 - lambda_ssim) loss[1] + lambda_ssim (1 - loss[2]) + loss[3],
+ *   loss[1] = mean |img - target|, loss[2] = mean SSIM(img, target),
+ *   loss[3] = lambda_pos mean(relu(-layer)),
+ * i.e. gau_loss (vanilla_3dgs/gsplat/pytorch_ssim.py:26-67: 11x11 Gaussian
+ * window, sigma 1.5, zero padding, C1 = (0.01 data_range)^2, C2 =
+ * (0.03 data_range)^2; data_range 1 there) plus the negative-weight penalty of
+ * finetune.py:375,381, with dlayer [K,H,W] and dpalette [K,3] its gradients
+ * (overwritten; either may be NULL) and image [3,H,W] (may be NULL) the colour
+ * image.  With palette NULL, layer is the colour image itself (K must be 3) and
+ * dlayer the image gradient: gau_loss alone when lambda_pos is 0. */
+int gsb_palette_l1_ssim(int K, int height, int width, const float* layer, const float* palette,
+                        const float* target, float lambda_ssim, float lambda_pos,
+                        float data_range, float* image, float* loss, float* dlayer,
+                        float* dpalette, void* stream);
+
 /* ============================================================ fused path
  * One view of the palette-weight rasterizer with the per-Gaussian work of
  * project / computeCov3D / computeCov2D / sh2Weight(_fast) / inverseCov2D /

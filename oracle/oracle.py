@@ -490,3 +490,87 @@ def palette_geo_loss(layer, target, chroma, clamp=True, lambda_pos=0.5, kind="ms
         dP[j] -= (Ainv_T_g * co[:, 2:3]).sum(0)
     return dict(loss=float(loss), target_weights=Wc.T.reshape(layer.shape),
                 dlayer=dWt.T.reshape(layer.shape), dchroma=dP)
+
+
+def ssim_window(window_size=11, sigma=1.5):
+    """The SSIM window as the reference builds it (vanilla_3dgs/gsplat/
+    pytorch_ssim.py:12-23), in FP32: g[x] = exp(-(x - size//2)^2 / (2 sigma^2))
+    rounded to FP32 and divided by its FP32 sum, the 2-D window the FP32
+    outer product g g^T.  Returns (g [size], window [size,size]) as float64
+    arrays holding those FP32 values."""
+    g = np.array([np.exp(-float(x - window_size // 2) ** 2 / (2.0 * sigma * sigma))
+                  for x in range(window_size)], dtype=np.float32)
+    g = (g / np.float32(g.astype(np.float64).sum())).astype(np.float32)
+    return g.astype(np.float64), np.outer(g, g).astype(np.float32).astype(np.float64)
+
+
+def _filter(a, w2):
+    """Per-channel 2-D filtering of a [C,H,W] with the window w2 (zero padding of
+    size//2 on every side, output the input's size): F.conv2d with groups=C and
+    padding=window//2 (pytorch_ssim.py:27-39).  w2 is point-symmetric, so the
+    same call is its own adjoint."""
+    r = w2.shape[0] // 2
+    C_, H, W = a.shape
+    p = np.zeros((C_, H + 2 * r, W + 2 * r))
+    p[:, r:r + H, r:r + W] = a
+    out = np.zeros_like(a, dtype=np.float64)
+    for i in range(w2.shape[0]):
+        for j in range(w2.shape[1]):
+            out += w2[i, j] * p[:, i:i + H, j:j + W]
+    return out
+
+
+def l1_ssim_loss(image, target, lambda_ssim=0.2, range_=1.0, window_size=11):
+    """gau_loss (vanilla_3dgs/gsplat/pytorch_ssim.py:26-67) in FP64:
+    loss = (1 - lambda) mean|x - y| + lambda (1 - mean SSIM(x, y)), the SSIM map
+    from the 11x11 sigma 1.5 window with C1 = (0.01 range)^2, C2 = (0.03 range)^2.
+    Returns dict(loss, l1, ssim, dimage) with dimage = d loss / d image.
+
+    The gradient: with mu_x = G*x, s_xx = G*x^2, s_xy = G*(xy) and the SSIM map
+    S = A1 A2 / (B1 B2), A1 = 2 mu_x mu_y + C1, A2 = 2 (s_xy - mu_x mu_y) + C2,
+    B1 = mu_x^2 + mu_y^2 + C1, B2 = s_xx - mu_x^2 + s_yy - mu_y^2 + C2,
+      dS/dmu_x = 2 mu_y (A2 - A1) / (B1 B2) - 2 mu_x S (1/B1 - 1/B2),
+      dS/ds_xx = -S / B2,   dS/ds_xy = 2 A1 / (B1 B2),
+    and d sum_p S(p) / dx(q) = (G*dS/dmu_x)(q) + 2 x(q) (G*dS/ds_xx)(q) +
+    y(q) (G*dS/ds_xy)(q) (the window is point-symmetric, so its adjoint under
+    zero padding is the same filter).  The window holds the reference's FP32
+    values, so the FP64 result equals the reference module run in FP64."""
+    x = np.asarray(image, np.float64)
+    y = np.asarray(target, np.float64)
+    _, g = ssim_window(window_size)
+    C1, C2 = (0.01 * range_) ** 2, (0.03 * range_) ** 2
+    mx, my = _filter(x, g), _filter(y, g)
+    sxx, syy, sxy = _filter(x * x, g), _filter(y * y, g), _filter(x * y, g)
+    A1 = 2 * mx * my + C1
+    A2 = 2 * (sxy - mx * my) + C2
+    B1 = mx * mx + my * my + C1
+    B2 = (sxx - mx * mx) + (syy - my * my) + C2
+    S = A1 * A2 / (B1 * B2)
+    n = x.size
+    l1 = np.abs(x - y).sum() / n
+    ssim = S.sum() / n
+    dmx = 2 * my * (A2 - A1) / (B1 * B2) - 2 * mx * S * (1 / B1 - 1 / B2)
+    dsxx = -S / B2
+    dsxy = 2 * A1 / (B1 * B2)
+    dS = _filter(dmx, g) + 2 * x * _filter(dsxx, g) + y * _filter(dsxy, g)
+    dimage = (1 - lambda_ssim) * np.sign(x - y) / n - lambda_ssim * dS / n
+    return dict(loss=float((1 - lambda_ssim) * l1 + lambda_ssim * (1 - ssim)), l1=float(l1),
+                ssim=float(ssim), dimage=dimage)
+
+
+def palette_l1_ssim_loss(layer, palette, target, lambda_ssim=0.2, lambda_pos=0.5, range_=1.0):
+    """The differentiation workload's finetune loss on the palette colour image
+    img = sum_k palette[k] layer_k, in FP64: gau_loss(img, target) plus
+    lambda_pos mean(relu(-layer)) (finetune.py:375,381).  Returns dict(loss, l1,
+    ssim, penalty (lambda_pos-scaled), image [3,H,W], dlayer [K,H,W],
+    dpalette [K,3])."""
+    layer = np.asarray(layer, np.float64)
+    P = np.asarray(palette, np.float64)
+    img = np.einsum("kc,khw->chw", P, layer)
+    r = l1_ssim_loss(img, target, lambda_ssim, range_)
+    dimg = r["dimage"]
+    pen = lambda_pos * np.maximum(-layer, 0.0).sum() / layer.size
+    dlayer = np.einsum("kc,chw->khw", P, dimg) - lambda_pos * (layer < 0) / layer.size
+    dpal = np.einsum("khw,chw->kc", layer, dimg)
+    return dict(loss=r["loss"] + float(pen), l1=r["l1"], ssim=r["ssim"], penalty=float(pen),
+                image=img, dlayer=dlayer, dpalette=dpal)

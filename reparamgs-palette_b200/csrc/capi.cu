@@ -2,6 +2,7 @@
 // argument validation, workspace carving and kernel launches.  No entry point
 // allocates device memory or synchronises, except gsb_splat_counts, which
 // must return the patch count to the host.
+#include <cmath>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -362,6 +363,25 @@ GSB_API int gsb_palette_l1(int K, int height, int width, const float* layer,
   GSB_CHECK_ARG(((int64_t)height * width == 0) || (layer && target), "palette_l1: null input");
   return launch_palette_l1(K, height, width, layer, palette, target, image, loss, dlayer, dpalette,
                            ST(stream));
+}
+
+GSB_API int gsb_palette_l1_ssim(int K, int height, int width, const float* layer,
+                                const float* palette, const float* target, float lambda_ssim,
+                                float lambda_pos, float data_range, float* image, float* loss,
+                                float* dlayer, float* dpalette, void* stream) {
+  GSB_CHECK_ARG(K >= 1 && K <= GSB_MAX_CHANNELS, "palette_l1_ssim: channels must be in [1, %d]",
+                GSB_MAX_CHANNELS);
+  GSB_CHECK_ARG(palette || K == 3, "palette_l1_ssim: without a palette the image has 3 channels");
+  GSB_CHECK_ARG(palette || !dpalette, "palette_l1_ssim: dpalette needs a palette");
+  GSB_CHECK_ARG(height >= 0 && width >= 0, "palette_l1_ssim: negative image size");
+  GSB_CHECK_ARG(loss, "palette_l1_ssim: null loss");
+  GSB_CHECK_ARG(((int64_t)height * width == 0) || (layer && target),
+                "palette_l1_ssim: null input");
+  GSB_CHECK_ARG(std::isfinite(lambda_ssim) && std::isfinite(lambda_pos) &&
+                    std::isfinite(data_range) && data_range > 0.f,
+                "palette_l1_ssim: lambdas must be finite and data_range positive");
+  return launch_palette_l1_ssim(K, height, width, layer, palette, target, lambda_ssim, lambda_pos,
+                                data_range, image, loss, dlayer, dpalette, ST(stream));
 }
 
 GSB_API int gsb_palette_geo_loss(int chroma_count, int height, int width, const float* layer,

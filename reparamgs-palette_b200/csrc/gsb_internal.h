@@ -38,6 +38,12 @@ int launch_palette_geo_loss(int KC, int H, int W, const float* layer, const floa
                             float* wbary, float* loss, float* dlayer, float* dchroma,
                             cudaStream_t st);
 
+// ssim.cu
+int launch_palette_l1_ssim(int K, int H, int W, const float* layer, const float* palette,
+                           const float* target, float lambda_ssim, float lambda_pos,
+                           float data_range, float* image, float* loss, float* dlayer,
+                           float* dpal, cudaStream_t st);
+
 // binning.cu -- per-Gaussian binning state carved out of one caller buffer.
 struct SplatState {
   float4* records;       // [n * rec_vec4]

@@ -64,6 +64,8 @@ _SIGS = {
     "gsb_palette_l1": (_i32, [_i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_palette_geo_loss": (_i32, [_i32, _i32, _i32, _p, _p, _p, _i32, _i32, _f32, _p, _p, _p,
                                     _p, _p]),
+    "gsb_palette_l1_ssim": (_i32, [_i32, _i32, _i32, _p, _p, _p, _f32, _f32, _f32, _p, _p, _p, _p,
+                                   _p]),
     "gsb_splat_backward_packed": (_i32, [_i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _p,
                                          _p, _p, _p, _p]),
     "gsb_render_preprocess": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p]),

@@ -15,6 +15,13 @@ image ``image[c] = sum_k palette[k][c] * layer[k]`` and returns
 the backward is a scale by the incoming gradient.  It replaces the torch
 ``einsum`` + L1 sequence a finetune step would otherwise run (whose backward
 is a large-K split GEMM).
+
+``palette_l1_ssim_loss(layer, palette, target, lambda_ssim, lambda_pos)`` is
+the differentiation workload's loss: gau_loss (vanilla_3dgs/gsplat/
+pytorch_ssim.py:64-67, ``(1 - lambda) L1 + lambda (1 - SSIM)`` with the 11x11
+sigma-1.5 window) on the palette colour image, plus ``lambda_pos *
+mean(relu(-layer))``; ``gau_loss(image, gt_image, loss_lambda)`` is the same
+kernel on a colour image.  One launch computes the loss and its gradient.
 """
 import torch
 
@@ -119,3 +126,65 @@ def barycentric_target(target, chroma, clamp=False):
                   _lib.ptr(target), _lib.ptr(chroma), int(bool(clamp)), _lib.LOSS_MSE, 0.0,
                   _lib.ptr(out), _lib.ptr(loss), None, None, _lib.stream_of(target))
     return out
+
+
+def _l1_ssim(name, K, H, W, layer, palette, target, lambda_ssim, lambda_pos, data_range,
+             need_grad):
+    dev = layer.device
+    loss = torch.empty((4,), dtype=torch.float32, device=dev)
+    dlayer = torch.empty_like(layer) if need_grad else None
+    dpal = torch.empty((K, 3), dtype=torch.float32, device=dev) if (
+        need_grad and palette is not None) else None
+    with torch.cuda.device(dev):
+        _lib.call(name, "gsb_palette_l1_ssim", K, H, W, _lib.ptr(layer),
+                  None if palette is None else _lib.ptr(palette), _lib.ptr(target),
+                  float(lambda_ssim), float(lambda_pos), float(data_range), None, _lib.ptr(loss),
+                  None if dlayer is None else _lib.ptr(dlayer),
+                  None if dpal is None else _lib.ptr(dpal), _lib.stream_of(layer))
+    return loss, dlayer, dpal
+
+
+class PaletteL1SsimLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, layer, palette, target, lambda_ssim, lambda_pos, data_range):
+        if not (layer.is_cuda and layer.dtype == torch.float32 and layer.dim() == 3):
+            raise TypeError("palette_l1_ssim_loss: layer must be a CUDA float32 tensor [K,H,W]")
+        layer = layer.contiguous()
+        K, H, W = (int(x) for x in layer.shape)
+        target = target.to(torch.float32).contiguous()
+        if palette is not None:
+            palette = palette.detach().to(torch.float32).contiguous()
+            if tuple(palette.shape) != (K, 3):
+                raise ValueError("palette_l1_ssim_loss: palette must be [K,3]")
+        elif K != 3:
+            raise ValueError("gau_loss: the image must be [3,H,W]")
+        if tuple(target.shape) != (3, H, W):
+            raise ValueError("palette_l1_ssim_loss: target must be [3,H,W]")
+        need = any(ctx.needs_input_grad[:2])
+        loss, dlayer, dpal = _l1_ssim("palette_l1_ssim_loss", K, H, W, layer, palette, target,
+                                      lambda_ssim, lambda_pos, data_range, need)
+        ctx.save_for_backward(dlayer, dpal)
+        return loss  # [total, L1, SSIM, penalty]; only the total is differentiated
+
+    @staticmethod
+    def backward(ctx, g):
+        dlayer, dpal = ctx.saved_tensors
+        g = g[0]
+        return (None if dlayer is None else dlayer * g, None if dpal is None else dpal * g,
+                None, None, None, None)
+
+
+def palette_l1_ssim_loss(layer, palette, target, lambda_ssim=0.2, lambda_pos=0.5,
+                         data_range=1.0, parts=False):
+    """(1 - lambda_ssim) mean|img - target| + lambda_ssim (1 - mean SSIM(img,
+    target)) + lambda_pos mean(relu(-layer)), img = sum_k palette[k] layer[k].
+    With ``parts`` also returns the tensor [total, L1, SSIM, penalty]."""
+    p = PaletteL1SsimLoss.apply(layer, palette, target, float(lambda_ssim), float(lambda_pos),
+                                float(data_range))
+    return (p[0], p.detach()) if parts else p[0]
+
+
+def gau_loss(image, gt_image, loss_lambda=0.2):
+    """gau_loss of vanilla_3dgs/gsplat/pytorch_ssim.py:64-67 on a colour image
+    [3,H,W]: (1 - loss_lambda) L1 + loss_lambda (1 - SSIM), one kernel."""
+    return PaletteL1SsimLoss.apply(image, None, gt_image, float(loss_lambda), 0.0, 1.0)[0]
