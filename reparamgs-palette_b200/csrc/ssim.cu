@@ -7,8 +7,8 @@
 // SSIM's gradient at a pixel q needs the SSIM partials at every pixel within
 // the window radius R = 5 of q, and each partial needs the window statistics
 // (mean, second moments) of the pixels within R of it.  A block therefore
-// owns a 32x32 output tile and stages the image and the target over the tile
-// plus 2R on every side; the statistics and partials are computed on the tile
+// owns a 32x32 output tile and stages the image (all three channels, from one
+// read of the layer stack) and the target over the tile plus 2R on every side; the statistics and partials are computed on the tile
 // plus R, and the partials are filtered back onto the tile.  The halo work is
 // recomputed by the neighbouring blocks instead of exchanged, so the loss and
 // its full gradient come out of one launch (the gradient of a mean does not
@@ -35,11 +35,12 @@ constexpr int kRunH1 = 3, kRunV1 = 3, kRunH2 = 4;
 static_assert(kSsimMR % kRunH1 == 0 && kSsimMR % kRunV1 == 0 && kSsimTile % kRunH2 == 0, "runs");
 static_assert(kSsimThreads == 8 * kSsimTile && kSsimPix == 4, "thread layout");
 
-constexpr size_t kSsimSmemFloats = 2 * kSsimXR * kSsimXR   // image, target
+constexpr size_t kSsimSmemFloats = 3 * kSsimXR * kSsimXR   // image, 3 channels
+                                   + kSsimXR * kSsimXR      // target, one channel
                                    + 5 * kSsimXR * kSsimMR  // horizontal pass of 5 statistics
                                    + 3 * kSsimMR * kSsimMR  // SSIM partials
                                    + 3 * 8;                 // palette
-constexpr size_t kSsimSmemBytes = kSsimSmemFloats * sizeof(float);
+constexpr size_t kSsimSmemBytes = kSsimSmemFloats * sizeof(float);  // 108.3 KB: 2 blocks/SM
 
 struct SsimWindow {
   float g[kSsimTaps];
@@ -69,10 +70,11 @@ __global__ void __launch_bounds__(kSsimThreads, 2)
                       float* __restrict__ loss, float* __restrict__ dlayer,
                       float* __restrict__ dpal) {
   pdl_wait();
+  constexpr int XR2 = kSsimXR * kSsimXR;
   extern __shared__ float smem[];
-  float* sX = smem;                             // [52][52] image channel c
-  float* sY = sX + kSsimXR * kSsimXR;           // [52][52] target channel c
-  float* sH = sY + kSsimXR * kSsimXR;           // [5][52][42], later [3][42][32]
+  float* sX3 = smem;                            // [3][52][52] image
+  float* sY = sX3 + 3 * XR2;                    // [52][52] target channel c
+  float* sH = sY + XR2;                         // [5][52][42], later [3][42][32]
   float* sM = sH + 5 * kSsimXR * kSsimMR;       // [3][42][42]
   float* sP = sM + 3 * kSsimMR * kSsimMR;       // [K][3]
   __shared__ float red[kSsimThreads / 32][3 + 3 * K];
@@ -81,45 +83,66 @@ __global__ void __launch_bounds__(kSsimThreads, 2)
   const int x0 = blockIdx.x * kSsimTile, y0 = blockIdx.y * kSsimTile;
   const int64_t hw = (int64_t)H * W;
   if (tid < 3 * K) sP[tid] = PAL ? palette[tid] : (tid / 3 == tid % 3 ? 1.f : 0.f);
+  __syncthreads();
 
-  // this thread's output pixels: column tx, rows ty0 .. ty0 + 3 of the tile
-  const int tx = tid & 31, ty0 = (tid >> 5) * kSsimPix;
-  const int gx = x0 + tx;
-  float lv[kSsimPix][K], dl[kSsimPix][K], dp[K][3];
+  // 0. the image over the tile + 2R, all three channels (zero outside), from
+  //    one read of the layer stack; positions four at a time so each thread
+  //    has 4K loads in flight
+  constexpr int kStage = (XR2 + kSsimThreads - 1) / kSsimThreads;  // 11 positions per thread
+#pragma unroll 1
+  for (int e0 = 0; e0 < kStage; e0 += 4) {
+    float l[4][K];
 #pragma unroll
-  for (int o = 0; o < kSsimPix; ++o) {
-    const int gy = y0 + ty0 + o;
-    const bool in = gx < W && gy < H;
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + (e0 + u) * kSsimThreads;
+      const int r = e / kSsimXR, q = e - r * kSsimXR;
+      const int iy = y0 - 2 * kSsimR + r, ix = x0 - 2 * kSsimR + q;
+      const bool in = e0 + u < kStage && e < XR2 && iy >= 0 && iy < H && ix >= 0 && ix < W;
+      const int64_t p = in ? (int64_t)iy * W + ix : 0;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      lv[o][k] = in ? layer[k * hw + (int64_t)gy * W + gx] : 0.f;
-      dl[o][k] = 0.f;
+      for (int k = 0; k < K; ++k) l[u][k] = in ? layer[k * hw + p] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + (e0 + u) * kSsimThreads;
+      if (e0 + u < kStage && e < XR2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float xv = 0.f;
+#pragma unroll
+          for (int k = 0; k < K; ++k) xv = fmaf(sP[3 * k + c], l[u][k], xv);
+          sX3[c * XR2 + e] = xv;
+        }
+      }
     }
   }
-#pragma unroll
-  for (int k = 0; k < K; ++k) dp[k][0] = dp[k][1] = dp[k][2] = 0.f;
+
+  // this thread's output pixels: column tx, rows ty0 .. ty0 + 3 of the tile;
+  // dxs = d loss / d image there, per channel
+  const int tx = tid & 31, ty0 = (tid >> 5) * kSsimPix;
+  const int gx = x0 + tx;
+  float dxs[3][kSsimPix];
   float l1 = 0.f, ssum = 0.f;
-  __syncthreads();
 
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
-    // 1. stage the image and target channel over the tile + 2R (zero outside)
-    for (int e = tid; e < kSsimXR * kSsimXR; e += kSsimThreads) {
-      const int r = e / kSsimXR, q = e - r * kSsimXR;
-      const int iy = y0 - 2 * kSsimR + r, ix = x0 - 2 * kSsimR + q;
-      float xv = 0.f, yv = 0.f;
-      if (iy >= 0 && iy < H && ix >= 0 && ix < W) {
-        const int64_t p = (int64_t)iy * W + ix;
-        if (PAL) {
+    const float* sX = sX3 + c * XR2;
+    // 1. the target channel over the tile + 2R (zero outside), loads first
+    {
+      float yv[kStage];
 #pragma unroll
-          for (int k = 0; k < K; ++k) xv = fmaf(sP[3 * k + c], layer[k * hw + p], xv);
-        } else {
-          xv = layer[c * hw + p];
-        }
-        yv = target[c * hw + p];
+      for (int u = 0; u < kStage; ++u) {
+        const int e = tid + u * kSsimThreads;
+        const int r = e / kSsimXR, q = e - r * kSsimXR;
+        const int iy = y0 - 2 * kSsimR + r, ix = x0 - 2 * kSsimR + q;
+        const bool in = e < XR2 && iy >= 0 && iy < H && ix >= 0 && ix < W;
+        yv[u] = in ? target[c * hw + (int64_t)iy * W + ix] : 0.f;
       }
-      sX[e] = xv;
-      sY[e] = yv;
+#pragma unroll
+      for (int u = 0; u < kStage; ++u) {
+        const int e = tid + u * kSsimThreads;
+        if (e < XR2) sY[e] = yv[u];
+      }
     }
     __syncthreads();
 
@@ -190,7 +213,9 @@ __global__ void __launch_bounds__(kSsimThreads, 2)
           const float A2 = 2.f * (a[4][o] - mxy) + sc.c2;
           const float B1 = mxx + myy + sc.c1;
           const float B2 = (a[2][o] - mxx) + (a[3][o] - myy) + sc.c2;
-          const float rB1 = 1.f / B1, rB2 = 1.f / B2;
+          // B1 >= C1 > 0 and B2 > 0 up to rounding: the fast reciprocal's
+          // relative error (2 ulp) is far below the gradient tolerance
+          const float rB1 = __fdividef(1.f, B1), rB2 = __fdividef(1.f, B2);
           const float inv = rB1 * rB2;
           const float S = A1 * A2 * inv;
           dm = 2.f * my * (A2 - A1) * inv - 2.f * mx * S * (rB1 - rB2);
@@ -234,7 +259,7 @@ __global__ void __launch_bounds__(kSsimThreads, 2)
     }
     __syncthreads();
 
-    // 5. vertical pass onto this thread's pixels, and the per-pixel gradient
+    // 5. vertical pass onto this thread's pixels, and d loss / d image there
     float gs[3][kSsimPix];
 #pragma unroll
     for (int m = 0; m < 3; ++m)
@@ -256,6 +281,7 @@ __global__ void __launch_bounds__(kSsimThreads, 2)
 #pragma unroll
     for (int o = 0; o < kSsimPix; ++o) {
       const int ty = ty0 + o, gy = y0 + ty;
+      float dx = 0.f;
       if (gx < W && gy < H) {
         const int s = (ty + 2 * kSsimR) * kSsimXR + tx + 2 * kSsimR;
         const float xv = sX[s], yv = sY[s];
@@ -263,34 +289,37 @@ __global__ void __launch_bounds__(kSsimThreads, 2)
         const float d = xv - yv;
         l1 += fabsf(d);
         const float sg = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
-        const float dx = sc.w_l1 * sg - sc.w_ssim * dS;
+        dx = sc.w_l1 * sg - sc.w_ssim * dS;
         if (image) image[c * hw + (int64_t)gy * W + gx] = xv;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          dl[o][k] = fmaf(sP[3 * k + c], dx, dl[o][k]);
-          // c is not a compile-time index: select instead of indexing, so dp
-          // stays in registers
-          const float t = lv[o][k] * dx;
-          dp[k][0] += c == 0 ? t : 0.f;
-          dp[k][1] += c == 1 ? t : 0.f;
-          dp[k][2] += c == 2 ? t : 0.f;
-        }
       }
+      // c is not a compile-time index: select, so dxs stays in registers
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+        if (cc == c) dxs[cc][o] = dx;
     }
-    __syncthreads();  // the next channel overwrites the staged tiles
+    __syncthreads();  // the next channel overwrites the staged target and passes
   }
 
-  // negative-weight penalty and the layer gradient
-  float pen = 0.f;
+  // layer and palette gradients, negative-weight penalty
+  float pen = 0.f, dp[K][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k) dp[k][0] = dp[k][1] = dp[k][2] = 0.f;
 #pragma unroll
   for (int o = 0; o < kSsimPix; ++o) {
     const int gy = y0 + ty0 + o;
     if (gx < W && gy < H) {
+      const int64_t p = (int64_t)gy * W + gx;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        const float l = lv[o][k];
+        const float l = layer[k * hw + p];
         pen += fmaxf(-l, 0.f);
-        if (dlayer) dlayer[k * hw + (int64_t)gy * W + gx] = dl[o][k] - (l < 0.f ? sc.w_pos : 0.f);
+        float g = l < 0.f ? -sc.w_pos : 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          g = fmaf(sP[3 * k + c], dxs[c][o], g);
+          dp[k][c] = fmaf(l, dxs[c][o], dp[k][c]);
+        }
+        if (dlayer) dlayer[k * hw + p] = g;
       }
     }
   }
