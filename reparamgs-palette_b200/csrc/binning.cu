@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kBinBlock)
     float4* rec = records + i * V;
 #pragma unroll
     for (int k = 0; k < kMaxChannels; ++k)
-      if (k < C) f[11 + k] = ld(feats, i * C + k);
+      if (k < C) f[record_channel(k)] = ld(feats, i * C + k);
 #pragma unroll
     for (int v = 0; v < 5; ++v)
       if (v < V) rec[v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);

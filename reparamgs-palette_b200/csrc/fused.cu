@@ -195,11 +195,11 @@ __global__ void __launch_bounds__(kFuseThreads)
               float acc = 0.f;
 #pragma unroll
               for (int k = 0; k < K; ++k) acc += w[k] * s_pal[3 * k + c];
-              f[11 + c] = acc;
+              f[record_channel(c)] = acc;
             }
           } else {
 #pragma unroll
-            for (int k = 0; k < K; ++k) f[11 + k] = w[k];
+            for (int k = 0; k < K; ++k) f[record_channel(k)] = w[k];
           }
         }
       }

@@ -69,6 +69,8 @@ struct RecordLayout {
   static constexpr int kFloats = ((11 + K) + 3) / 4 * 4;
   static constexpr int kVec4 = kFloats / 4;
 };
+// Float index of channel k inside a record (gsb_record.cuh).
+__host__ __device__ constexpr int record_channel(int k) { return k == 0 ? 7 : 11 + k; }
 
 // ----------------------------------------------------------- error plumbing
 void set_error(const char* fmt, ...);

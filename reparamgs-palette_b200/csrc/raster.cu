@@ -10,7 +10,8 @@
 // list is staged through shared memory in batches of 256 packed records;
 // within a batch every warp first tests 32 records at a time against its
 // pixel block (one record per lane, ballot) using the record's conservative
-// support box, then walks only the overlapping records in list order.  Per
+// support box and then its cut ellipse, then walks only the overlapping
+// records in list order.  Per
 // pixel, a record whose Mahalanobis distance exceeds its cut is skipped
 // without evaluating exp() -- the reference would skip it too
 // (alpha' < 0.002) -- and every other record is evaluated with the
@@ -69,31 +70,33 @@ __device__ __forceinline__ void stage_batch(const int32_t* __restrict__ gsid, in
   }
 }
 
-__device__ __forceinline__ bool box_overlaps_rect(float4 box, int wx, int wy, int ex, int ey) {
-  return box.y >= (float)wx && box.x <= (float)(wx + ex) && box.w >= (float)wy &&
-         box.z <= (float)(wy + ey);
+// First stage of the warp's record test: does the record's support box
+// u +- (hx, hy) meet the pixel block [x0, x0+ex] x [y0, y0+ey]?  Written so
+// that a non-finite centre passes (as an unbounded box does) and an empty
+// box (-inf extents) fails.
+__device__ __forceinline__ bool box_meets_block(float4 v0, float4 v2, int x0, int y0, int ex,
+                                                int ey) {
+  const float hx = 0.5f * (float)ex, hy = 0.5f * (float)ey;
+  return !(fabsf(v0.x - ((float)x0 + hx)) > v2.x + hx) &&
+         !(fabsf(v0.y - ((float)y0 + hy)) > v2.y + hy);
 }
 
 // Second, exact stage of the warp's record test: can the record's cut
-// ellipse d^T Q d <= cut reach the pixel block [x0,x1] x [y0,y1] at all?
+// ellipse d^T Q d <= c2 reach the pixel block [x0,x1] x [y0,y1] at all?
 // The minimum of the quadratic over the (continuous) block is 0 when the
 // centre lies inside, else it is attained on one of the four edges, where it
 // is a clamped 1-D quadratic minimum.  The record is dropped only when that
-// minimum exceeds the cut inflated exactly as the support box is (rounding of
-// the FP32 quadratic form grows with the conic's condition number): every
-// pixel of the block would then fail the per-pixel test maha <= cut, so the
-// results do not change.  Degenerate or ill-conditioned conics always pass
-// (their support box is unbounded too).
-__device__ __forceinline__ bool ellipse_meets_block(float4 v1, float4 v2, float x0, float y0,
-                                                    float x1, float y1) {
-  const float ux = v1.x, uy = v1.y, qa = v1.z, qb = v1.w, qc = v2.x, cut = v2.y;
-  if (!(isfinite(ux) && isfinite(uy)) || (ux >= x0 && ux <= x1 && uy >= y0 && uy <= y1))
+// minimum exceeds c2 (the cut already widened for the rounding of the FP32
+// quadratic form): every pixel of the block would then fail the per-pixel
+// test, so the results do not change.  Records whose conic is degenerate or
+// ill-conditioned carry c2 = +inf and always pass.
+__device__ __forceinline__ bool ellipse_meets_block(float4 v0, float4 v1, float4 v2, float x0,
+                                                    float y0, float x1, float y1) {
+  const float ux = v0.x, uy = v0.y, qa = v0.z, qb = v0.w, qc = v1.x, c2 = v1.y;
+  const float ia = v2.z, ic = v2.w;
+  if (!(c2 < INFINITY) || !(isfinite(ux) && isfinite(uy)) ||
+      (ux >= x0 && ux <= x1 && uy >= y0 && uy <= y1))
     return true;
-  const float det = qa * qc - qb * qb;
-  const float kappa = (qa + qc) * (qa + qc) / det;
-  if (!(det > 0.f && qa > 0.f && qc > 0.f && kappa < 1e5f)) return true;
-  const float c2 = cut * (1.f + 4e-6f * kappa) + 1e-3f;
-  const float ia = 1.f / qa, ic = 1.f / qc;
   float m = INFINITY;
   // vertical edges x = x0, x1: d_x fixed, d_y free in [uy - y1, uy - y0]
 #pragma unroll
@@ -114,10 +117,10 @@ __device__ __forceinline__ bool ellipse_meets_block(float4 v1, float4 v2, float 
 
 template <int K>
 __device__ __forceinline__ void load_feats(const float4* srec, int j, float v2w, float* f) {
-  f[0] = v2w;
+  f[0] = v2w;  // channel 0 sits in v1.w
 #pragma unroll
   for (int k = 1; k < K; ++k) {
-    const int idx = 11 + k;  // float index inside the record
+    const int idx = record_channel(k);  // float index inside the record
     const float4 q = srec[(idx >> 2) * kBatch + j];
     f[k] = (idx & 3) == 0 ? q.x : (idx & 3) == 1 ? q.y : (idx & 3) == 2 ? q.z : q.w;
   }
@@ -151,24 +154,24 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4)
     if (!__all_sync(0xffffffffu, done)) {
       for (int s = 0; s < cnt; s += 32) {
         const int j = s + (threadIdx.x & 31);
-        bool ov = j < cnt && box_overlaps_rect(srec[j], wx, wy, 7, 3);
+        bool ov = j < cnt && box_meets_block(srec[j], srec[2 * kBatch + j], wx, wy, 7, 3);
         if (ov)
-          ov = ellipse_meets_block(srec[kBatch + j], srec[2 * kBatch + j], (float)wx, (float)wy,
-                                   (float)(wx + 7), (float)(wy + 3));
+          ov = ellipse_meets_block(srec[j], srec[kBatch + j], srec[2 * kBatch + j], (float)wx,
+                                   (float)wy, (float)(wx + 7), (float)(wy + 3));
         unsigned mask = __ballot_sync(0xffffffffu, ov);
         while (mask) {
           const int jj = s + __ffs(mask) - 1;
           mask &= mask - 1;
           if (done) continue;
-          const float4 v1 = srec[kBatch + jj];      // ux uy qa qb
-          const float4 v2 = srec[2 * kBatch + jj];  // qc cut alpha f0
-          const float dx = v1.x - (float)px, dy = v1.y - (float)py;
-          const float maha = fmaxf(0.0f, maha_sq(v1.z, v1.w, v2.x, dx, dy));
-          if (maha > v2.y) continue;
-          const float ap = fminf(kAlphaMax, v2.z * expf(-0.5f * maha));
+          const float4 v0 = srec[jj];           // ux uy qa qb
+          const float4 v1 = srec[kBatch + jj];  // qc c2 alpha ch0
+          const float dx = v0.x - (float)px, dy = v0.y - (float)py;
+          const float maha = fmaxf(0.0f, maha_sq(v0.z, v0.w, v1.x, dx, dy));
+          if (maha > v1.y) continue;
+          const float ap = fminf(kAlphaMax, v1.z * expf(-0.5f * maha));
           if (ap < kAlphaMin) continue;
           float f[K];
-          load_feats<K>(srec, jj, v2.w, f);
+          load_feats<K>(srec, jj, v1.w, f);
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] += T * ap * f[k];
           cont = base + jj + 1;
@@ -236,12 +239,12 @@ struct BwdPixel {
 // One contributor of one pixel in the adjoint: recovers T, accumulates the
 // pixel's gradient terms into x (x[0..K) features, then alpha, u, conic).
 template <int K, bool GEOM, bool DTAU>
-__device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, float4 v1,
-                                              float4 v2, float dx, float dy, const float4* srec,
+__device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, float4 v0,
+                                              float4 v1, float dx, float dy, const float4* srec,
                                               int jj, float* x) {
-  if (!(idx < p.cont) || m > v2.y) return false;
+  if (!(idx < p.cont) || m > v1.y) return false;
   const float g = expf(-0.5f * m);
-  const float ap = fminf(kAlphaMax, v2.z * g);
+  const float ap = fminf(kAlphaMax, v1.z * g);
   if (ap < kAlphaMin) return false;
   const float one_m = 1.f - ap;
   p.T = __fdividef(p.T, one_m);
@@ -250,7 +253,7 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
   for (int k = 0; k < K; ++k) x[k] += p.dl[k] * wgt;
   if (GEOM) {
     float f[K];
-    load_feats<K>(srec, jj, v2.w, f);
+    load_feats<K>(srec, jj, v1.w, f);
     float dap = 0.f;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -259,8 +262,8 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
     }
     if (DTAU) dap += p.dTf * __fdividef(-p.Tf, one_m);
     x[K] += dap * g;                                    // alpha
-    x[K + 1] += dap * ((-v1.z * dx - v1.w * dy) * ap);  // u.x
-    x[K + 2] += dap * ((-v1.w * dx - v2.x * dy) * ap);  // u.y
+    x[K + 1] += dap * ((-v0.z * dx - v0.w * dy) * ap);  // u.x
+    x[K + 2] += dap * ((-v0.w * dx - v1.x * dy) * ap);  // u.y
     x[K + 3] += dap * (-0.5f * ap * (dx * dx));         // conic a
     x[K + 4] += dap * (-1.0f * ap * (dx * dy));         // conic b
     x[K + 5] += dap * (-0.5f * ap * (dy * dy));         // conic c
@@ -334,9 +337,9 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
     for (int s_hi = hi; s_hi > 0; s_hi -= 32) {
       const int s_lo = max(0, s_hi - 32);
       const int j = s_lo + lane;
-      bool ov = j < s_hi && box_overlaps_rect(srec[j], pp.wx, pp.wy, 7, 7);
+      bool ov = j < s_hi && box_meets_block(srec[j], srec[2 * kBatch + j], pp.wx, pp.wy, 7, 7);
       if (ov)
-        ov = ellipse_meets_block(srec[kBatch + j], srec[2 * kBatch + j], (float)pp.wx,
+        ov = ellipse_meets_block(srec[j], srec[kBatch + j], srec[2 * kBatch + j], (float)pp.wx,
                                  (float)pp.wy, (float)(pp.wx + 7), (float)(pp.wy + 7));
       unsigned mask = __ballot_sync(0xffffffffu, ov);
       while (mask) {
@@ -347,13 +350,13 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
         float x[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) x[v] = 0.f;
+        const float4 v0 = srec[jj];
         const float4 v1 = srec[kBatch + jj];
-        const float4 v2 = srec[2 * kBatch + jj];
-        const float dx = v1.x - fx, dy0 = v1.y - fy0, dy1 = v1.y - fy1;
-        const float m0 = fmaxf(0.f, maha_sq(v1.z, v1.w, v2.x, dx, dy0));
-        const float m1 = fmaxf(0.f, maha_sq(v1.z, v1.w, v2.x, dx, dy1));
-        bool hit = adjoint_pixel<K, GEOM, DTAU>(p[0], idx, m0, v1, v2, dx, dy0, srec, jj, x);
-        hit |= adjoint_pixel<K, GEOM, DTAU>(p[1], idx, m1, v1, v2, dx, dy1, srec, jj, x);
+        const float dx = v0.x - fx, dy0 = v0.y - fy0, dy1 = v0.y - fy1;
+        const float m0 = fmaxf(0.f, maha_sq(v0.z, v0.w, v1.x, dx, dy0));
+        const float m1 = fmaxf(0.f, maha_sq(v0.z, v0.w, v1.x, dx, dy1));
+        bool hit = adjoint_pixel<K, GEOM, DTAU>(p[0], idx, m0, v0, v1, dx, dy0, srec, jj, x);
+        hit |= adjoint_pixel<K, GEOM, DTAU>(p[1], idx, m1, v0, v1, dx, dy1, srec, jj, x);
         const unsigned cm = __ballot_sync(0xffffffffu, hit);
         if (!cm) continue;
         const int64_t g = sgid[jj];

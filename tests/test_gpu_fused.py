@@ -125,8 +125,8 @@ def test_fused_preprocess_state_matches_operator_sequence(cuda_ok, mode, rank, d
     assert np.array_equal(dep1, dep2)
     V = (11 + K + 3) // 4
     r1, r2 = (a[o[5]:o[5] + n * V * 16].view(np.float32).reshape(n, V * 4)[live] for a in (a1, a2))
-    names = ["xmin", "xmax", "ymin", "ymax", "ux", "uy", "qa", "qb", "qc", "cut", "alpha"] + \
-            [f"w{k}" for k in range(K)]
+    names = ["ux", "uy", "qa", "qb", "qc", "c2", "alpha", "w0", "hx", "hy", "ia", "ic"] + \
+            [f"w{k}" for k in range(1, K)]
     report = {}
     fin = np.isfinite(r1) & np.isfinite(r2)
     assert np.array_equal(np.isfinite(r1), np.isfinite(r2))
@@ -136,7 +136,7 @@ def test_fused_preprocess_state_matches_operator_sequence(cuda_ok, mode, rank, d
             scale = max(np.abs(r1[fin[:, j], j]).max(), 1e-30)
             report[nm] = (int(d.sum()), float(np.abs(r1[d, j] - r2[d, j]).max() / scale))
     print(f"record fields differing ({mode}, rank {rank}, {dtype}):", report)
-    for nm in ("ux", "uy", "cut", "alpha"):
+    for nm in ("ux", "uy", "alpha"):
         assert nm not in report, report
     assert all(v[1] < 1e-5 for v in report.values()), report
 
