@@ -172,7 +172,7 @@ int gsb_splat_sort(int64_t n, int height, int width, const gsb_splat_plan* plan,
  * they render (device memory owned by another runtime's pool, a plug-in
  * handed only its input and output buffers, a fixed start-up footprint):
  * the sort's temporaries live in one device array inside this library, of
- * gsb_splat_sort_static_max_bytes() bytes (32 MiB: about 1.9M patches with
+ * gsb_splat_sort_static_max_bytes() bytes (32 MiB: about 2.0M patches with
  * 32-bit keys, 1.3M with 64-bit keys), which every GPU that loads the library
  * holds until the process exits.  Plans needing more return GSB_ERR_CAPACITY
  * with a message; use gsb_splat_sort then.  Allocates nothing; the first

@@ -88,6 +88,32 @@ __device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t* war
   return base + incl - v;
 }
 
+// ------------------------------------------------------------------ zero
+// Clears up to two word arrays in one launch.  A kernel rather than memset
+// nodes, so that it joins the programmatic-dependent-launch chain of the
+// kernels around it.
+__global__ void k_zero2(uint32_t* __restrict__ a, int64_t na, uint32_t* __restrict__ b,
+                        int64_t nb) {
+  pdl_wait();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na + nb; i += stride) {
+    if (i < na)
+      a[i] = 0u;
+    else
+      b[i - na] = 0u;
+  }
+}
+
+int launch_zero2(void* a, int64_t na, void* b, int64_t nb, cudaStream_t st) {
+  if (!a) na = 0;
+  if (!b) nb = 0;
+  if (na + nb == 0) return GSB_OK;
+  const int64_t blocks = std::min<int64_t>((na + nb + 255) / 256, 148 * 8);
+  launch_pdl(k_zero2, dim3((unsigned)blocks), dim3(256), 0, st, (uint32_t*)a, na, (uint32_t*)b,
+             nb);
+  return check_launch("zero");
+}
+
 // ------------------------------------------------------------------ pack
 // One thread per Gaussian: tile rectangle and patch count (getRects,
 // gsplatcu/kernel.cu:127-162, including its in-place depth/areas updates),
@@ -232,8 +258,14 @@ __global__ void __launch_bounds__(kBinBlock)
     k_emit(int64_t n, uint32_t gx, int dkey_bits, const uint2* __restrict__ rects,
            const uint32_t* __restrict__ dkeys, const uint32_t* __restrict__ counts,
            const uint32_t* __restrict__ block_offs, KT* __restrict__ keys,
-           int32_t* __restrict__ vals, int64_t cap) {
+           int32_t* __restrict__ vals, int64_t cap, int2* __restrict__ ranges,
+           int64_t n_tiles) {
   pdl_wait();
+  // the ranges start empty (getRanges writes only tiles that have patches);
+  // cleared here, long before k_ranges writes them
+  for (int64_t t = (int64_t)blockIdx.x * kBinBlock + threadIdx.x; t < n_tiles;
+       t += (int64_t)gridDim.x * kBinBlock)
+    ranges[t] = make_int2(0, 0);
   __shared__ uint32_t warp_tot[8];
   __shared__ uint32_t s_incl[8][32];
   __shared__ uint2 s_rect[8][32];
@@ -276,8 +308,8 @@ __global__ void __launch_bounds__(kBinBlock)
 
 // ------------------------------------------------------------ radix sort
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 8;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
+constexpr int kSortItems = 12;  // measured: 8 -> 12 keys per thread, 7 % less sort time
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per block
 
 template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
@@ -462,8 +494,10 @@ static void pack_t(int64_t n, uint32_t gx, uint32_t gy, int C, const float* us, 
 int launch_pack(int64_t n, int H, int W, int channels, const float* us, const float* cinv,
                 const float* alphas, const void* feats, int feat_dtype, float* depths,
                 int32_t* areas, bool bin, const SplatState& s, cudaStream_t st) {
-  if (bin && cudaMemsetAsync(s.stats, 0, 16 * sizeof(uint32_t), st) != cudaSuccess)
-    return check_launch("splat_pack (memset)", 0);
+  if (bin) {
+    const int rc = launch_zero2(s.stats, 16, nullptr, 0, st);
+    if (rc) return rc;
+  }
   if (n == 0) return GSB_OK;
   const uint32_t gx = (uint32_t)div_up(W, kTile), gy = (uint32_t)div_up(H, kTile);
   if (feat_dtype == GSB_DTYPE_BF16)
@@ -532,7 +566,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
   uint32_t* dtot = (uint32_t*)(b + p.off_digit_tot);
   const uint32_t gx = (uint32_t)div_up(W, kTile);
   launch_pdl(k_emit<KT>, dim3((unsigned)s.n_blocks), dim3(kBinBlock), 0, st, n, gx, p.dkey_bits,
-             s.rects, s.dkeys, s.counts, s.block_sums, ka, p.passes == 0 ? gsid_out : va, p.M);
+             s.rects, s.dkeys, s.counts, s.block_sums, ka, p.passes == 0 ? gsid_out : va, p.M,
+             (int2*)ranges_out, p.n_tiles);
   int rc = check_launch("splat_sort (emit)");
   if (rc) return rc;
   const size_t smem =
@@ -573,9 +608,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
 int launch_sort(const SortPlan& p, int64_t n, int H, int W, const SplatState& s, void* ws,
                 int32_t* gsid_out, int32_t* ranges_out, cudaStream_t st) {
   (void)H;
-  if (cudaMemsetAsync(ranges_out, 0, (size_t)p.n_tiles * 2 * sizeof(int32_t), st) != cudaSuccess)
-    return check_launch("splat_sort (memset)", 0);
-  if (p.M == 0) return GSB_OK;
+  if (p.M == 0)  // no emission to clear the ranges
+    return launch_zero2(ranges_out, p.n_tiles * 2, nullptr, 0, st);
   return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, nullptr, st)
                 : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, nullptr, st);
 }
@@ -591,11 +625,11 @@ int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const Splat
                          void* ws, int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
                          cudaStream_t st) {
   (void)H;
-  if (cudaMemsetAsync(ranges_out, 0, (size_t)p.n_tiles * 2 * sizeof(int32_t), st) != cudaSuccess)
-    return check_launch("splat_sort_capacity (memset)", 0);
-  k_capacity_status<<<1, 1, 0, st>>>(p.M, p.dkey_bits, s.stats, status);
+  launch_pdl(k_capacity_status, dim3(1), dim3(1), 0, st, p.M, p.dkey_bits,
+             (const uint32_t*)s.stats, status);
   int rc = check_launch("splat_sort_capacity (status)");
-  if (rc || p.M == 0 || n == 0) return rc;
+  if (rc) return rc;
+  if (p.M == 0 || n == 0) return launch_zero2(ranges_out, p.n_tiles * 2, nullptr, 0, st);
   return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, s.stats, st)
                 : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, s.stats, st);
 }

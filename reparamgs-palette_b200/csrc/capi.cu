@@ -446,10 +446,9 @@ GSB_API int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float*
   GSB_CHECK_ARG(n == 0 || (pws && rots && scales && alphas), "render_preprocess: null input");
   const SplatState s =
       carve_state(state, n, params->palette ? 3 : params->K, cam->height, cam->width);
-  if (cudaMemsetAsync(s.stats, 0, 16 * sizeof(uint32_t), ST(stream)) != cudaSuccess ||
-      cudaMemsetAsync(s.block_sums, 0, (size_t)(s.n_blocks > 0 ? s.n_blocks : 1) * 4,
-                      ST(stream)) != cudaSuccess)
-    return check_launch("render_preprocess (memset)", 0);
+  if ((rc = launch_zero2(s.stats, 16, s.block_sums, s.n_blocks > 0 ? s.n_blocks : 1,
+                         ST(stream))))
+    return rc;
   FusedArgs f{};
   f.n = n;
   f.gx = (uint32_t)div_up(cam->width, kTile);
@@ -503,11 +502,9 @@ GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* p
   float* g_feat = (float*)scratch;
   float* g_u = g_feat + (size_t)n * K;
   float* g_conic = g_u + (size_t)n * 2;
-  if (n > 0 &&
-      (cudaMemsetAsync(scratch, 0, (size_t)n * (geom ? K + 5 : K) * sizeof(float), ST(stream)) !=
-           cudaSuccess ||
-       (geom && cudaMemsetAsync(dalphas, 0, (size_t)n * sizeof(float), ST(stream)) != cudaSuccess)))
-    return check_launch("render_backward (memset)", 0);
+  if (n > 0 && (rc = launch_zero2(scratch, n * (geom ? K + 5 : K), geom ? dalphas : nullptr,
+                                  geom ? n : 0, ST(stream))))
+    return rc;
   rc = launch_draw_backward(n, cam->height, cam->width, K, ranges, gsid, s, contrib, final_tau,
                             dloss_dout, geom ? dloss_dtau : nullptr, g_feat,
                             geom ? dalphas : nullptr, geom ? g_u : nullptr,

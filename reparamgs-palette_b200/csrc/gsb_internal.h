@@ -44,6 +44,10 @@ int launch_palette_l1_ssim(int K, int H, int W, const float* layer, const float*
                            float data_range, float* image, float* loss, float* dlayer,
                            float* dpal, cudaStream_t st);
 
+// binning.cu -- clears a[0, na) and b[0, nb) (32-bit words; either may be
+// null) in one kernel launched in the programmatic-dependent-launch chain.
+int launch_zero2(void* a, int64_t na, void* b, int64_t nb, cudaStream_t st);
+
 // binning.cu -- per-Gaussian binning state carved out of one caller buffer.
 struct SplatState {
   float4* records;       // [n * rec_vec4]

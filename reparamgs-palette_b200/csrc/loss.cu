@@ -79,9 +79,10 @@ int launch_palette_l1(int K, int H, int W, const float* layer, const float* pale
                       const float* target, float* image, float* loss, float* dlayer, float* dpal,
                       cudaStream_t st) {
   const int64_t hw = (int64_t)H * W;
-  if (cudaMemsetAsync(loss, 0, sizeof(float), st) != cudaSuccess ||
-      (dpal && cudaMemsetAsync(dpal, 0, sizeof(float) * 3 * K, st) != cudaSuccess))
-    return check_launch("palette_l1 (memset)", 0);
+  {
+    const int rc = launch_zero2(loss, 1, dpal, 3 * K, st);
+    if (rc) return rc;
+  }
   if (hw == 0) return GSB_OK;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -387,9 +388,10 @@ int launch_palette_geo_loss(int KC, int H, int W, const float* layer, const floa
                             float* wbary, float* loss, float* dlayer, float* dchroma,
                             cudaStream_t st) {
   const int64_t hw = (int64_t)H * W;
-  if (cudaMemsetAsync(loss, 0, sizeof(float) * 3, st) != cudaSuccess ||
-      (dchroma && cudaMemsetAsync(dchroma, 0, sizeof(float) * 3 * KC, st) != cudaSuccess))
-    return check_launch("palette_geo_loss (memset)", 0);
+  {
+    const int rc = launch_zero2(loss, 3, dchroma, 3 * KC, st);
+    if (rc) return rc;
+  }
   if (hw == 0) return GSB_OK;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);

@@ -26,7 +26,7 @@
 
 namespace gsb {
 
-// 32 MiB: about 1.9M patches with 32-bit keys, 1.3M with 64-bit keys.
+// 32 MiB: about 2.0M patches with 32-bit keys, 1.3M with 64-bit keys.
 constexpr size_t kStaticSortBytes = size_t(32) << 20;
 static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortBytes];
 
