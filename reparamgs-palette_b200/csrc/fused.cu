@@ -116,6 +116,33 @@ __device__ __forceinline__ bool stage_params(int64_t n, int64_t row0, const floa
   return true;
 }
 
+// Full-SH rows are 16K floats long, a multiple of 16: read one row per
+// thread, the 32 lanes of a warp would hit 2 (or 1) of the 32 shared-memory
+// banks.  Rows of even length are therefore copied once to an odd stride
+// before the per-thread reads (the accumulation order is unchanged).
+template <int W>
+struct PadRows {
+  static constexpr bool kPad = W > 1 && W % 2 == 0;
+  static constexpr int kStride = kPad ? W + 1 : W;
+  static constexpr int kExtra = kPad ? W + 1 : 0;  // extra floats per thread
+};
+
+template <int W>
+__device__ __forceinline__ const float* pad_rows(const float* rows, float* pad, bool copy) {
+  if constexpr (!PadRows<W>::kPad) {
+    return rows;
+  } else {
+    const int nt = blockDim.x;
+    if (copy)
+      for (int e = threadIdx.x; e < nt * W; e += nt) {
+        const int r = e / W, c = e - r * W;
+        pad[r * (W + 1) + c] = rows[e];
+      }
+    __syncthreads();
+    return pad;
+  }
+}
+
 // Palette weights of one Gaussian from its staged parameter rows.
 template <int MODE, int K, int P, int Q, int R>
 __device__ __forceinline__ void weights_of(const float* w0, const float* wa, const float* wb,
@@ -159,6 +186,7 @@ __global__ void __launch_bounds__(kFuseThreads)
   const bool staged = stage_params<MODE, K, P, Q, R, T>(n, row0, pws, rots, scales, alphas, w0,
                                                         wa, wb, sm, &bar);
   const Staged<MODE, K, P, Q, R> S(sm);
+  const float* w0rows = pad_rows<WS::W0>(S.w0, sm + nt * WS::IN, staged);
   const int64_t i = row0 + t;
   uint32_t cnt = 0, dk = 0;
   float f[4 * V];  // this Gaussian's record (kept until the block writes its records)
@@ -186,8 +214,8 @@ __global__ void __launch_bounds__(kFuseThreads)
           float dir[3], Y[16], w[K];
           view_direction(pw, make_float3(cr.c[0], cr.c[1], cr.c[2]), dir, nullptr, nullptr);
           sh_basis(dir, WS::L + 1, Y);
-          weights_of<MODE, K, P, Q, R>(S.w0 + t * WS::W0, S.wa + t * WS::WA, S.wb + t * WS::WB,
-                                       Y, w);
+          weights_of<MODE, K, P, Q, R>(w0rows + t * PadRows<WS::W0>::kStride, S.wa + t * WS::WA,
+                                       S.wb + t * WS::WB, Y, w);
           record_head(p.ux, p.uy, conic[0], conic[1], conic[2], S.al[t], f);
           if constexpr (COL) {
 #pragma unroll
@@ -348,7 +376,10 @@ __global__ void __launch_bounds__(kFuseThreads)
                                                  &bar))
     return;
   const int64_t i = row0 + t;
-  float* o_w0 = sm + nt * BP::o_dw0 + t * WS::W0;
+  // full-SH gradient rows are built at an odd stride past the plan's regions
+  // (see PadRows) and packed contiguously before they are stored
+  using PR = PadRows<WS::W0>;
+  float* o_w0 = PR::kPad ? sm + nt * BP::floats + t * PR::kStride : sm + nt * BP::o_dw0 + t * WS::W0;
   float* o_wa = sm + nt * BP::o_dwa + t * WS::WA;
   float* o_wb = sm + nt * BP::o_dwb + t * WS::WB;
   if (i < n) {
@@ -498,6 +529,15 @@ __global__ void __launch_bounds__(kFuseThreads)
     }
   }
   // parameter gradients: shared memory -> global, block span by block span
+  if constexpr (PR::kPad) {
+    __syncthreads();
+    float* dst = sm + nt * BP::o_dw0;
+    const float* src = sm + nt * BP::floats;
+    for (int e = t; e < nt * WS::W0; e += nt) {
+      const int r = e / WS::W0, c = e - r * WS::W0;
+      dst[e] = src[r * PR::kStride + c];
+    }
+  }
   fence_proxy_async_shared();
   __syncthreads();
   write_rows<WS::W0>(d_w0, row0, n, sm + nt * BP::o_dw0);
@@ -520,7 +560,7 @@ static int set_smem(Kern kern, int smem) {
 template <int MODE, int K, int P, int Q, int R, typename T>
 static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   using WS = WRows<MODE, K, P, Q, R>;
-  const int smem = WS::IN * kFuseThreads * 4;
+  const int smem = (WS::IN + PadRows<WS::W0>::kExtra) * kFuseThreads * 4;
   const int grid = div_up(f.n, kFuseThreads);
   int rc;
   if (!backward) {
@@ -536,8 +576,10 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   const bool geom = f.g_u != nullptr;
   auto kern = geom ? k_render_backward_pre<MODE, K, P, Q, R, T, true>
                    : k_render_backward_pre<MODE, K, P, Q, R, T, false>;
-  const int bsmem = (geom ? BwdPlan<MODE, K, P, Q, R, true>::floats
-                          : BwdPlan<MODE, K, P, Q, R, false>::floats) * kFuseThreads * 4;
+  const int bsmem = ((geom ? BwdPlan<MODE, K, P, Q, R, true>::floats
+                           : BwdPlan<MODE, K, P, Q, R, false>::floats) +
+                     PadRows<WS::W0>::kExtra) *
+                    kFuseThreads * 4;
   if ((rc = set_smem(kern, bsmem))) return rc;
   launch_pdl(kern, dim3(grid), dim3(kFuseThreads), bsmem, st, f.n, f.cam, f.pws, f.rots,
              f.scales, (const T*)f.w0, (const T*)f.wa, (const T*)f.wb, f.g_feat, f.g_u, f.g_conic,
