@@ -76,44 +76,87 @@ struct Staged {
   }
 };
 
-// Stage one block's parameter rows (pws, rots, scales, alphas, colour
-// parameters) into shared memory, by bulk copies when every span is aligned
-// FP32 and the block is full.  Returns false if a bulk wait expired (the
-// status word is set and the block must not use the staged rows).
+// Extra shared memory of the forward, in floats per thread, past the staged
+// rows: the odd-stride copy of even-length rows (PadRows), then, for BF16
+// low-rank factors, their raw bulk-copied rows (full-SH BF16 rows land raw in
+// the float row area itself and are converted straight into the odd-stride
+// copy).
 template <int MODE, int K, int P, int Q, int R, typename T>
-__device__ __forceinline__ bool stage_params(int64_t n, int64_t row0, const float* pws,
-                                             const float* rots, const float* scales,
-                                             const float* alphas, const T* w0, const T* wa,
-                                             const T* wb, float* sm, uint64_t* bar) {
+struct FwdExtra {
+  using WS = WRows<MODE, K, P, Q, R>;
+  static constexpr bool kRawLowrank = sizeof(T) == 2 && MODE != GSB_WEIGHTS_FULL;
+  static constexpr int kRawFloats = kRawLowrank ? (WS::W0 + WS::WA + WS::WB + 1) / 2 : 0;
+};
+
+// How the block's colour-parameter rows ended up in shared memory.
+enum StageResult { kStageFailed = 0, kStagedFloat = 1, kStagedRawBf16 = 2 };
+
+// Stage one block's parameter rows (pws, rots, scales, alphas, colour
+// parameters) into shared memory, by bulk copies when the block is full and
+// every span is 16-byte aligned.  FP32 rows land in their float areas; BF16
+// colour rows are bulk-copied raw (full SH: into the float area of the SH
+// rows; low-rank: into `raw`) and converted by the caller (kStagedRawBf16).
+// Without bulk copies every row is converted to float while staged.
+// Returns kStageFailed if a bulk wait expired (the status word is set and the
+// block must not use the staged rows).
+template <int MODE, int K, int P, int Q, int R, typename T>
+__device__ __forceinline__ int stage_params(int64_t n, int64_t row0, const float* pws,
+                                            const float* rots, const float* scales,
+                                            const float* alphas, const T* w0, const T* wa,
+                                            const T* wb, float* sm, float* raw, uint64_t* bar) {
   using WS = WRows<MODE, K, P, Q, R>;
   const Staged<MODE, K, P, Q, R> S(sm);
   const int nt = blockDim.x;
   const bool full = row0 + nt <= n;
-  bool bulk = full && sizeof(T) == 4 && aligned16(pws + row0 * 3) && aligned16(rots + row0 * 4) &&
+  bool bulk = full && aligned16(pws + row0 * 3) && aligned16(rots + row0 * 4) &&
               aligned16(scales + row0 * 3) && aligned16(alphas + row0) &&
-              aligned16(w0 + row0 * WS::W0);
+              aligned16(w0 + row0 * WS::W0) && (nt * WS::W0 * sizeof(T)) % 16 == 0;
   if (MODE != GSB_WEIGHTS_FULL)
-    bulk = bulk && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB);
+    bulk = bulk && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB) &&
+           (nt * WS::WA * sizeof(T)) % 16 == 0 && (nt * WS::WB * sizeof(T)) % 16 == 0;
+  const bool raw16 = bulk && sizeof(T) == 2;
   if (bulk && threadIdx.x == 0) {
     mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, (uint32_t)(nt * WS::IN * 4));
+    mbar_arrive_expect_tx(
+        bar, (uint32_t)(nt * 11 * 4 + nt * (WS::W0 + WS::WA + WS::WB) * sizeof(T)));
   }
   stage_rows<3>(pws, row0, n, (float*)S.p, bulk, bar);
   stage_rows<4>(rots, row0, n, (float*)S.q, bulk, bar);
   stage_rows<3>(scales, row0, n, (float*)S.s, bulk, bar);
   stage_rows<1>(alphas, row0, n, (float*)S.al, bulk, bar);
-  stage_rows<WS::W0>(w0, row0, n, (float*)S.w0, bulk, bar);
-  if constexpr (MODE != GSB_WEIGHTS_FULL) {
-    stage_rows<WS::WA>(wa, row0, n, (float*)S.wa, bulk, bar);
-    stage_rows<WS::WB>(wb, row0, n, (float*)S.wb, bulk, bar);
+  if (raw16) {
+    if (threadIdx.x == 0) {
+      if constexpr (MODE == GSB_WEIGHTS_FULL) {
+        bulk_load((void*)S.w0, w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 2), bar);
+      } else {
+        char* r = (char*)raw;
+        bulk_load(r, w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 2), bar);
+        r += nt * WS::W0 * 2;
+        bulk_load(r, wa + row0 * WS::WA, (uint32_t)(nt * WS::WA * 2), bar);
+        r += nt * WS::WA * 2;
+        bulk_load(r, wb + row0 * WS::WB, (uint32_t)(nt * WS::WB * 2), bar);
+      }
+    }
+  } else {
+    stage_rows<WS::W0>(w0, row0, n, (float*)S.w0, bulk, bar);
+    if constexpr (MODE != GSB_WEIGHTS_FULL) {
+      stage_rows<WS::WA>(wa, row0, n, (float*)S.wa, bulk, bar);
+      stage_rows<WS::WB>(wb, row0, n, (float*)S.wb, bulk, bar);
+    }
   }
   __syncthreads();
   if (bulk && !mbar_wait(bar, 0)) {
     if (threadIdx.x == 0) atomicOr(&g_fused_status, kStatusBulkTimeout);
     mbar_wait(bar, 0);  // bounded second wait for copies still in flight
-    return false;
+    return kStageFailed;
   }
-  return true;
+  return raw16 ? kStagedRawBf16 : kStagedFloat;
+}
+
+// Converts `count` raw BF16 values to floats, shared memory to shared memory.
+__device__ __forceinline__ void bf16_rows_to_float(const __nv_bfloat16* src, float* dst,
+                                                   int count) {
+  for (int e = threadIdx.x; e < count; e += blockDim.x) dst[e] = __bfloat162float(src[e]);
 }
 
 // Full-SH rows are 16K floats long, a multiple of 16: read one row per
@@ -127,16 +170,16 @@ struct PadRows {
   static constexpr int kExtra = kPad ? W + 1 : 0;  // extra floats per thread
 };
 
-template <int W>
-__device__ __forceinline__ const float* pad_rows(const float* rows, float* pad, bool copy) {
+template <int W, typename S>
+__device__ __forceinline__ const float* pad_rows(const S* rows, float* pad, bool copy) {
   if constexpr (!PadRows<W>::kPad) {
-    return rows;
+    return (const float*)rows;
   } else {
     const int nt = blockDim.x;
     if (copy)
       for (int e = threadIdx.x; e < nt * W; e += nt) {
         const int r = e / W, c = e - r * W;
-        pad[r * (W + 1) + c] = rows[e];
+        pad[r * (W + 1) + c] = (float)rows[e];
       }
     __syncthreads();
     return pad;
@@ -183,10 +226,25 @@ __global__ void __launch_bounds__(kFuseThreads)
   }
   const int nt = blockDim.x, t = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
-  const bool staged = stage_params<MODE, K, P, Q, R, T>(n, row0, pws, rots, scales, alphas, w0,
-                                                        wa, wb, sm, &bar);
+  using FX = FwdExtra<MODE, K, P, Q, R, T>;
+  float* raw = sm + nt * (WS::IN + PadRows<WS::W0>::kExtra);
+  const int how = stage_params<MODE, K, P, Q, R, T>(n, row0, pws, rots, scales, alphas, w0, wa,
+                                                    wb, sm, raw, &bar);
+  const bool staged = how != kStageFailed;
   const Staged<MODE, K, P, Q, R> S(sm);
-  const float* w0rows = pad_rows<WS::W0>(S.w0, sm + nt * WS::IN, staged);
+  if constexpr (FX::kRawLowrank) {  // raw BF16 factors -> their float rows
+    if (how == kStagedRawBf16) {
+      const __nv_bfloat16* r = (const __nv_bfloat16*)raw;
+      bf16_rows_to_float(r, (float*)S.w0, nt * WS::W0);
+      bf16_rows_to_float(r + nt * WS::W0, (float*)S.wa, nt * WS::WA);
+      bf16_rows_to_float(r + nt * (WS::W0 + WS::WA), (float*)S.wb, nt * WS::WB);
+    }
+    __syncthreads();
+  }
+  const float* w0rows =
+      (sizeof(T) == 2 && MODE == GSB_WEIGHTS_FULL && how == kStagedRawBf16)
+          ? pad_rows<WS::W0>((const __nv_bfloat16*)S.w0, sm + nt * WS::IN, true)
+          : pad_rows<WS::W0>(S.w0, sm + nt * WS::IN, staged);
   const int64_t i = row0 + t;
   uint32_t cnt = 0, dk = 0;
   float f[4 * V];  // this Gaussian's record (kept until the block writes its records)
@@ -300,23 +358,37 @@ struct BwdPlan {
   static constexpr int floats = in_floats + out_floats;
 };
 
+// Raw BF16 rows of the backward's staged colour parameters (bulk-copied,
+// then converted into their float areas), in floats per thread.
+template <int MODE, int K, int P, int Q, int R, bool GEOM, typename T>
+struct BwdRaw {
+  using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
+  static constexpr int kHalfs = sizeof(T) == 2 ? BP::W0_ + BP::A_ + BP::B_ : 0;
+  static constexpr int kFloats = (kHalfs + 1) / 2;
+};
+
 template <int MODE, int K, int P, int Q, int R, bool GEOM, typename T>
 __device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const float* pws,
                                                const float* rots, const float* scales,
                                                const T* w0, const T* wa, const T* wb,
-                                               const float* g_feat, float* sm, uint64_t* bar) {
+                                               const float* g_feat, float* sm, float* raw,
+                                               uint64_t* bar) {
   using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
   using WS = WRows<MODE, K, P, Q, R>;
   const int nt = blockDim.x;
   const bool full = row0 + nt <= n;
   bool bulk = full && aligned16(pws + row0 * 3) && aligned16(g_feat + row0 * K);
   if (GEOM) bulk = bulk && aligned16(rots + row0 * 4) && aligned16(scales + row0 * 3);
-  if (BP::kW0) bulk = bulk && sizeof(T) == 4 && aligned16(w0 + row0 * WS::W0);
+  if (BP::kW0)
+    bulk = bulk && aligned16(w0 + row0 * WS::W0) && (nt * WS::W0 * sizeof(T)) % 16 == 0;
   if (BP::kAB)
-    bulk = bulk && sizeof(T) == 4 && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB);
+    bulk = bulk && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB) &&
+           (nt * WS::WA * sizeof(T)) % 16 == 0 && (nt * WS::WB * sizeof(T)) % 16 == 0;
+  const bool raw16 = bulk && sizeof(T) == 2;
   if (bulk && threadIdx.x == 0) {
     mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, (uint32_t)(nt * BP::in_floats * 4));
+    mbar_arrive_expect_tx(bar, (uint32_t)(nt * (BP::P_ + BP::G_ + BP::Q_ + BP::S_) * 4 +
+                                          nt * (BP::W0_ + BP::A_ + BP::B_) * sizeof(T)));
   }
   stage_rows<3>(pws, row0, n, sm + nt * BP::o_p, bulk, bar);
   stage_rows<K>(g_feat, row0, n, sm + nt * BP::o_g, bulk, bar);
@@ -324,16 +396,45 @@ __device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const fl
     stage_rows<4>(rots, row0, n, sm + nt * BP::o_q, bulk, bar);
     stage_rows<3>(scales, row0, n, sm + nt * BP::o_s, bulk, bar);
   }
-  if constexpr (BP::kW0) stage_rows<WS::W0>(w0, row0, n, sm + nt * BP::o_w0, bulk, bar);
-  if constexpr (BP::kAB) {
-    stage_rows<WS::WA>(wa, row0, n, sm + nt * BP::o_a, bulk, bar);
-    stage_rows<WS::WB>(wb, row0, n, sm + nt * BP::o_b, bulk, bar);
+  if (raw16) {
+    if (threadIdx.x == 0) {
+      char* r = (char*)raw;
+      if constexpr (BP::kW0) {
+        bulk_load(r, w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 2), bar);
+        r += nt * WS::W0 * 2;
+      }
+      if constexpr (BP::kAB) {
+        bulk_load(r, wa + row0 * WS::WA, (uint32_t)(nt * WS::WA * 2), bar);
+        r += nt * WS::WA * 2;
+        bulk_load(r, wb + row0 * WS::WB, (uint32_t)(nt * WS::WB * 2), bar);
+      }
+    }
+  } else {
+    if constexpr (BP::kW0) stage_rows<WS::W0>(w0, row0, n, sm + nt * BP::o_w0, bulk, bar);
+    if constexpr (BP::kAB) {
+      stage_rows<WS::WA>(wa, row0, n, sm + nt * BP::o_a, bulk, bar);
+      stage_rows<WS::WB>(wb, row0, n, sm + nt * BP::o_b, bulk, bar);
+    }
   }
   __syncthreads();
   if (bulk && !mbar_wait(bar, 0)) {
     if (threadIdx.x == 0) atomicOr(&g_fused_status, kStatusBulkTimeout);
     mbar_wait(bar, 0);  // bounded second wait for copies still in flight
     return false;
+  }
+  if constexpr (sizeof(T) == 2) {  // raw BF16 rows -> their float areas
+    if (raw16) {
+      const __nv_bfloat16* r = (const __nv_bfloat16*)raw;
+      if constexpr (BP::kW0) {
+        bf16_rows_to_float(r, sm + nt * BP::o_w0, nt * WS::W0);
+        r += nt * WS::W0;
+      }
+      if constexpr (BP::kAB) {
+        bf16_rows_to_float(r, sm + nt * BP::o_a, nt * WS::WA);
+        bf16_rows_to_float(r + nt * WS::WA, sm + nt * BP::o_b, nt * WS::WB);
+      }
+    }
+    __syncthreads();
   }
   return true;
 }
@@ -372,8 +473,9 @@ __global__ void __launch_bounds__(kFuseThreads)
   __shared__ __align__(8) uint64_t bar;
   const int nt = blockDim.x, t = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
+  float* raw = sm + nt * (BP::floats + PadRows<WS::W0>::kExtra);
   if (!stage_backward<MODE, K, P, Q, R, GEOM, T>(n, row0, pws, rots, scales, w0, wa, wb, g_feat, sm,
-                                                 &bar))
+                                                 raw, &bar))
     return;
   const int64_t i = row0 + t;
   // full-SH gradient rows are built at an odd stride past the plan's regions
@@ -560,7 +662,9 @@ static int set_smem(Kern kern, int smem) {
 template <int MODE, int K, int P, int Q, int R, typename T>
 static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   using WS = WRows<MODE, K, P, Q, R>;
-  const int smem = (WS::IN + PadRows<WS::W0>::kExtra) * kFuseThreads * 4;
+  const int smem =
+      (WS::IN + PadRows<WS::W0>::kExtra + FwdExtra<MODE, K, P, Q, R, T>::kRawFloats) *
+      kFuseThreads * 4;
   const int grid = div_up(f.n, kFuseThreads);
   int rc;
   if (!backward) {
@@ -576,8 +680,10 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   const bool geom = f.g_u != nullptr;
   auto kern = geom ? k_render_backward_pre<MODE, K, P, Q, R, T, true>
                    : k_render_backward_pre<MODE, K, P, Q, R, T, false>;
-  const int bsmem = ((geom ? BwdPlan<MODE, K, P, Q, R, true>::floats
-                           : BwdPlan<MODE, K, P, Q, R, false>::floats) +
+  const int bsmem = ((geom ? BwdPlan<MODE, K, P, Q, R, true>::floats +
+                                 BwdRaw<MODE, K, P, Q, R, true, T>::kFloats
+                           : BwdPlan<MODE, K, P, Q, R, false>::floats +
+                                 BwdRaw<MODE, K, P, Q, R, false, T>::kFloats) +
                      PadRows<WS::W0>::kExtra) *
                     kFuseThreads * 4;
   if ((rc = set_smem(kern, bsmem))) return rc;
