@@ -37,6 +37,11 @@ struct WRows {
   static constexpr int WB = MODE == GSB_WEIGHTS_FULL ? 0 : R * Q;
   static constexpr int L = MODE == GSB_WEIGHTS_FULL ? 15 : P * Q / K;
   static constexpr int IN = 3 + 4 + 3 + 1 + W0 + WA + WB;  // staged floats per Gaussian
+  // The forward stages full-SH rows (16K floats, a multiple of 16) at a stride
+  // of an odd number of float4s, so that one thread per row reading float4s
+  // touches distinct shared-memory banks; other rows stay contiguous.
+  static constexpr int W0S = MODE == GSB_WEIGHTS_FULL ? 4 * ((W0 / 4) | 1) : W0;
+  static constexpr int INS = 3 + 4 + 3 + 1 + W0S + WA + WB;  // forward staged floats
 };
 
 // Camera: rotation, translation and centre stay in device memory (so a
@@ -71,21 +76,18 @@ struct Staged {
     s = q + nt * 4;
     al = s + nt * 3;
     w0 = al + nt;
-    wa = w0 + nt * WS::W0;
+    wa = w0 + nt * WS::W0S;
     wb = wa + nt * WS::WA;
   }
 };
 
 // Extra shared memory of the forward, in floats per thread, past the staged
-// rows: the odd-stride copy of even-length rows (PadRows), then, for BF16
-// low-rank factors, their raw bulk-copied rows (full-SH BF16 rows land raw in
-// the float row area itself and are converted straight into the odd-stride
-// copy).
+// rows: the raw bulk-copied BF16 colour rows, converted into the float rows.
 template <int MODE, int K, int P, int Q, int R, typename T>
 struct FwdExtra {
   using WS = WRows<MODE, K, P, Q, R>;
   static constexpr bool kRawLowrank = sizeof(T) == 2 && MODE != GSB_WEIGHTS_FULL;
-  static constexpr int kRawFloats = kRawLowrank ? (WS::W0 + WS::WA + WS::WB + 1) / 2 : 0;
+  static constexpr int kRawFloats = sizeof(T) == 2 ? (WS::W0 + WS::WA + WS::WB + 1) / 2 : 0;
 };
 
 // How the block's colour-parameter rows ended up in shared memory.
@@ -120,29 +122,41 @@ __device__ __forceinline__ int stage_params(int64_t n, int64_t row0, const float
     mbar_arrive_expect_tx(
         bar, (uint32_t)(nt * 11 * 4 + nt * (WS::W0 + WS::WA + WS::WB) * sizeof(T)));
   }
+  if constexpr (MODE == GSB_WEIGHTS_FULL && sizeof(T) == 4) {
+    if (bulk) __syncthreads();  // the barrier is initialised before any thread's copy
+  }
   stage_rows<3>(pws, row0, n, (float*)S.p, bulk, bar);
   stage_rows<4>(rots, row0, n, (float*)S.q, bulk, bar);
   stage_rows<3>(scales, row0, n, (float*)S.s, bulk, bar);
   stage_rows<1>(alphas, row0, n, (float*)S.al, bulk, bar);
   if (raw16) {
     if (threadIdx.x == 0) {
-      if constexpr (MODE == GSB_WEIGHTS_FULL) {
-        bulk_load((void*)S.w0, w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 2), bar);
-      } else {
-        char* r = (char*)raw;
-        bulk_load(r, w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 2), bar);
+      char* r = (char*)raw;
+      bulk_load(r, w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 2), bar);
+      if constexpr (MODE != GSB_WEIGHTS_FULL) {
         r += nt * WS::W0 * 2;
         bulk_load(r, wa + row0 * WS::WA, (uint32_t)(nt * WS::WA * 2), bar);
         r += nt * WS::WA * 2;
         bulk_load(r, wb + row0 * WS::WB, (uint32_t)(nt * WS::WB * 2), bar);
       }
     }
+  } else if constexpr (MODE == GSB_WEIGHTS_FULL) {
+    // one copy per row, into the odd-float4 stride
+    float* dst = (float*)S.w0;
+    if (bulk) {
+      bulk_load(dst + threadIdx.x * WS::W0S, w0 + (row0 + threadIdx.x) * WS::W0,
+                (uint32_t)(WS::W0 * sizeof(T)), bar);
+    } else {
+      const int64_t rows = min((int64_t)nt, n - row0);
+      for (int e = threadIdx.x; e < rows * WS::W0; e += nt) {
+        const int r = e / WS::W0, c = e - r * WS::W0;
+        dst[r * WS::W0S + c] = ld(w0, row0 * WS::W0 + e);
+      }
+    }
   } else {
     stage_rows<WS::W0>(w0, row0, n, (float*)S.w0, bulk, bar);
-    if constexpr (MODE != GSB_WEIGHTS_FULL) {
-      stage_rows<WS::WA>(wa, row0, n, (float*)S.wa, bulk, bar);
-      stage_rows<WS::WB>(wb, row0, n, (float*)S.wb, bulk, bar);
-    }
+    stage_rows<WS::WA>(wa, row0, n, (float*)S.wa, bulk, bar);
+    stage_rows<WS::WB>(wb, row0, n, (float*)S.wb, bulk, bar);
   }
   __syncthreads();
   if (bulk && !mbar_wait(bar, 0)) {
@@ -159,32 +173,16 @@ __device__ __forceinline__ void bf16_rows_to_float(const __nv_bfloat16* src, flo
   for (int e = threadIdx.x; e < count; e += blockDim.x) dst[e] = __bfloat162float(src[e]);
 }
 
-// Full-SH rows are 16K floats long, a multiple of 16: read one row per
+// Full-SH rows are 16K floats long, a multiple of 16: written one row per
 // thread, the 32 lanes of a warp would hit 2 (or 1) of the 32 shared-memory
-// banks.  Rows of even length are therefore copied once to an odd stride
-// before the per-thread reads (the accumulation order is unchanged).
+// banks.  The adjoint therefore builds its SH-gradient rows at an odd stride
+// and packs them before storing them.
 template <int W>
 struct PadRows {
   static constexpr bool kPad = W > 1 && W % 2 == 0;
   static constexpr int kStride = kPad ? W + 1 : W;
   static constexpr int kExtra = kPad ? W + 1 : 0;  // extra floats per thread
 };
-
-template <int W, typename S>
-__device__ __forceinline__ const float* pad_rows(const S* rows, float* pad, bool copy) {
-  if constexpr (!PadRows<W>::kPad) {
-    return (const float*)rows;
-  } else {
-    const int nt = blockDim.x;
-    if (copy)
-      for (int e = threadIdx.x; e < nt * W; e += nt) {
-        const int r = e / W, c = e - r * W;
-        pad[r * (W + 1) + c] = (float)rows[e];
-      }
-    __syncthreads();
-    return pad;
-  }
-}
 
 // Palette weights of one Gaussian from its staged parameter rows.
 template <int MODE, int K, int P, int Q, int R>
@@ -216,7 +214,7 @@ __global__ void __launch_bounds__(kFuseThreads)
   pdl_wait();
   using WS = WRows<MODE, K, P, Q, R>;
   constexpr int V = RecordLayout<COL ? 3 : K>::kVec4;
-  static_assert(WS::IN >= 4 * V, "the record span reuses the input staging area");
+  static_assert(WS::INS >= 4 * V, "the record span reuses the input staging area");
   extern __shared__ __align__(16) float sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t warp_tot[kFuseThreads / 32];
@@ -226,25 +224,35 @@ __global__ void __launch_bounds__(kFuseThreads)
   }
   const int nt = blockDim.x, t = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
-  using FX = FwdExtra<MODE, K, P, Q, R, T>;
-  float* raw = sm + nt * (WS::IN + PadRows<WS::W0>::kExtra);
+  float* raw = sm + nt * WS::INS;
   const int how = stage_params<MODE, K, P, Q, R, T>(n, row0, pws, rots, scales, alphas, w0, wa,
                                                     wb, sm, raw, &bar);
   const bool staged = how != kStageFailed;
   const Staged<MODE, K, P, Q, R> S(sm);
-  if constexpr (FX::kRawLowrank) {  // raw BF16 factors -> their float rows
+  if constexpr (sizeof(T) == 2) {  // raw BF16 colour rows -> their float rows
     if (how == kStagedRawBf16) {
       const __nv_bfloat16* r = (const __nv_bfloat16*)raw;
-      bf16_rows_to_float(r, (float*)S.w0, nt * WS::W0);
-      bf16_rows_to_float(r + nt * WS::W0, (float*)S.wa, nt * WS::WA);
-      bf16_rows_to_float(r + nt * (WS::W0 + WS::WA), (float*)S.wb, nt * WS::WB);
+      if constexpr (MODE == GSB_WEIGHTS_FULL) {
+        // 8 values (16 bytes) at a time into the odd-float4 stride
+        constexpr int C8 = WS::W0 / 8;
+        for (int e = t; e < nt * C8; e += nt) {
+          const int rr = e / C8, c = e - rr * C8;
+          const uint4 v = reinterpret_cast<const uint4*>(r)[e];
+          const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+          const float2 a = __bfloat1622float2(h[0]), b = __bfloat1622float2(h[1]);
+          const float2 c2 = __bfloat1622float2(h[2]), d = __bfloat1622float2(h[3]);
+          float4* dst = reinterpret_cast<float4*>((float*)S.w0 + rr * WS::W0S + 8 * c);
+          dst[0] = make_float4(a.x, a.y, b.x, b.y);
+          dst[1] = make_float4(c2.x, c2.y, d.x, d.y);
+        }
+      } else {
+        bf16_rows_to_float(r, (float*)S.w0, nt * WS::W0);
+        bf16_rows_to_float(r + nt * WS::W0, (float*)S.wa, nt * WS::WA);
+        bf16_rows_to_float(r + nt * (WS::W0 + WS::WA), (float*)S.wb, nt * WS::WB);
+      }
     }
     __syncthreads();
   }
-  const float* w0rows =
-      (sizeof(T) == 2 && MODE == GSB_WEIGHTS_FULL && how == kStagedRawBf16)
-          ? pad_rows<WS::W0>((const __nv_bfloat16*)S.w0, sm + nt * WS::IN, true)
-          : pad_rows<WS::W0>(S.w0, sm + nt * WS::IN, staged);
   const int64_t i = row0 + t;
   uint32_t cnt = 0, dk = 0;
   float f[4 * V];  // this Gaussian's record (kept until the block writes its records)
@@ -272,8 +280,23 @@ __global__ void __launch_bounds__(kFuseThreads)
           float dir[3], Y[16], w[K];
           view_direction(pw, make_float3(cr.c[0], cr.c[1], cr.c[2]), dir, nullptr, nullptr);
           sh_basis(dir, WS::L + 1, Y);
-          weights_of<MODE, K, P, Q, R>(w0rows + t * PadRows<WS::W0>::kStride, S.wa + t * WS::WA,
-                                       S.wb + t * WS::WB, Y, w);
+          if constexpr (MODE == GSB_WEIGHTS_FULL) {
+            // the row as float4s (conflict-free at the odd-float4 stride)
+            float row[WS::W0];
+            const float4* src = reinterpret_cast<const float4*>(S.w0 + t * WS::W0S);
+#pragma unroll
+            for (int c = 0; c < WS::W0 / 4; ++c) {
+              const float4 v = src[c];
+              row[4 * c] = v.x;
+              row[4 * c + 1] = v.y;
+              row[4 * c + 2] = v.z;
+              row[4 * c + 3] = v.w;
+            }
+            sh_weights_full<K>([&](int idx) { return row[idx]; }, 16, Y, w);
+          } else {
+            weights_of<MODE, K, P, Q, R>(S.w0 + t * WS::W0, S.wa + t * WS::WA, S.wb + t * WS::WB,
+                                         Y, w);
+          }
           record_head(p.ux, p.uy, conic[0], conic[1], conic[2], S.al[t], f);
           if constexpr (COL) {
 #pragma unroll
@@ -662,9 +685,7 @@ static int set_smem(Kern kern, int smem) {
 template <int MODE, int K, int P, int Q, int R, typename T>
 static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   using WS = WRows<MODE, K, P, Q, R>;
-  const int smem =
-      (WS::IN + PadRows<WS::W0>::kExtra + FwdExtra<MODE, K, P, Q, R, T>::kRawFloats) *
-      kFuseThreads * 4;
+  const int smem = (WS::INS + FwdExtra<MODE, K, P, Q, R, T>::kRawFloats) * kFuseThreads * 4;
   const int grid = div_up(f.n, kFuseThreads);
   int rc;
   if (!backward) {
