@@ -245,13 +245,10 @@ __global__ void __launch_bounds__(kFuseThreads)
           dst[0] = make_float4(a.x, a.y, b.x, b.y);
           dst[1] = make_float4(c2.x, c2.y, d.x, d.y);
         }
-      } else {
-        bf16_rows_to_float(r, (float*)S.w0, nt * WS::W0);
-        bf16_rows_to_float(r + nt * WS::W0, (float*)S.wa, nt * WS::WA);
-        bf16_rows_to_float(r + nt * (WS::W0 + WS::WA), (float*)S.wb, nt * WS::WB);
       }
+      // (low-rank BF16 factors are read raw: their row strides are odd)
     }
-    __syncthreads();
+    if constexpr (MODE == GSB_WEIGHTS_FULL) __syncthreads();
   }
   const int64_t i = row0 + t;
   uint32_t cnt = 0, dk = 0;
@@ -293,6 +290,10 @@ __global__ void __launch_bounds__(kFuseThreads)
               row[4 * c + 3] = v.w;
             }
             sh_weights_full<K>([&](int idx) { return row[idx]; }, 16, Y, w);
+          } else if (sizeof(T) == 2 && how == kStagedRawBf16) {
+            const __nv_bfloat16* r = (const __nv_bfloat16*)raw;
+            lowrank_weights<K, P, Q, R>(r + t * WS::W0, r + nt * WS::W0 + t * WS::WA,
+                                        r + nt * (WS::W0 + WS::WA) + t * WS::WB, Y, w);
           } else {
             weights_of<MODE, K, P, Q, R>(S.w0 + t * WS::W0, S.wa + t * WS::WA, S.wb + t * WS::WB,
                                          Y, w);

@@ -300,12 +300,17 @@ __device__ __forceinline__ void sh_weights_full(Loader load, int nb, const float
 // w_k = C0 dc_k + sum_l C[g/Q][g%Q] Y_{l+1}, g = l*K + k, C = A B with
 // a = A [P,R] and b = B [R,Q] row-major.  Summation order fixed: each
 // coefficient over r, then over l, then added to the DC term.
-template <int K, int P, int Q, int R>
-__device__ __forceinline__ void lowrank_weights(const float* dc, const float* a, const float* b,
+// The factors may be FP32 or BF16 (shared memory or registers); the
+// arithmetic is FP32 either way.
+__device__ __forceinline__ float as_f32(float v) { return v; }
+__device__ __forceinline__ float as_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <int K, int P, int Q, int R, typename S>
+__device__ __forceinline__ void lowrank_weights(const S* dc, const S* a, const S* b,
                                                 const float* Y, float* wk) {
   constexpr int L = P * Q / K;
 #pragma unroll
-  for (int k = 0; k < K; ++k) wk[k] = SH_C0 * dc[k];
+  for (int k = 0; k < K; ++k) wk[k] = SH_C0 * as_f32(dc[k]);
   if (L > 0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -313,9 +318,9 @@ __device__ __forceinline__ void lowrank_weights(const float* dc, const float* a,
 #pragma unroll
       for (int l = 0; l < L; ++l) {
         const int g = l * K + k, row = g / Q, col = g % Q;
-        float coef = a[row * R] * b[col];
+        float coef = as_f32(a[row * R]) * as_f32(b[col]);
 #pragma unroll
-        for (int r = 1; r < R; ++r) coef += a[row * R + r] * b[r * Q + col];
+        for (int r = 1; r < R; ++r) coef += as_f32(a[row * R + r]) * as_f32(b[r * Q + col]);
         acc += coef * Y[l + 1];
       }
       wk[k] += acc;
