@@ -654,7 +654,11 @@ def run_b200(a):
                                    views_per_s=round(world * VIEWS * 1000.0 / mv_ms, 2)),
                     serving=serving,
                     stages_ms={k: round(v, 4) for k, v in stages.items()},
-                    patches=alg["M"])
+                    patches=alg["M"],
+                    # sort throughput and the compositing's nominal pixel work
+                    # (every patch against the 256 pixels of its tile)
+                    sort_keys_per_s=round(alg["M"] / (stages["bin_sort"] / 1000.0), 1),
+                    draw_evaluations_per_s=round(alg["M"] * 256 / (stages["draw"] / 1000.0), 1))
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
