@@ -143,19 +143,21 @@ def make_views(wl, a, device):
 
 def step_views(wl, mv, backward=True):
     """One step of the multi-view finetune workload: VIEWS views rendered
-    through the fused path from BF16 rank-3 factors (FP32 arithmetic), each
-    with 0.8 L1 + 0.2 (1 - SSIM) of its palette colour image against its
-    target plus 0.5 mean(relu(-weights)) (one fused kernel per view,
+    through the fused path from BF16 rank-3 factors (FP32 arithmetic,
+    palette_b200.render.render_palette_views), each with 0.8 L1 + 0.2 (1 -
+    SSIM) of its palette colour image against its target plus 0.5
+    mean(relu(-weights)) (one fused kernel per view,
     palette_b200.loss.palette_l1_ssim_loss), averaged over the views; the
-    backward gives dc, A, B (BF16) and palette gradients."""
+    backward sums the views' dc, A, B gradients in FP32 and returns them in
+    BF16, with the palette gradient."""
     from palette_b200.loss import palette_l1_ssim_loss
-    from palette_b200.render import render_palette
+    from palette_b200.render import render_palette_views
     for p in (mv["dc"], mv["A"], mv["B"], mv["palette"]):
         p.grad = None
+    layers, _, _ = render_palette_views(wl["pws"], wl["rots"], wl["scales"], wl["alphas"],
+                                        mv["cams"], dc=mv["dc"], A=mv["A"], B=mv["B"])
     total = None
-    for cam, tgt in zip(mv["cams"], mv["targets"]):
-        layer, _, _ = render_palette(wl["pws"], wl["rots"], wl["scales"], wl["alphas"], cam,
-                                     dc=mv["dc"], A=mv["A"], B=mv["B"])
+    for layer, tgt in zip(layers, mv["targets"]):
         loss = palette_l1_ssim_loss(layer, mv["palette"], tgt, lambda_ssim=0.2, lambda_pos=0.5)
         total = loss if total is None else total + loss
     total = total / len(mv["cams"])

@@ -360,6 +360,23 @@ int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* pws, cons
                         void* scratch, float* dpws, float* drots, float* dscales, float* dalphas,
                         float* dw0, float* dA, float* dB, void* stream);
 
+/* gsb_render_backward for several views of one scene: the same arguments and
+ * gradients, but ADDED to what dw0, dA, dB (and, when given, dpws, drots,
+ * dscales, dalphas) already hold instead of overwriting them.  A training
+ * step over a batch of views calls gsb_render_backward for its first view and
+ * this entry for the others, so the views' gradients are summed in FP32 in the
+ * output buffers, whatever the storage dtype of the parameters.  The reference
+ * has no counterpart: its backward handles one view per call, and a batch of
+ * views is summed by torch autograd in the parameters' dtype. */
+int gsb_render_backward_accumulate(int64_t n, const gsb_camera* cam, const float* pws,
+                                   const float* rots, const float* scales, const float* alphas,
+                                   const gsb_palette_params* params, const void* state,
+                                   const int32_t* ranges, const int32_t* gsid,
+                                   const int32_t* contrib, const float* final_tau,
+                                   const float* dloss_dout, const float* dloss_dtau,
+                                   void* scratch, float* dpws, float* drots, float* dscales,
+                                   float* dalphas, float* dw0, float* dA, float* dB, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

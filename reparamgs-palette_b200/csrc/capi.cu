@@ -475,14 +475,14 @@ GSB_API size_t gsb_render_backward_bytes(int64_t n, int K) {
   return (size_t)n * (K + 5) * sizeof(float) + 256;
 }
 
-GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* pws,
-                                const float* rots, const float* scales, const float* alphas,
-                                const gsb_palette_params* params, const void* state,
-                                const int32_t* ranges, const int32_t* gsid,
-                                const int32_t* contrib, const float* final_tau,
-                                const float* dloss_dout, const float* dloss_dtau, void* scratch,
-                                float* dpws, float* drots, float* dscales, float* dalphas,
-                                float* dw0, float* dA, float* dB, void* stream) {
+static int render_backward(int64_t n, const gsb_camera* cam, const float* pws, const float* rots,
+                           const float* scales, const float* alphas,
+                           const gsb_palette_params* params, const void* state,
+                           const int32_t* ranges, const int32_t* gsid, const int32_t* contrib,
+                           const float* final_tau, const float* dloss_dout,
+                           const float* dloss_dtau, void* scratch, float* dpws, float* drots,
+                           float* dscales, float* dalphas, float* dw0, float* dA, float* dB,
+                           bool acc, void* stream) {
   GSB_CHECK_ARG(cam && cam->Rcw && cam->tcw && cam->twc, "render_backward: null camera");
   int rc = check_image("render_backward", n, cam->height, cam->width, params ? params->K : 1);
   if (rc) return rc;
@@ -502,8 +502,10 @@ GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* p
   float* g_feat = (float*)scratch;
   float* g_u = g_feat + (size_t)n * K;
   float* g_conic = g_u + (size_t)n * 2;
-  if (n > 0 && (rc = launch_zero2(scratch, n * (geom ? K + 5 : K), geom ? dalphas : nullptr,
-                                  geom ? n : 0, ST(stream))))
+  // (accumulating: dalphas keeps the previous views' sum; the adjoint adds to it)
+  if (n > 0 && (rc = launch_zero2(scratch, n * (geom ? K + 5 : K),
+                                  geom && !acc ? dalphas : nullptr, geom && !acc ? n : 0,
+                                  ST(stream))))
     return rc;
   rc = launch_draw_backward(n, cam->height, cam->width, K, ranges, gsid, s, contrib, final_tau,
                             dloss_dout, geom ? dloss_dtau : nullptr, g_feat,
@@ -529,6 +531,31 @@ GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* p
   f.d_w0 = dw0;
   f.d_wa = dA;
   f.d_wb = dB;
+  f.accumulate = acc;
   return launch_render(params->mode, params->dtype, K, params->P, params->Q, params->rank, f, true,
                        ST(stream));
+}
+
+GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* pws,
+                                const float* rots, const float* scales, const float* alphas,
+                                const gsb_palette_params* params, const void* state,
+                                const int32_t* ranges, const int32_t* gsid,
+                                const int32_t* contrib, const float* final_tau,
+                                const float* dloss_dout, const float* dloss_dtau, void* scratch,
+                                float* dpws, float* drots, float* dscales, float* dalphas,
+                                float* dw0, float* dA, float* dB, void* stream) {
+  return render_backward(n, cam, pws, rots, scales, alphas, params, state, ranges, gsid, contrib,
+                         final_tau, dloss_dout, dloss_dtau, scratch, dpws, drots, dscales, dalphas,
+                         dw0, dA, dB, false, stream);
+}
+
+GSB_API int gsb_render_backward_accumulate(
+    int64_t n, const gsb_camera* cam, const float* pws, const float* rots, const float* scales,
+    const float* alphas, const gsb_palette_params* params, const void* state,
+    const int32_t* ranges, const int32_t* gsid, const int32_t* contrib, const float* final_tau,
+    const float* dloss_dout, const float* dloss_dtau, void* scratch, float* dpws, float* drots,
+    float* dscales, float* dalphas, float* dw0, float* dA, float* dB, void* stream) {
+  return render_backward(n, cam, pws, rots, scales, alphas, params, state, ranges, gsid, contrib,
+                         final_tau, dloss_dout, dloss_dtau, scratch, dpws, drots, dscales, dalphas,
+                         dw0, dA, dB, true, stream);
 }

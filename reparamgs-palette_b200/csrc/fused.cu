@@ -475,6 +475,35 @@ __device__ __forceinline__ void write_rows(float* g, int64_t row0, int64_t n, co
   }
 }
 
+// Adds one gradient array's block span (`rows` rows) from shared memory to
+// global memory, coalesced, with kAddBatch loads in flight per thread before
+// the adds and stores (one read-add-write at a time would pay a global-memory
+// latency per element).  Element e of the span comes from s[src(e)].
+constexpr int kAddBatch = 8;
+template <int ROWLEN, typename Src>
+__device__ __forceinline__ void add_span(float* g, int64_t row0, int64_t rows, Src src) {
+  const int total = (int)rows * ROWLEN, nt = blockDim.x;
+  float* base = g + row0 * ROWLEN;
+  for (int j0 = threadIdx.x; j0 < total; j0 += nt * kAddBatch) {
+    float v[kAddBatch];
+#pragma unroll
+    for (int u = 0; u < kAddBatch; ++u) {
+      const int j = j0 + u * nt;
+      v[u] = j < total ? base[j] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kAddBatch; ++u) {
+      const int j = j0 + u * nt;
+      if (j < total) base[j] = v[u] + src(j);
+    }
+  }
+}
+
+template <int ROWLEN>
+__device__ __forceinline__ void add_rows(float* g, int64_t row0, int64_t rows, const float* s) {
+  add_span<ROWLEN>(g, row0, rows, [s](int j) { return s[j]; });
+}
+
 // g_feat [n,K] (dL/dweights), g_u [n,2], g_conic [n,3] come from the
 // compositing adjoint, which also writes dL/dalpha directly.  Without GEOM
 // (weights-only backward: g_u, g_conic and the geometry outputs unused) only
@@ -488,7 +517,7 @@ __global__ void __launch_bounds__(kFuseThreads)
                           const float* __restrict__ g_u, const float* __restrict__ g_conic,
                           float* __restrict__ d_pws, float* __restrict__ d_rots,
                           float* __restrict__ d_scales, float* __restrict__ d_w0,
-                          float* __restrict__ d_wa, float* __restrict__ d_wb) {
+                          float* __restrict__ d_wa, float* __restrict__ d_wb, bool acc) {
   pdl_wait();
   using WS = WRows<MODE, K, P, Q, R>;
   using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
@@ -647,14 +676,33 @@ __global__ void __launch_bounds__(kFuseThreads)
 #pragma unroll
       for (int j = 0; j < 3; ++j) dpw[j] += dd[0] * Jd[j] + dd[1] * Jd[3 + j] + dd[2] * Jd[6 + j];
 #pragma unroll
-      for (int j = 0; j < 3; ++j) d_pws[3 * i + j] = dpw[j];
+      for (int j = 0; j < 3; ++j) d_pws[3 * i + j] = (acc ? d_pws[3 * i + j] : 0.f) + dpw[j];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) d_rots[4 * i + j] = dq[j];
+      for (int j = 0; j < 4; ++j) d_rots[4 * i + j] = (acc ? d_rots[4 * i + j] : 0.f) + dq[j];
 #pragma unroll
-      for (int j = 0; j < 3; ++j) d_scales[3 * i + j] = ds[j];
+      for (int j = 0; j < 3; ++j) d_scales[3 * i + j] = (acc ? d_scales[3 * i + j] : 0.f) + ds[j];
     }
   }
-  // parameter gradients: shared memory -> global, block span by block span
+  // parameter gradients: shared memory -> global, block span by block span;
+  // with `acc`, added to what the outputs hold (coalesced read-add-write)
+  if (acc) {
+    __syncthreads();
+    const int64_t rows = min((int64_t)nt, n - row0);
+    if constexpr (PR::kPad) {
+      const float* src = sm + nt * BP::floats;
+      add_span<WS::W0>(d_w0, row0, rows, [src](int j) {
+        const int r = j / WS::W0, c = j - r * WS::W0;
+        return src[r * PR::kStride + c];
+      });
+    } else {
+      add_rows<WS::W0>(d_w0, row0, rows, sm + nt * BP::o_dw0);
+    }
+    if constexpr (MODE != GSB_WEIGHTS_FULL) {
+      add_rows<WS::WA>(d_wa, row0, rows, sm + nt * BP::o_dwa);
+      add_rows<WS::WB>(d_wb, row0, rows, sm + nt * BP::o_dwb);
+    }
+    return;
+  }
   if constexpr (PR::kPad) {
     __syncthreads();
     float* dst = sm + nt * BP::o_dw0;
@@ -711,7 +759,7 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
   if ((rc = set_smem(kern, bsmem))) return rc;
   launch_pdl(kern, dim3(grid), dim3(kFuseThreads), bsmem, st, f.n, f.cam, f.pws, f.rots,
              f.scales, (const T*)f.w0, (const T*)f.wa, (const T*)f.wb, f.g_feat, f.g_u, f.g_conic,
-             f.d_pws, f.d_rots, f.d_scales, f.d_w0, f.d_wa, f.d_wb);
+             f.d_pws, f.d_rots, f.d_scales, f.d_w0, f.d_wa, f.d_wb, f.accumulate);
   return check_launch("render_backward");
 }
 

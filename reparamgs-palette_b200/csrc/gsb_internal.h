@@ -118,6 +118,7 @@ struct FusedArgs {
   const float* palette;      // forward, may be null: [K,3] -> colour records
   const float *g_feat, *g_u, *g_conic;  // backward: screen-space gradients (g_u null: weights only)
   float *d_pws, *d_rots, *d_scales, *d_w0, *d_wa, *d_wb;
+  bool accumulate;  // backward: add to the d_* outputs instead of overwriting them
 };
 int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedArgs& f, bool backward,
                   cudaStream_t st);

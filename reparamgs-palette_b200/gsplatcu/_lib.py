@@ -72,6 +72,8 @@ _SIGS = {
     "gsb_render_backward_bytes": (_sz, [_i64, _i32]),
     "gsb_render_backward": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
                                    _p, _p, _p, _p, _p, _p, _p, _p]),
+    "gsb_render_backward_accumulate": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
+                                              _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
 }
 
 _lib = None

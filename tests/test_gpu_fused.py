@@ -251,3 +251,49 @@ def test_fused_forward_overlapped_count_and_overflow(cuda_ok):
         assert max_abs(layer, ref["layer"]) < IMG_TOL and max_abs(ft, ref["final_tau"]) < IMG_TOL
         assert torch.equal(depths, ref["depths"].reshape(-1))
     assert gsc._CAPACITY[(15000, 96, 160)][0] >= int(ref["gsid"].numel())
+
+
+@pytest.mark.parametrize("dtype,geom", [(torch.float32, False), (torch.float32, True),
+                                        (torch.bfloat16, False)])
+def test_render_views_sums_view_gradients_in_fp32(cuda_ok, dtype, geom):
+    """render_palette_views: each view's forward equals render_palette's; the
+    backward equals the sum of the single-view gradients taken in FP32 (first
+    view through gsb_render_backward, the others through
+    gsb_render_backward_accumulate), cast once to the parameters' dtype.  FP32
+    sums are compared to 1e-6 relative (the adjoint's atomics may add in a
+    different order); BF16 gradients to one BF16 rounding of the FP32 sum."""
+    from palette_b200.render import render_palette_views
+    sc, st, _ = _setup("lowrank", 3, dtype, n=20000, W=96, H=80, eye=(4.0, -6.0, 1.0))
+    cams = [look_at(e, width=96, height=80, device="cuda")
+            for e in ((4.0, -6.0, 1.0), (-5.0, -5.0, 2.0), (0.5, 7.0, -1.0))]
+    g = torch.Generator("cuda").manual_seed(9)
+    dls = [torch.randn((5, 80, 96), device="cuda", generator=g) for _ in cams]
+    names = ["dc", "A", "B"] + (list(GEOM) if geom else [])
+
+    def leaves(dt):
+        return {k: st[k].detach().to(dt if k in ("dc", "A", "B") else torch.float32).clone()
+                .requires_grad_(k in names) for k in list(GEOM) + ["dc", "A", "B"]}
+    lv = leaves(dtype)
+    layers, taus, depths = render_palette_views(lv["pws"], lv["rots"], lv["scales"], lv["alphas"],
+                                                cams, dc=lv["dc"], A=lv["A"], B=lv["B"])
+    torch.autograd.backward(layers, dls)
+    # reference: single views with FP32 copies of the same parameter values
+    ref = leaves(torch.float32)
+    for v, cam in enumerate(cams):
+        layer, ft, d = render_palette(ref["pws"], ref["rots"], ref["scales"], ref["alphas"], cam,
+                                      dc=ref["dc"], A=ref["A"], B=ref["B"])
+        if dtype == torch.float32:
+            assert torch.equal(layers[v], layer) and torch.equal(taus[v], ft)
+            assert torch.equal(depths[v], d)
+        else:
+            assert max_abs(layers[v], layer) < 1e-5
+        layer.backward(dls[v])
+    for k in names:
+        got, want = lv[k].grad, ref[k].grad
+        assert got.dtype == lv[k].dtype
+        if dtype == torch.float32:
+            assert rel_err(got, np_of(want).astype(np.float64)) < 1e-6, k
+        else:  # the FP32 sum rounded once to BF16 (atomics order aside: within 1 BF16 ulp)
+            assert rel_err(got.float(), np_of(want).astype(np.float64)) < 5e-3, k
+            close = (got.float() - want.to(torch.bfloat16).float()).abs()
+            assert bool((close <= want.abs() * 2.0 ** -7 + 1e-30).all()), k
