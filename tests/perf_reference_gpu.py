@@ -9,7 +9,10 @@ and once through this build's gsplatcu, on identical synthetic inputs, plus
 this build's fused path (palette_b200.render.render_palette, weights-only
 backward) on the same scene.  Device time per iteration by CUDA events
 (median of 10 repeats after warm-up, then the median over 3 rounds in which
-the implementations alternate, after 2 s of GPU load to settle the clocks).  Not collected by pytest: run it
+the implementations alternate, after 2 s of GPU load to settle the clocks).
+Forward calls are also timed back to back (``*_forward_pipelined``: 10 calls
+between one pair of events), where a call's host work overlaps the device
+work of the calls before it.  Not collected by pytest: run it
 on a GPU box and keep the printed JSON.
 
     python tests/perf_reference_gpu.py [--gaussians 1000000] [--width 1920] [--height 1080]
@@ -74,6 +77,22 @@ def timed(fn, reps=10, warm=3):
     return statistics.median(ts)
 
 
+def timed_pipelined(fn, reps=10, warm=3):
+    """Time per call of `reps` calls issued back to back between one pair of
+    events: the host work of a call overlaps the device work of the calls
+    before it (a throughput, where timed() measures the latency of one call)."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
 def burn(seconds=2.0):
     """Keep the GPU busy so that its clocks have ramped up before timing."""
     a = torch.randn((4096, 4096), device="cuda")
@@ -130,6 +149,8 @@ def main():
             row = {}
             for name, g in (("reference", ref), ("b200_ops", ours)):
                 row[name + "_forward"] = timed(lambda: forward(g, st, cam, mode), a.reps)
+                row[name + "_forward_pipelined"] = timed_pipelined(
+                    lambda: forward(g, st, cam, mode), a.reps)
 
                 def fb():
                     saved, _ = forward(g, st, cam, mode)
@@ -137,12 +158,13 @@ def main():
                 row[name + "_fwd_bwd"] = timed(fb, a.reps)
             with torch.no_grad():
                 row["b200_fused_forward"] = timed(lambda: fused(False), a.reps)
+                row["b200_fused_forward_pipelined"] = timed_pipelined(lambda: fused(False), a.reps)
             row["b200_fused_fwd_bwd"] = timed(lambda: fused(True), a.reps)
             rounds.append(row)
         row = {k: statistics.median(r[k] for r in rounds) for k in rounds[0]}
         row["reference_forward_range"] = [min(r["reference_forward"] for r in rounds),
                                           max(r["reference_forward"] for r in rounds)]
-        for k in ("forward", "fwd_bwd"):
+        for k in ("forward", "forward_pipelined", "fwd_bwd"):
             row[f"speedup_ops_{k}"] = row[f"reference_{k}"] / row[f"b200_ops_{k}"]
             row[f"speedup_fused_{k}"] = row[f"reference_{k}"] / row[f"b200_fused_{k}"]
         out["cases"][mode + ("" if mode == "full" else "_rank1")] = {
