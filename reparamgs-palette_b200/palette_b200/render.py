@@ -24,7 +24,9 @@ its backward sums the views' gradients in FP32 inside the kernels (the first
 view overwrites the FP32 gradient buffers, the others add to them) and casts
 once, so BF16 parameters are not accumulated in BF16.
 """
+import contextlib
 import ctypes as C
+import weakref
 
 import torch
 
@@ -37,11 +39,33 @@ def _f32c(t):
     return t if t.dtype == _F32 and t.is_contiguous() else t.to(_F32).contiguous()
 
 
+# gsb_camera structs of recently used camera objects, rebuilt when any of the
+# camera's fields or tensors (identity or in-place version) changes.  An entry
+# holds its tensors, so their identities cannot be reused while it lives.
+_CAMS = weakref.WeakKeyDictionary()
+
+
+def _cam_signature(cam):
+    return (id(cam.Rcw), cam.Rcw._version, id(cam.tcw), cam.tcw._version, id(cam.twc),
+            cam.twc._version, float(cam.fx), float(cam.fy), float(cam.cx), float(cam.cy),
+            int(cam.width), int(cam.height))
+
+
 def camera_struct(cam):
     """(gsb_camera, tensors to keep alive) for a camera-like object."""
+    try:
+        hit = _CAMS.get(cam)
+    except TypeError:  # not weak-referenceable: no caching
+        hit = None
+    if hit is not None and hit[0] == _cam_signature(cam):
+        return hit[1], hit[2]
     Rcw, tcw, twc = _f32c(cam.Rcw), _f32c(cam.tcw), _f32c(cam.twc)
     c = _lib.Camera(Rcw.data_ptr(), tcw.data_ptr(), twc.data_ptr(), float(cam.fx), float(cam.fy),
                     float(cam.cx), float(cam.cy), int(cam.width), int(cam.height))
+    try:  # the entry keeps the camera's own tensors, so their ids stay theirs
+        _CAMS[cam] = (_cam_signature(cam), c, (Rcw, tcw, twc, cam.Rcw, cam.tcw, cam.twc))
+    except TypeError:
+        pass
     return c, (Rcw, tcw, twc)
 
 
@@ -67,7 +91,8 @@ def _render_one(pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank):
     L = _lib.lib()
     camst, keep = camera_struct(cam)
     params = _params(mode, K, P, Q, rank, w0, A, B)
-    with torch.cuda.device(dev):
+    on_dev = dev.index == torch.cuda.current_device()
+    with contextlib.nullcontext() if on_dev else torch.cuda.device(dev):
         st = _lib.stream_of(pws)
         state = torch.empty(int(L.gsb_splat_state_bytes(n, K, H, W)), dtype=torch.uint8,
                             device=dev)
@@ -165,6 +190,10 @@ def render_palette(pws, rots, scales, alphas, cam, shs=None, dc=None, A=None, B=
     pws, rots, scales = _check("pws", pws), _check("rots", rots), _check("scales", scales)
     alphas = _check("alphas", alphas)
     w0, A, B, mode, K, P, Q, rank = _weight_args(shs, dc, A, B, K)
+    if not (torch.is_grad_enabled() and any(
+            t is not None and t.requires_grad for t in (pws, rots, scales, alphas, w0, A, B))):
+        # nothing to differentiate: render without the autograd node
+        return _render_one(pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank)[:3]
     return _RenderPalette.apply(pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank)
 
 
