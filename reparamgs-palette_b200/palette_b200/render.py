@@ -69,11 +69,34 @@ def camera_struct(cam):
     return c, (Rcw, tcw, twc)
 
 
+_PARAMS = {}
+_STATE_BYTES = {}
+
+
 def _params(mode, K, P, Q, rank, w0, A, B):
-    return _lib.PaletteParams(mode, _lib.DTYPE_BF16 if w0.dtype == torch.bfloat16 else
-                              _lib.DTYPE_F32, K, P, Q, rank, w0.data_ptr(),
-                              A.data_ptr() if A is not None else None,
-                              B.data_ptr() if B is not None else None)
+    """gsb_palette_params of the weight parameters (pointers and shapes only,
+    so a struct built for the same tensors' storage can be reused)."""
+    key = (mode, w0.dtype, K, P, Q, rank, w0.data_ptr(),
+           A.data_ptr() if A is not None else 0, B.data_ptr() if B is not None else 0)
+    p = _PARAMS.get(key)
+    if p is None:
+        if len(_PARAMS) > 64:
+            _PARAMS.clear()
+        p = _PARAMS[key] = _lib.PaletteParams(
+            mode, _lib.DTYPE_BF16 if w0.dtype == torch.bfloat16 else _lib.DTYPE_F32, K, P, Q,
+            rank, key[6], A.data_ptr() if A is not None else None,
+            B.data_ptr() if B is not None else None)
+    return p
+
+
+def _state_bytes(n, K, H, W):
+    key = (n, K, H, W)
+    b = _STATE_BYTES.get(key)
+    if b is None:
+        if len(_STATE_BYTES) > 256:
+            _STATE_BYTES.clear()
+        b = _STATE_BYTES[key] = int(_lib.lib().gsb_splat_state_bytes(n, K, H, W))
+    return b
 
 
 def _check(name, t, dtypes=(_F32,)):
@@ -94,8 +117,7 @@ def _render_one(pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank):
     on_dev = dev.index == torch.cuda.current_device()
     with contextlib.nullcontext() if on_dev else torch.cuda.device(dev):
         st = _lib.stream_of(pws)
-        state = torch.empty(int(L.gsb_splat_state_bytes(n, K, H, W)), dtype=torch.uint8,
-                            device=dev)
+        state = torch.empty(_state_bytes(n, K, H, W), dtype=torch.uint8, device=dev)
         depths = torch.empty((n,), dtype=_F32, device=dev)
         _lib.call("render_palette", "gsb_render_preprocess", n, C.byref(camst), _lib.ptr(pws),
                   _lib.ptr(rots), _lib.ptr(scales), _lib.ptr(alphas), C.byref(params),
