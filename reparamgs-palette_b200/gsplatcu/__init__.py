@@ -241,14 +241,32 @@ _CAPACITY = {}
 _READBACK = {}
 
 
+def _mapped_address(host):
+    """Device address of a pinned host tensor, or None when the runtime does
+    not map it into the device's address space."""
+    try:
+        from cuda.bindings import runtime as rt
+        err, dptr = rt.cudaHostGetDevicePointer(host.data_ptr(), 0)
+        if err == rt.cudaError_t.cudaSuccess:
+            return int(dptr)
+        rt.cudaGetLastError()  # a refused query must not surface at the next launch check
+    except Exception:
+        pass
+    return None
+
+
 def _readback_buffers(dev):
-    """(device status words, pinned host copy, event) of the calling thread on
-    `dev`; the host copy is read before the thread renders again."""
+    """(device status words, pinned host words, event, device address of the
+    host words or None) of the calling thread on `dev`.  With an address the
+    status kernel writes the host words directly (no copy in the stream
+    between it and the sort); the host words are read before the thread
+    renders again."""
     key = (dev, threading.get_ident())
     b = _READBACK.get(key)
     if b is None:
-        b = (torch.empty((4,), dtype=torch.int32, device=dev),
-             torch.empty((4,), dtype=torch.int32, pin_memory=True), torch.cuda.Event())
+        host = torch.empty((4,), dtype=torch.int32, pin_memory=True)
+        b = (torch.empty((4,), dtype=torch.int32, device=dev), host, torch.cuda.Event(),
+             _mapped_address(host))
         _READBACK[key] = b
     return b
 
@@ -266,9 +284,13 @@ def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_
     key = (n, H, W)
     if key in _CAPACITY:
         cap, dkey = _CAPACITY[key]
-        status, host, counted = _readback_buffers(dev)
-        call(op, "gsb_splat_patch_status", n, H, W, cap, dkey, ptr(state), ptr(status), st)
-        host.copy_(status, non_blocking=True)
+        status, host, counted, mapped = _readback_buffers(dev)
+        if mapped is not None:
+            call(op, "gsb_splat_patch_status", n, H, W, cap, dkey, ptr(state), C.c_void_p(mapped),
+                 st)
+        else:
+            call(op, "gsb_splat_patch_status", n, H, W, cap, dkey, ptr(state), ptr(status), st)
+            host.copy_(status, non_blocking=True)
         counted.record(torch.cuda.current_stream(dev))
         ws = torch.empty(max(1, int(L.gsb_splat_sort_capacity_bytes(n, H, W, cap, dkey))),
                          dtype=torch.uint8, device=dev)
