@@ -193,7 +193,8 @@ int gsb_splat_sort_static(int64_t n, int height, int width, const gsb_splat_plan
  * `sort_ws` of gsb_splat_sort_capacity_bytes(...) bytes and gsid_out of
  * patch_capacity entries.  status (device uint32[3]) receives the overflow
  * bits GSB_STATUS_PATCH_OVERFLOW / GSB_STATUS_DEPTH_KEY_OVERFLOW (or 0) and
- * the true patch count (low, high word); on an
+ * the true patch count (low, high word); it may be NULL when the caller
+ * reads the same words through gsb_splat_patch_status.  On an
  * overflow every range is left empty (the image then shows nothing) and the
  * caller re-renders with a larger capacity.  Without overflow the results
  * equal gsb_splat_sort's.  No counterpart in the reference, which always

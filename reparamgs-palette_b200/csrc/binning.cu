@@ -34,19 +34,21 @@ static void state_layout(int64_t n, int channels, int H, int W, size_t* offs) {
   offs[3] = b; b += align256((size_t)(nb > 0 ? nb : 1) * 4);          // block sums
   offs[4] = b; b += align256(16 * 4);                                 // stats
   offs[5] = b; b += align256((size_t)n * record_vec4(channels) * 16); // records
-  offs[6] = b;
+  const int64_t np = (n + kPartBlock - 1) / kPartBlock;
+  offs[6] = b; b += 2 * align256((size_t)(np > 0 ? np : 1) * 4);      // part sums, part max
+  offs[7] = b;
   (void)gx;
   (void)gy;
 }
 
 size_t splat_state_bytes(int64_t n, int channels, int H, int W) {
-  size_t offs[7];
+  size_t offs[8];
   state_layout(n, channels, H, W, offs);
-  return offs[6];
+  return offs[7];
 }
 
 SplatState carve_state(void* base, int64_t n, int channels, int H, int W) {
-  size_t o[7];
+  size_t o[8];
   state_layout(n, channels, H, W, o);
   char* p = (char*)base;
   SplatState s;
@@ -60,6 +62,9 @@ SplatState carve_state(void* base, int64_t n, int channels, int H, int W) {
   s.block_sums = (uint32_t*)(p + o[3]);
   s.stats = (uint32_t*)(p + o[4]);
   s.records = (float4*)(p + o[5]);
+  s.n_parts = (n + kPartBlock - 1) / kPartBlock;
+  s.part_sums = (uint32_t*)(p + o[6]);
+  s.part_max = s.part_sums + align256((size_t)(s.n_parts > 0 ? s.n_parts : 1) * 4) / 4;
   return s;
 }
 
@@ -174,21 +179,52 @@ __global__ void __launch_bounds__(kBinBlock)
 }
 
 // Single-block exclusive scan of the per-block patch counts; writes the
-// total M (low/high words) into stats[0] / stats[3].
+// total M (low/high words) into stats[0] / stats[3].  With `psum` (the fused
+// preprocess) each block's count is first summed from its kBinBlock /
+// kPartBlock parts, and stats[1] (largest depth key) and the other stats
+// words are written here too, so that nothing needs zeroing beforehand.
 __global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__ sums, int64_t nb,
-                                                          uint32_t* __restrict__ stats) {
+                                                          uint32_t* __restrict__ stats,
+                                                          const uint32_t* __restrict__ psum,
+                                                          const uint32_t* __restrict__ pmax,
+                                                          int64_t nparts) {
   pdl_wait();
+  constexpr int kPer = kBinBlock / kPartBlock;
   __shared__ uint32_t warp_tot[32];
   __shared__ unsigned long long carry;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (threadIdx.x == 0) carry = 0ull;
+  if (psum) {
+    uint32_t m = 0;
+    for (int64_t j = threadIdx.x; j < nparts; j += 1024) m = max(m, pmax[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) warp_tot[w] = m;
+    __syncthreads();
+    if (threadIdx.x < 16) {
+      uint32_t mm = 0;
+      if (threadIdx.x == 1)
+        for (int k = 0; k < 32; ++k) mm = max(mm, warp_tot[k]);
+      if (threadIdx.x != 0 && threadIdx.x != 3) stats[threadIdx.x] = mm;  // 1: max; rest 0
+    }
+  }
   __syncthreads();
   for (int64_t base = 0; base < nb; base += 1024 * 4) {
     uint32_t v[4], s = 0;
     const int64_t j0 = base + (int64_t)threadIdx.x * 4;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      v[k] = (j0 + k < nb) ? sums[j0 + k] : 0u;
+      if (psum) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+          const int64_t pj = (j0 + k) * kPer + q;
+          t += pj < nparts ? psum[pj] : 0u;
+        }
+        v[k] = (j0 + k < nb) ? t : 0u;
+      } else {
+        v[k] = (j0 + k < nb) ? sums[j0 + k] : 0u;
+      }
       s += v[k];
     }
     uint32_t incl = s;
@@ -507,9 +543,11 @@ int launch_pack(int64_t n, int H, int W, int channels, const float* us, const fl
   return check_launch("splat_pack");
 }
 
-int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st) {
-  if (n == 0) return GSB_OK;
-  launch_pdl(k_scan_block_sums, dim3(1), dim3(1024), 0, st, s.block_sums, s.n_blocks, s.stats);
+int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st, bool from_parts) {
+  if (n == 0) return from_parts ? launch_zero2(s.stats, 16, nullptr, 0, st) : GSB_OK;
+  launch_pdl(k_scan_block_sums, dim3(1), dim3(1024), 0, st, s.block_sums, s.n_blocks, s.stats,
+             from_parts ? (const uint32_t*)s.part_sums : nullptr,
+             from_parts ? (const uint32_t*)s.part_max : nullptr, s.n_parts);
   return check_launch("splat_scan");
 }
 
@@ -625,10 +663,12 @@ int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const Splat
                          void* ws, int32_t* gsid_out, int32_t* ranges_out, uint32_t* status,
                          cudaStream_t st) {
   (void)H;
-  launch_pdl(k_capacity_status, dim3(1), dim3(1), 0, st, p.M, p.dkey_bits,
-             (const uint32_t*)s.stats, status);
-  int rc = check_launch("splat_sort_capacity (status)");
-  if (rc) return rc;
+  if (status) {  // (callers that read the status through gsb_splat_patch_status pass null)
+    launch_pdl(k_capacity_status, dim3(1), dim3(1), 0, st, p.M, p.dkey_bits,
+               (const uint32_t*)s.stats, status);
+    const int rc = check_launch("splat_sort_capacity (status)");
+    if (rc) return rc;
+  }
   if (p.M == 0 || n == 0) return launch_zero2(ranges_out, p.n_tiles * 2, nullptr, 0, st);
   return p.wide ? sort_t<uint64_t>(p, n, W, s, ws, gsid_out, ranges_out, s.stats, st)
                 : sort_t<uint32_t>(p, n, W, s, ws, gsid_out, ranges_out, s.stats, st);

@@ -288,7 +288,7 @@ GSB_API int gsb_splat_sort_capacity(int64_t n, int height, int width, int64_t pa
   if (rc) return rc;
   GSB_CHECK_ARG(patch_capacity >= 0 && patch_capacity < (int64_t)INT32_MAX,
                 "splat_sort_capacity: capacity out of range");
-  GSB_CHECK_ARG(state && ranges_out && status, "splat_sort_capacity: null pointer");
+  GSB_CHECK_ARG(state && ranges_out, "splat_sort_capacity: null pointer");
   GSB_CHECK_ARG(patch_capacity == 0 || (sort_ws && gsid_out),
                 "splat_sort_capacity: null workspace/output");
   const SortPlan p = make_sort_plan(n, height, width, patch_capacity, max_depth_key);
@@ -446,9 +446,6 @@ GSB_API int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float*
   GSB_CHECK_ARG(n == 0 || (pws && rots && scales && alphas), "render_preprocess: null input");
   const SplatState s =
       carve_state(state, n, params->palette ? 3 : params->K, cam->height, cam->width);
-  if ((rc = launch_zero2(s.stats, 16, s.block_sums, s.n_blocks > 0 ? s.n_blocks : 1,
-                         ST(stream))))
-    return rc;
   FusedArgs f{};
   f.n = n;
   f.gx = (uint32_t)div_up(cam->width, kTile);
@@ -467,7 +464,7 @@ GSB_API int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float*
   rc = launch_render(params->mode, params->dtype, params->K, params->P, params->Q, params->rank, f,
                      false, ST(stream));
   if (rc) return rc;
-  return launch_count_scan(n, s, ST(stream));
+  return launch_count_scan(n, s, ST(stream), true);
 }
 
 GSB_API size_t gsb_render_backward_bytes(int64_t n, int K) {

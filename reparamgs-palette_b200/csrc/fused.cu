@@ -209,15 +209,16 @@ __global__ void __launch_bounds__(kFuseThreads)
                         const T* __restrict__ w0, const T* __restrict__ wa,
                         const T* __restrict__ wb, float4* __restrict__ records,
                         uint2* __restrict__ rects, uint32_t* __restrict__ dkeys,
-                        uint32_t* __restrict__ counts, uint32_t* __restrict__ block_sums,
-                        uint32_t* __restrict__ stats, float* __restrict__ depths_out) {
+                        uint32_t* __restrict__ counts, uint32_t* __restrict__ part_sums,
+                        uint32_t* __restrict__ part_max, float* __restrict__ depths_out) {
   pdl_wait();
   using WS = WRows<MODE, K, P, Q, R>;
   constexpr int V = RecordLayout<COL ? 3 : K>::kVec4;
   static_assert(WS::INS >= 4 * V, "the record span reuses the input staging area");
   extern __shared__ __align__(16) float sm[];
   __shared__ __align__(8) uint64_t bar;
-  __shared__ uint32_t warp_tot[kFuseThreads / 32];
+  __shared__ uint32_t warp_tot[kFuseThreads / 32], warp_max[kFuseThreads / 32];
+  static_assert(kFuseThreads == kPartBlock, "one part per preprocess block");
   __shared__ float s_pal[COL ? 3 * K : 1];
   if constexpr (COL) {
     if (threadIdx.x < 3 * K) s_pal[threadIdx.x] = pal[threadIdx.x];
@@ -330,12 +331,16 @@ __global__ void __launch_bounds__(kFuseThreads)
   uint32_t m = dk;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0 && m) atomicMax(stats + 1, m);
+  if (lane == 0) warp_max[w] = m;
   __syncthreads();  // every thread is done with the staged inputs from here on
-  if (t == 0) {  // block_sums count blocks of kBinBlock Gaussians (zeroed by the caller)
-    uint32_t tot = 0;
-    for (int k = 0; k < nt / 32; ++k) tot += warp_tot[k];
-    if (tot) atomicAdd(block_sums + row0 / kBinBlock, tot);
+  if (t == 0) {  // this block's part of the patch-count scan (k_scan_block_sums)
+    uint32_t tot = 0, mx = 0;
+    for (int k = 0; k < nt / 32; ++k) {
+      tot += warp_tot[k];
+      mx = max(mx, warp_max[k]);
+    }
+    part_sums[blockIdx.x] = tot;
+    part_max[blockIdx.x] = mx;
   }
   // records: assembled over the input staging area, written as one span (the
   // rows of Gaussians without patches are never read)
@@ -743,7 +748,7 @@ static int launch_fused(const FusedArgs& f, bool backward, cudaStream_t st) {
     if ((rc = set_smem(kern, smem))) return rc;
     launch_pdl(kern, dim3(grid), dim3(kFuseThreads), smem, st, f.n, f.gx, f.gy, f.cam, f.palette,
                f.pws, f.rots, f.scales, f.alphas, (const T*)f.w0, (const T*)f.wa, (const T*)f.wb,
-               f.st.records, f.st.rects, f.st.dkeys, f.st.counts, f.st.block_sums, f.st.stats,
+               f.st.records, f.st.rects, f.st.dkeys, f.st.counts, f.st.part_sums, f.st.part_max,
                f.depths_out);
     return check_launch("render_preprocess");
   }

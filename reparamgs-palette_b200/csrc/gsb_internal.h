@@ -56,11 +56,14 @@ struct SplatState {
   uint32_t* counts;      // [n] patches per Gaussian
   uint32_t* block_sums;  // [n_blocks] -> exclusive block offsets after the scan
   uint32_t* stats;       // [16]: 0/3 = M low/high, 1 = max depth key
+  uint32_t* part_sums;   // [n_parts] patches per kPartBlock Gaussians (fused preprocess)
+  uint32_t* part_max;    // [n_parts] their largest depth key
   int rec_vec4;          // float4 vectors per record
-  int64_t n_blocks;
+  int64_t n_blocks, n_parts;
   int gx, gy;
 };
 constexpr int kBinBlock = 256;      // Gaussians per binning block
+constexpr int kPartBlock = 64;      // Gaussians per fused-preprocess block (a quarter binning block)
 constexpr int kRadixBits = 9;                  // digit width of one radix pass
 constexpr int kRadixBins = 1 << kRadixBits;  // digits per pass
 int record_vec4(int channels);
@@ -70,7 +73,9 @@ SplatState carve_state(void* base, int64_t n, int channels, int H, int W);
 int launch_pack(int64_t n, int H, int W, int channels, const float* us, const float* cinv,
                 const float* alphas, const void* feats, int feat_dtype, float* depths,
                 int32_t* areas, bool bin, const SplatState& s, cudaStream_t st);
-int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st);
+// from_parts: the block sums and the largest depth key are formed from the
+// fused preprocess's per-part values (nothing needs zeroing beforehand).
+int launch_count_scan(int64_t n, const SplatState& s, cudaStream_t st, bool from_parts = false);
 
 struct SortPlan {
   int tile_bits, dkey_bits, key_bits, passes;

@@ -296,7 +296,7 @@ def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_
                          dtype=torch.uint8, device=dev)
         full = torch.empty((max(1, cap),), dtype=torch.int32, device=dev)
         call(op, "gsb_splat_sort_capacity", n, H, W, cap, dkey, ptr(state), ptr(ws), ptr(full),
-             ptr(ranges), ptr(status), st)
+             ptr(ranges), None, st)  # (status read above)
         call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(full), ptr(state),
              float(tau_init), ptr(out), ptr(contrib), ptr(final_tau), st)
         counted.synchronize()
