@@ -21,7 +21,12 @@ def example_scene():
 
 
 def np_of(t):
-    return t.detach().float().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+    """numpy copy of a tensor: floating types as float32 (numpy has no BF16),
+    integer types unchanged (a float32 copy would round them above 2^24)."""
+    if not isinstance(t, torch.Tensor):
+        return np.asarray(t)
+    t = t.detach()
+    return (t.float() if t.is_floating_point() else t).cpu().numpy()
 
 
 def forward_ops(gsc, sc, cam, mode="full"):
