@@ -219,9 +219,25 @@ __global__ void __launch_bounds__(kGeoThreads)
 #pragma unroll
   for (int i = 0; i < KC; ++i) dP[i][0] = dP[i][1] = dP[i][2] = 0.f;
   float lgeo = 0.f, lpos = 0.f;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < hw;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    const float C[3] = {target[p], target[hw + p], target[2 * hw + p]};
+  // The next pixel's inputs are loaded while this one is computed (few warps
+  // fit per SM at this register count, so the loads would stall otherwise).
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  float Cn[3], Ln[K];
+  auto fetch = [&](int64_t q) {
+    if (q < hw) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Cn[c] = target[c * hw + q];
+#pragma unroll
+      for (int k = 0; k < K; ++k) Ln[k] = layer[k * hw + q];
+    }
+  };
+  fetch((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < hw; p += stride) {
+    const float C[3] = {Cn[0], Cn[1], Cn[2]};
+    float Lp[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) Lp[k] = Ln[k];
+    fetch(p + stride);
     float err[KC], xs[KC][4];  // per tetrahedron: error and coordinates
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
@@ -268,7 +284,7 @@ __global__ void __launch_bounds__(kGeoThreads)
     float gW[K];  // d loss / d target
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const float wt = layer[k * hw + p];
+      const float wt = Lp[k];
       const float d = wt - Wc[k];
       float g;
       if (kind == 0) {
