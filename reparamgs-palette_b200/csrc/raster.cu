@@ -162,6 +162,40 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4)
         while (mask) {
           const int jj = s + __ffs(mask) - 1;
           mask &= mask - 1;
+          if (mask) {
+            // two records at once: both opacity terms first, so that their
+            // exp() chains overlap, then the two blends in list order
+            const int jb = s + __ffs(mask) - 1;
+            mask &= mask - 1;
+            if (done) continue;
+            const float4 a0 = srec[jj], a1 = srec[kBatch + jj];
+            const float4 b0 = srec[jb], b1 = srec[kBatch + jb];
+            const float dxa = a0.x - (float)px, dya = a0.y - (float)py;
+            const float dxb = b0.x - (float)px, dyb = b0.y - (float)py;
+            const float ma = fmaxf(0.0f, maha_sq(a0.z, a0.w, a1.x, dxa, dya));
+            const float mb = fmaxf(0.0f, maha_sq(b0.z, b0.w, b1.x, dxb, dyb));
+            const float apa = fminf(kAlphaMax, a1.z * expf(-0.5f * ma));
+            const float apb = fminf(kAlphaMax, b1.z * expf(-0.5f * mb));
+            if (!(ma > a1.y) && !(apa < kAlphaMin)) {
+              float f[K];
+              load_feats<K>(srec, jj, a1.w, f);
+#pragma unroll
+              for (int k = 0; k < K; ++k) acc[k] += T * apa * f[k];
+              cont = base + jj + 1;
+              T *= (1.f - apa);
+              if (T < kTransMin) done = true;
+            }
+            if (!done && !(mb > b1.y) && !(apb < kAlphaMin)) {
+              float f[K];
+              load_feats<K>(srec, jb, b1.w, f);
+#pragma unroll
+              for (int k = 0; k < K; ++k) acc[k] += T * apb * f[k];
+              cont = base + jb + 1;
+              T *= (1.f - apb);
+              if (T < kTransMin) done = true;
+            }
+            continue;
+          }
           if (done) continue;
           const float4 v0 = srec[jj];           // ux uy qa qb
           const float4 v1 = srec[kBatch + jj];  // qc c2 alpha ch0
@@ -193,17 +227,19 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4)
 }
 
 // ------------------------------------------------------------- adjoint
-// Sum of NV per-lane values over the warp with NV-1 + 5-log2(NV) shuffles:
-// each exchange step halves the values a lane carries (lanes with the step's
-// bit set keep the upper half), so the totals end up spread over the lanes.
-// Returns this lane's total; *idx is the value index it holds and *owner is
-// set on exactly one lane per index.
-template <int NV>
+// Sum of NV per-lane values over groups of 2*OFF0 lanes (the whole warp for
+// OFF0 = 16, each half-warp for OFF0 = 8) with NV-1 + log2(2*OFF0/NV)
+// shuffles: each exchange step halves the values a lane carries (lanes with
+// the step's bit set keep the upper half), so the totals end up spread over
+// the group's lanes.  Returns this lane's total; *idx is the value index it
+// holds and *owner is set on exactly one lane per index and group.
+template <int NV, int OFF0 = 16>
 __device__ __forceinline__ float warp_transpose_sum(float (&x)[NV], int lane, int* idx,
                                                     bool* owner) {
-  static_assert(NV >= 1 && NV <= 16 && (NV & (NV - 1)) == 0, "NV must be a power of two <= 16");
+  static_assert(NV >= 1 && NV <= 2 * OFF0 && (NV & (NV - 1)) == 0,
+                "NV must be a power of two no larger than the group");
   int id = 0;
-  int off = 16;
+  int off = OFF0;
 #pragma unroll
   for (int w = NV / 2; w >= 1; w >>= 1, off >>= 1) {
     const bool hi = (lane & off) != 0;
@@ -269,6 +305,94 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
     x[K + 5] += dap * (-0.5f * ap * (dy * dy));         // conic c
   }
   return true;
+}
+
+// Weights-only adjoint of two contributors at once: slot ja lies behind slot
+// jb in list order, so it is undone first.  Both records' opacity terms are
+// evaluated for both pixels before either transmittance update, so the four
+// exp() chains overlap; the skip tests and the T recovery are exactly those
+// of adjoint_pixel.  The two gradient vectors are summed together: one
+// exchange at offset 16 leaves ja's partial sums on lanes 0-15 and jb's on
+// lanes 16-31, then each half-warp transposes its K values (5 + 8 shuffles
+// for K = 5, against 2 x 9 for two single reductions).
+template <int K>
+__device__ __forceinline__ void adjoint_weights_pair(BwdPixel<K> (&p)[2], int base, int ja, int jb,
+                                                     const float4* srec, const int32_t* sgid,
+                                                     float fx, float fy0, float fy1, int lane,
+                                                     float* __restrict__ dfeat) {
+  const float4 a0 = srec[ja], a1 = srec[kBatch + ja];
+  const float4 b0 = srec[jb], b1 = srec[kBatch + jb];
+  const float fy[2] = {fy0, fy1};
+  float apa[2], apb[2];
+  bool ua[2], ub[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const float dxa = a0.x - fx, dya = a0.y - fy[q];
+    const float ma = fmaxf(0.f, maha_sq(a0.z, a0.w, a1.x, dxa, dya));
+    apa[q] = fminf(kAlphaMax, a1.z * expf(-0.5f * ma));
+    ua[q] = base + ja < p[q].cont && !(ma > a1.y) && !(apa[q] < kAlphaMin);
+    const float dxb = b0.x - fx, dyb = b0.y - fy[q];
+    const float mb = fmaxf(0.f, maha_sq(b0.z, b0.w, b1.x, dxb, dyb));
+    apb[q] = fminf(kAlphaMax, b1.z * expf(-0.5f * mb));
+    ub[q] = base + jb < p[q].cont && !(mb > b1.y) && !(apb[q] < kAlphaMin);
+  }
+  float xa[K], xb[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) xa[k] = xb[k] = 0.f;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (ua[q]) {
+      p[q].T = __fdividef(p[q].T, 1.f - apa[q]);
+      const float wgt = apa[q] * p[q].T;
+#pragma unroll
+      for (int k = 0; k < K; ++k) xa[k] += p[q].dl[k] * wgt;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (ub[q]) {
+      p[q].T = __fdividef(p[q].T, 1.f - apb[q]);
+      const float wgt = apb[q] * p[q].T;
+#pragma unroll
+      for (int k = 0; k < K; ++k) xb[k] += p[q].dl[k] * wgt;
+    }
+  }
+  const bool ha = ua[0] || ua[1], hb = ub[0] || ub[1];
+  const unsigned ca = __ballot_sync(0xffffffffu, ha), cb = __ballot_sync(0xffffffffu, hb);
+  if (!(ca | cb)) return;
+  if (__popc(ca) <= 1 && __popc(cb) <= 1) {
+    if (ha) {
+      const int64_t g = sgid[ja];
+#pragma unroll
+      for (int k = 0; k < K; ++k) atomicAdd(dfeat + g * K + k, xa[k]);
+    }
+    if (hb) {
+      const int64_t g = sgid[jb];
+#pragma unroll
+      for (int k = 0; k < K; ++k) atomicAdd(dfeat + g * K + k, xb[k]);
+    }
+    return;
+  }
+  constexpr int NV = Pow2<K>::value;
+  const bool hi = (lane & 16) != 0;
+  float y[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    if (k < K) {
+      const float send = hi ? xa[k] : xb[k];
+      const float keep = hi ? xb[k] : xa[k];
+      y[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    } else {
+      y[k] = 0.f;
+    }
+  }
+  int vidx;
+  bool owner;
+  const float tot = warp_transpose_sum<NV, 8>(y, lane, &vidx, &owner);
+  if (owner && vidx < K && (hi ? cb : ca) != 0u) {
+    const int64_t g = sgid[hi ? jb : ja];
+    atomicAdd(dfeat + g * K + vidx, tot);
+  }
 }
 
 // Walks each pixel's contributors back to front from its `contrib` index,
@@ -345,6 +469,13 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
       while (mask) {
         const int msb = 31 - __clz(mask);
         mask &= ~(1u << msb);
+        if (!GEOM && mask) {
+          const int msb2 = 31 - __clz(mask);
+          mask &= ~(1u << msb2);
+          adjoint_weights_pair<K>(p, base, s_lo + msb, s_lo + msb2, srec, sgid, fx, fy0, fy1,
+                                  lane, dfeat);
+          continue;
+        }
         const int jj = s_lo + msb;
         const int idx = base + jj;
         float x[NV];
