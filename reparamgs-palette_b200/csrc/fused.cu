@@ -396,12 +396,19 @@ struct BwdRaw {
   static constexpr int kFloats = (kHalfs + 1) / 2;
 };
 
+// Stages the block's input rows.  With `acc` (gradients added to what the
+// outputs hold) and a full, aligned block, the outputs' current rows are
+// bulk-loaded into the block's gradient area in the same transaction, so the
+// adjoint adds into them in shared memory and stores them like fresh rows.
+// Returns 0 when a bulk copy timed out, 2 when the gradient rows were
+// preloaded, else 1.
 template <int MODE, int K, int P, int Q, int R, bool GEOM, typename T>
-__device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const float* pws,
-                                               const float* rots, const float* scales,
-                                               const T* w0, const T* wa, const T* wb,
-                                               const float* g_feat, float* sm, float* raw,
-                                               uint64_t* bar) {
+__device__ __forceinline__ int stage_backward(int64_t n, int64_t row0, const float* pws,
+                                              const float* rots, const float* scales,
+                                              const T* w0, const T* wa, const T* wb,
+                                              const float* g_feat, bool acc, const float* d_w0,
+                                              const float* d_wa, const float* d_wb, float* sm,
+                                              float* raw, uint64_t* bar) {
   using BP = BwdPlan<MODE, K, P, Q, R, GEOM>;
   using WS = WRows<MODE, K, P, Q, R>;
   const int nt = blockDim.x;
@@ -414,10 +421,22 @@ __device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const fl
     bulk = bulk && aligned16(wa + row0 * WS::WA) && aligned16(wb + row0 * WS::WB) &&
            (nt * WS::WA * sizeof(T)) % 16 == 0 && (nt * WS::WB * sizeof(T)) % 16 == 0;
   const bool raw16 = bulk && sizeof(T) == 2;
+  bool pre = bulk && acc && aligned16(d_w0 + row0 * WS::W0) && (nt * WS::W0 * 4) % 16 == 0;
+  if (MODE != GSB_WEIGHTS_FULL)
+    pre = pre && aligned16(d_wa + row0 * WS::WA) && aligned16(d_wb + row0 * WS::WB) &&
+          (nt * WS::WA * 4) % 16 == 0 && (nt * WS::WB * 4) % 16 == 0;
   if (bulk && threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_arrive_expect_tx(bar, (uint32_t)(nt * (BP::P_ + BP::G_ + BP::Q_ + BP::S_) * 4 +
-                                          nt * (BP::W0_ + BP::A_ + BP::B_) * sizeof(T)));
+                                          nt * (BP::W0_ + BP::A_ + BP::B_) * sizeof(T) +
+                                          (pre ? nt * BP::out_floats * 4 : 0)));
+  }
+  if (pre && threadIdx.x == 0) {
+    bulk_load(sm + nt * BP::o_dw0, d_w0 + row0 * WS::W0, (uint32_t)(nt * WS::W0 * 4), bar);
+    if constexpr (MODE != GSB_WEIGHTS_FULL) {
+      bulk_load(sm + nt * BP::o_dwa, d_wa + row0 * WS::WA, (uint32_t)(nt * WS::WA * 4), bar);
+      bulk_load(sm + nt * BP::o_dwb, d_wb + row0 * WS::WB, (uint32_t)(nt * WS::WB * 4), bar);
+    }
   }
   stage_rows<3>(pws, row0, n, sm + nt * BP::o_p, bulk, bar);
   stage_rows<K>(g_feat, row0, n, sm + nt * BP::o_g, bulk, bar);
@@ -449,7 +468,7 @@ __device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const fl
   if (bulk && !mbar_wait(bar, 0)) {
     if (threadIdx.x == 0) atomicOr(&g_fused_status, kStatusBulkTimeout);
     mbar_wait(bar, 0);  // bounded second wait for copies still in flight
-    return false;
+    return 0;
   }
   if constexpr (sizeof(T) == 2) {  // raw BF16 rows -> their float areas
     if (raw16) {
@@ -465,7 +484,7 @@ __device__ __forceinline__ bool stage_backward(int64_t n, int64_t row0, const fl
     }
     __syncthreads();
   }
-  return true;
+  return pre ? 2 : 1;
 }
 
 // Writes one gradient array's block span from shared memory: one bulk copy
@@ -532,9 +551,11 @@ __global__ void __launch_bounds__(kFuseThreads)
   const int nt = blockDim.x, t = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
   float* raw = sm + nt * (BP::floats + PadRows<WS::W0>::kExtra);
-  if (!stage_backward<MODE, K, P, Q, R, GEOM, T>(n, row0, pws, rots, scales, w0, wa, wb, g_feat, sm,
-                                                 raw, &bar))
-    return;
+  const int staged = stage_backward<MODE, K, P, Q, R, GEOM, T>(
+      n, row0, pws, rots, scales, w0, wa, wb, g_feat, acc, d_w0, d_wa, d_wb, sm, raw, &bar);
+  if (!staged) return;
+  const bool pre = staged == 2;  // the outputs' rows are in the gradient area: add to them
+  const auto put = [pre](float* d, float v) { *d = pre ? *d + v : v; };
   const int64_t i = row0 + t;
   // full-SH gradient rows are built at an odd stride past the plan's regions
   // (see PadRows) and packed contiguously before they are stored
@@ -632,7 +653,12 @@ __global__ void __launch_bounds__(kFuseThreads)
         }
     } else {
 #pragma unroll
-      for (int k = 0; k < K; ++k) o_w0[k] = gw[k] * SH_C0;
+      for (int k = 0; k < K; ++k) {
+        if constexpr (PR::kPad)
+          o_w0[k] = gw[k] * SH_C0;  // packed (and added) below
+        else
+          put(o_w0 + k, gw[k] * SH_C0);
+      }
       // dC[p][q] = gw_k Y_{l+1} with g = l*K + k = p*Q + q
 #pragma unroll
       for (int pp = 0; pp < P; ++pp) {
@@ -657,7 +683,7 @@ __global__ void __launch_bounds__(kFuseThreads)
           }
         }
 #pragma unroll
-        for (int r = 0; r < R; ++r) o_wa[pp * R + r] = acc[r];
+        for (int r = 0; r < R; ++r) put(o_wa + pp * R + r, acc[r]);
       }
 #pragma unroll
       for (int qq = 0; qq < Q; ++qq) {
@@ -672,7 +698,7 @@ __global__ void __launch_bounds__(kFuseThreads)
           for (int r = 0; r < R; ++r) acc[r] += dC * s_wa[pp * R + r];
         }
 #pragma unroll
-        for (int r = 0; r < R; ++r) o_wb[r * Q + qq] = acc[r];
+        for (int r = 0; r < R; ++r) put(o_wb + r * Q + qq, acc[r]);
       }
     }
     if constexpr (GEOM) {
@@ -689,8 +715,9 @@ __global__ void __launch_bounds__(kFuseThreads)
     }
   }
   // parameter gradients: shared memory -> global, block span by block span;
-  // with `acc`, added to what the outputs hold (coalesced read-add-write)
-  if (acc) {
+  // with `acc` and no preloaded rows (a partial or unaligned block), added to
+  // what the outputs hold by a coalesced read-add-write
+  if (acc && !pre) {
     __syncthreads();
     const int64_t rows = min((int64_t)nt, n - row0);
     if constexpr (PR::kPad) {
@@ -714,7 +741,7 @@ __global__ void __launch_bounds__(kFuseThreads)
     const float* src = sm + nt * BP::floats;
     for (int e = t; e < nt * WS::W0; e += nt) {
       const int r = e / WS::W0, c = e - r * WS::W0;
-      dst[e] = src[r * PR::kStride + c];
+      dst[e] = pre ? dst[e] + src[r * PR::kStride + c] : src[r * PR::kStride + c];
     }
   }
   fence_proxy_async_shared();

@@ -297,3 +297,51 @@ def test_render_views_sums_view_gradients_in_fp32(cuda_ok, dtype, geom):
             assert rel_err(got.float(), np_of(want).astype(np.float64)) < 5e-3, k
             close = (got.float() - want.to(torch.bfloat16).float()).abs()
             assert bool((close <= want.abs() * 2.0 ** -7 + 1e-30).all()), k
+
+
+@pytest.mark.parametrize("mode,K,dtype", [("full", 5, torch.float32), ("full", 5, torch.bfloat16),
+                                          ("lowrank", 6, torch.float32)])
+def test_render_views_accumulate_padded_rows(cuda_ok, mode, K, dtype):
+    """The accumulating adjoint adds into the gradient rows it bulk-loads with
+    its inputs (full blocks) or by a read-add-write (the partial last block).
+    Full-SH rows (16K floats) and even-K rows are built at a padded stride and
+    packed before the store, so both take the add in the packing step: the
+    views' summed gradients equal the single-view gradients summed in FP32."""
+    from palette_b200.render import render_palette_views
+    n, W, H = 9000, 80, 64  # 70 full blocks of 128 and a partial one
+    sc = synthetic_scene(n, seed=5, mode=mode, rank=3)
+    st = to_torch(sc, "cuda", dtype)
+    if mode == "lowrank":  # K = 6 palette weights, rank-3 factors A [n,6,3], B [n,3,15]
+        gen = torch.Generator().manual_seed(6)
+        st["dc"] = (0.3 * torch.randn((n, K), generator=gen)).to("cuda", dtype)
+        st["A"] = (0.2 * torch.randn((n, K, 3), generator=gen)).to("cuda", dtype)
+        st["B"] = (0.2 * torch.randn((n, 3, 15), generator=gen)).to("cuda", dtype)
+    cams = [look_at(e, width=W, height=H, device="cuda")
+            for e in ((4.0, -6.0, 1.0), (-5.0, -5.0, 2.0), (0.5, 7.0, -1.0))]
+    g = torch.Generator("cuda").manual_seed(3)
+    dls = [torch.randn((K, H, W), device="cuda", generator=g) for _ in cams]
+    pnames = ["shs"] if mode == "full" else ["dc", "A", "B"]
+
+    def leaves(dt):
+        out = {k: st[k].detach().float() for k in GEOM}
+        out.update({k: st[k].detach().to(dt).clone().requires_grad_() for k in pnames})
+        return out
+
+    def kw(lv):
+        return {k: lv[k] for k in pnames}
+    lv = leaves(dtype)
+    layers, _, _ = render_palette_views(lv["pws"], lv["rots"], lv["scales"], lv["alphas"], cams,
+                                        **kw(lv))
+    torch.autograd.backward(layers, dls)
+    ref = leaves(torch.float32)
+    for v, cam in enumerate(cams):
+        layer, _, _ = render_palette(ref["pws"], ref["rots"], ref["scales"], ref["alphas"], cam,
+                                     **kw(ref))
+        layer.backward(dls[v])
+    for k in pnames:
+        got, want = lv[k].grad.float(), ref[k].grad
+        assert float(want.abs().max()) > 0, k
+        if dtype == torch.float32:
+            assert rel_err(got, np_of(want).astype(np.float64)) < 1e-6, k
+        else:
+            assert rel_err(got, np_of(want).astype(np.float64)) < 5e-3, k
