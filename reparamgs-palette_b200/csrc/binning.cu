@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kBinBlock)
            uint32_t* __restrict__ dkeys, uint32_t* __restrict__ counts,
            uint32_t* __restrict__ block_sums, uint32_t* __restrict__ stats) {
   pdl_wait();
-  __shared__ uint32_t warp_tot[8];
+  __shared__ uint32_t warp_tot[8], warp_max[kBinBlock / 32];
   const int64_t i = (int64_t)blockIdx.x * kBinBlock + threadIdx.x;
   uint32_t cnt = 0, dk = 0;
   if (i < n) {
@@ -168,14 +168,22 @@ __global__ void __launch_bounds__(kBinBlock)
       if (v < V) rec[v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
   }
   if (!bin) return;
-  uint32_t tot;
-  block_excl_scan256(cnt, warp_tot, &tot);
-  // block max of the depth keys of binned Gaussians
+  // block max of the depth keys of binned Gaussians: warp maxima, folded by
+  // thread 0 after the scan's barriers, one atomic per block (one per warp
+  // would queue ~n/32 atomics on the same word)
   uint32_t m = dk;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(stats + 1, m);
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+  if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = m;
+  uint32_t tot;
+  block_excl_scan256(cnt, warp_tot, &tot);
+  if (threadIdx.x == 0) {
+    uint32_t bm = 0;
+#pragma unroll
+    for (int k = 0; k < kBinBlock / 32; ++k) bm = max(bm, warp_max[k]);
+    if (bm) atomicMax(stats + 1, bm);
+    block_sums[blockIdx.x] = tot;
+  }
 }
 
 // Single-block exclusive scan of the per-block patch counts; writes the
