@@ -121,7 +121,7 @@ int launch_palette_l1(int K, int H, int W, const float* layer, const float* pale
 // raw coordinates' dependence on A_i, and the softmax term, which is exactly
 // zero unless two tetrahedra's errors tie to within ~1e-7).
 constexpr float kBaryTau = 1e-9f, kBaryEps = 1e-12f;
-constexpr int kGeoThreads = 128;  // ~140 registers per thread: 3 blocks per SM
+constexpr int kGeoThreads = 128;
 
 template <int KC>
 struct TetraConst {
@@ -139,12 +139,10 @@ __device__ __forceinline__ float softplus_grad(float x) {
   return x > 20.f ? 1.f : 1.f / (1.f + expf(-x));
 }
 
-// Forward of one tetrahedron: coords x[4] = (alpha, beta, gamma, delta),
-// softplus values, normaliser, projection and reconstruction error.
+// Barycentric coordinates x[4] = (alpha, beta, gamma, delta) of colour C in
+// one tetrahedron.
 template <int KC>
-__device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const float* Pi,
-                                               const float* Pj, const float* C, float* x, float* sp,
-                                               float& den, float* pr, float* rec) {
+__device__ __forceinline__ void tetra_coords(const TetraConst<KC>& T, const float* C, float* x) {
   float co[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
@@ -153,6 +151,15 @@ __device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const fl
   x[2] = co[1];
   x[3] = co[2];
   x[0] = 1.f - co[0] - co[1] - co[2];
+}
+
+// Forward of one tetrahedron: coords x[4], softplus values, normaliser,
+// projection and reconstruction error.
+template <int KC>
+__device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const float* Pi,
+                                               const float* Pj, const float* C, float* x, float* sp,
+                                               float& den, float* pr, float* rec) {
+  tetra_coords<KC>(T, C, x);
   den = kBaryEps;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -172,6 +179,130 @@ __device__ __forceinline__ float tetra_forward(const TetraConst<KC>& T, const fl
   return err;
 }
 
+// Softmax weights of the tetrahedra at temperature kBaryTau (shifted by the
+// smallest error) and their coordinates, as the reference computes them.
+template <int KC>
+__device__ __forceinline__ void bary_weights(const TetraConst<KC>* s_t, const float (*s_p)[3],
+                                             const float* C, float* prob, float (*xs)[4]) {
+  float err[KC];
+#pragma unroll
+  for (int i = 0; i < KC; ++i) {
+    float sp[4], den, pr[4], rec[3];
+    err[i] = tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, xs[i], sp, den, pr, rec);
+  }
+  float emin = INFINITY;
+#pragma unroll
+  for (int i = 0; i < KC; ++i) emin = fminf(emin, err[i]);
+  float psum = 0.f;
+#pragma unroll
+  for (int i = 0; i < KC; ++i) {
+    prob[i] = expf((emin - err[i]) * (1.f / kBaryTau));
+    psum += prob[i];
+  }
+  const float rpsum = 1.f / psum;
+#pragma unroll
+  for (int i = 0; i < KC; ++i) prob[i] *= rpsum;
+}
+
+// Pixels whose softmax is not one-hot (tetrahedra tied to within ~1e-7 in
+// reconstruction error, or non-finite errors) take these two out-of-line
+// functions, which keep every tetrahedron's terms; their registers do not
+// weigh on the one-hot path.  Data passes through the thread's slots of a
+// shared-memory scratch `scr` (stride kGeoThreads).
+// Target weights W = sum_i prob_i raw_i -> scr[k].
+template <int KC>
+__device__ __noinline__ void bary_target_general(const TetraConst<KC>* s_t,
+                                                 const float (*s_p)[3], float c0, float c1,
+                                                 float c2, float* scr) {
+  constexpr int K = KC + 2;
+  const float C[3] = {c0, c1, c2};
+  float prob[KC], xs[KC][4];
+  bary_weights<KC>(s_t, s_p, C, prob, xs);
+  float Wb[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) Wb[k] = 0.f;
+#pragma unroll
+  for (int i = 0; i < KC; ++i) {
+    Wb[0] += prob[i] * xs[i][0];
+    Wb[1] += prob[i] * xs[i][1];
+    Wb[i + 2] += prob[i] * xs[i][2];
+    Wb[(i + 1) % KC + 2] += prob[i] * xs[i][3];
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) scr[k * kGeoThreads] = Wb[k];
+}
+
+// Palette gradient of the target given gWb = dL/dW (scr[k]): the raw
+// coordinates' path and the softmax path (the reconstruction error's adjoint
+// for tetrahedra with a non-zero error gradient).  Writes the 3 KC values
+// d/d chroma[i][c] -> scr[3 i + c].
+template <int KC>
+__device__ __noinline__ void bary_adjoint_general(const TetraConst<KC>* s_t,
+                                                  const float (*s_p)[3], float c0, float c1,
+                                                  float c2, float* scr) {
+  constexpr int K = KC + 2;
+  const float C[3] = {c0, c1, c2};
+  float prob[KC], xs[KC][4], gWb[K], dP[KC][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k) gWb[k] = scr[k * kGeoThreads];
+#pragma unroll
+  for (int i = 0; i < KC; ++i) dP[i][0] = dP[i][1] = dP[i][2] = 0.f;
+  bary_weights<KC>(s_t, s_p, C, prob, xs);
+  float gprob[KC], gdot = 0.f;
+#pragma unroll
+  for (int i = 0; i < KC; ++i) {
+    const float* x = xs[i];
+    gprob[i] = x[0] * gWb[0] + x[1] * gWb[1] + x[2] * gWb[i + 2] + x[3] * gWb[(i + 1) % KC + 2];
+    gdot += prob[i] * gprob[i];
+  }
+#pragma unroll
+  for (int i = 0; i < KC; ++i) {
+    const float gerr = -prob[i] * (gprob[i] - gdot) * (1.f / kBaryTau);
+    if (prob[i] == 0.f && gerr == 0.f) continue;  // contributes nothing
+    const TetraConst<KC>& T = s_t[i];
+    const int ti = i, tj = (i + 1) % KC;
+    const float* Pi = s_p[ti];
+    const float* Pj = s_p[tj];
+    const float* x = xs[i];
+    float gx[4] = {prob[i] * gWb[0], prob[i] * gWb[1], prob[i] * gWb[ti + 2],
+                   prob[i] * gWb[tj + 2]};
+    if (gerr != 0.f) {  // error path: err = |rec - C|^2
+      float xr[4], sp[4], den, pr[4], rec[3];
+      tetra_forward<KC>(T, Pi, Pj, C, xr, sp, den, pr, rec);
+      float grec[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) grec[c] = 2.f * (rec[c] - C[c]) * gerr;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dP[ti][c] += grec[c] * pr[2];
+        dP[tj][c] += grec[c] * pr[3];
+      }
+      const float gpr[4] = {0.f, grec[0] + grec[1] + grec[2],
+                            grec[0] * Pi[0] + grec[1] * Pi[1] + grec[2] * Pi[2],
+                            grec[0] * Pj[0] + grec[1] * Pj[1] + grec[2] * Pj[2]};
+      const float gps = (gpr[0] * sp[0] + gpr[1] * sp[1] + gpr[2] * sp[2] + gpr[3] * sp[3]) /
+                        (den * den);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gx[k] += (gpr[k] / den - gps) * softplus_grad(xr[k]);
+    }
+    // coords (beta, gamma, delta) = A^-1 C; alpha = 1 - sum
+    const float gco[3] = {gx[1] - gx[0], gx[2] - gx[0], gx[3] - gx[0]};
+    float v[3];  // A^-T gco
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      v[c] = T.ainv[c] * gco[0] + T.ainv[3 + c] * gco[1] + T.ainv[6 + c] * gco[2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      dP[ti][c] -= v[c] * x[2];
+      dP[tj][c] -= v[c] * x[3];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KC; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) scr[(3 * i + c) * kGeoThreads] = dP[i][c];
+}
+
 template <int KC>
 __global__ void __launch_bounds__(kGeoThreads)
     k_palette_geo_loss(int64_t hw, const float* __restrict__ layer,
@@ -184,6 +315,7 @@ __global__ void __launch_bounds__(kGeoThreads)
   __shared__ TetraConst<KC> s_t[KC];
   __shared__ float s_p[KC][3];
   __shared__ float red[kGeoThreads / 32][3 * KC + 2];
+  __shared__ float s_scr[3 * KC > KC + 2 ? 3 * KC : KC + 2][kGeoThreads];  // general-path data
   if (threadIdx.x < 3 * KC) s_p[threadIdx.x / 3][threadIdx.x % 3] = chroma[threadIdx.x];
   __syncthreads();
   if (threadIdx.x < KC) {
@@ -238,33 +370,45 @@ __global__ void __launch_bounds__(kGeoThreads)
 #pragma unroll
     for (int k = 0; k < K; ++k) Lp[k] = Ln[k];
     fetch(p + stride);
-    float err[KC], xs[KC][4];  // per tetrahedron: error and coordinates
-#pragma unroll
-    for (int i = 0; i < KC; ++i) {
-      float sp[4], den, pr[4], rec[3];
-      err[i] = tetra_forward<KC>(s_t[i], s_p[i], s_p[(i + 1) % KC], C, xs[i], sp, den, pr, rec);
+    // Reconstruction errors; the softmax over -err / 1e-9 is one-hot unless
+    // two errors agree to ~1e-7: then the winner's weight is exp(0) = 1, the
+    // others underflow to 0, and the target and its palette gradient involve
+    // the winner's coordinates alone (with exactly the values the general
+    // expressions give).
+    float* scr = &s_scr[0][threadIdx.x];
+    float err[KC];
+#pragma unroll 1
+    for (int i = 0; i < KC; ++i) {  // one tetrahedron at a time (register pressure)
+      float x[4], sp[4], den, pr[4], rec[3];
+      scr[i * kGeoThreads] =
+          tetra_forward<KC>(s_t[i], s_p[i], s_p[i + 1 == KC ? 0 : i + 1], C, x, sp, den, pr, rec);
     }
-    // softmax over the tetrahedra of -err / tau (shifted by the maximum)
+#pragma unroll
+    for (int i = 0; i < KC; ++i) err[i] = scr[i * kGeoThreads];
     float emin = INFINITY;
 #pragma unroll
     for (int i = 0; i < KC; ++i) emin = fminf(emin, err[i]);
-    float prob[KC], psum = 0.f;
+    int nz = 0, win = 0;
 #pragma unroll
     for (int i = 0; i < KC; ++i) {
-      prob[i] = expf((emin - err[i]) * (1.f / kBaryTau));
-      psum += prob[i];
+      if (expf((emin - err[i]) * (1.f / kBaryTau)) != 0.f) {
+        ++nz;
+        win = i;
+      }
     }
-    const float rpsum = 1.f / psum;
-    float Wb[K];
+    const bool onehot = nz == 1;
+    const int wj = win + 1 == KC ? 0 : win + 1;
+    float Wb[K], xw[4];
+    if (onehot) {
+      tetra_coords<KC>(s_t[win], C, xw);
+      Wb[0] = xw[0];
+      Wb[1] = xw[1];
 #pragma unroll
-    for (int k = 0; k < K; ++k) Wb[k] = 0.f;
+      for (int k = 2; k < K; ++k) Wb[k] = k - 2 == win ? xw[2] : k - 2 == wj ? xw[3] : 0.f;
+    } else {
+      bary_target_general<KC>(s_t, s_p, C[0], C[1], C[2], scr);
 #pragma unroll
-    for (int i = 0; i < KC; ++i) {
-      prob[i] *= rpsum;
-      Wb[0] += prob[i] * xs[i][0];
-      Wb[1] += prob[i] * xs[i][1];
-      Wb[i + 2] += prob[i] * xs[i][2];
-      Wb[(i + 1) % KC + 2] += prob[i] * xs[i][3];
+      for (int k = 0; k < K; ++k) Wb[k] = scr[k * kGeoThreads];
     }
     float Wc[K], m[K], s_raw = 0.f, s = 1.f;
     if (clamp) {
@@ -316,55 +460,36 @@ __global__ void __launch_bounds__(kGeoThreads)
 #pragma unroll
       for (int k = 0; k < K; ++k) gWb[k] = gW[k];
     }
-    // W = sum_i prob_i raw_i: raw path and softmax path
-    float gprob[KC], gdot = 0.f;
+    if (onehot) {
+      // the winner's raw-coordinate path: coords (beta, gamma, delta) = A^-1 C,
+      // alpha = 1 - sum; d/d c_i through A^-1 (the error path carries 0)
+      float g2 = 0.f, g3 = 0.f;
 #pragma unroll
-    for (int i = 0; i < KC; ++i) {
-      const float* x = xs[i];
-      gprob[i] = x[0] * gWb[0] + x[1] * gWb[1] + x[2] * gWb[i + 2] + x[3] * gWb[(i + 1) % KC + 2];
-      gdot += prob[i] * gprob[i];
-    }
-#pragma unroll
-    for (int i = 0; i < KC; ++i) {
-      const float gerr = -prob[i] * (gprob[i] - gdot) * (1.f / kBaryTau);
-      if (prob[i] == 0.f && gerr == 0.f) continue;  // contributes nothing
-      const TetraConst<KC>& T = s_t[i];
-      const int ti = i, tj = (i + 1) % KC;
-      const float* Pi = s_p[ti];
-      const float* Pj = s_p[tj];
-      const float* x = xs[i];
-      float gx[4] = {prob[i] * gWb[0], prob[i] * gWb[1], prob[i] * gWb[ti + 2],
-                     prob[i] * gWb[tj + 2]};
-      if (gerr != 0.f) {  // error path (near-ties only): err = |rec - C|^2
-        float xr[4], sp[4], den, pr[4], rec[3];
-        tetra_forward<KC>(T, Pi, Pj, C, xr, sp, den, pr, rec);
-        float grec[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) grec[c] = 2.f * (rec[c] - C[c]) * gerr;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          dP[ti][c] += grec[c] * pr[2];
-          dP[tj][c] += grec[c] * pr[3];
-        }
-        const float gpr[4] = {0.f, grec[0] + grec[1] + grec[2],
-                              grec[0] * Pi[0] + grec[1] * Pi[1] + grec[2] * Pi[2],
-                              grec[0] * Pj[0] + grec[1] * Pj[1] + grec[2] * Pj[2]};
-        const float gps = (gpr[0] * sp[0] + gpr[1] * sp[1] + gpr[2] * sp[2] + gpr[3] * sp[3]) /
-                          (den * den);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) gx[k] += (gpr[k] / den - gps) * softplus_grad(xr[k]);
+      for (int k = 2; k < K; ++k) {
+        if (k - 2 == win) g2 = gWb[k];
+        if (k - 2 == wj) g3 = gWb[k];
       }
-      // coords (beta, gamma, delta) = A^-1 C; alpha = 1 - sum
-      const float gco[3] = {gx[1] - gx[0], gx[2] - gx[0], gx[3] - gx[0]};
+      const float gco[3] = {gWb[1] - gWb[0], g2 - gWb[0], g3 - gWb[0]};
+      const TetraConst<KC>& T = s_t[win];
       float v[3];  // A^-T gco
 #pragma unroll
       for (int c = 0; c < 3; ++c)
         v[c] = T.ainv[c] * gco[0] + T.ainv[3 + c] * gco[1] + T.ainv[6 + c] * gco[2];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        dP[ti][c] -= v[c] * x[2];
-        dP[tj][c] -= v[c] * x[3];
-      }
+      for (int i = 0; i < KC; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (i == win) dP[i][c] -= v[c] * xw[2];
+          if (i == wj) dP[i][c] -= v[c] * xw[3];
+        }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) scr[k * kGeoThreads] = gWb[k];
+      bary_adjoint_general<KC>(s_t, s_p, C[0], C[1], C[2], scr);
+#pragma unroll
+      for (int i = 0; i < KC; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dP[i][c] += scr[(3 * i + c) * kGeoThreads];
     }
   }
   // block reduction: dchroma (3 KC values), geo and pos loss sums

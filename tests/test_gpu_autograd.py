@@ -111,3 +111,35 @@ def test_palette_geo_loss_matches_oracle(cuda_ok, clamp, kind):
     assert same.mean() > 0.999  # pixels on a tetrahedron boundary may pick the other one
     assert rel_err(L.grad, ref["dlayer"]) < 1e-4
     assert rel_err(P.grad, ref["dchroma"]) < 1e-3
+
+
+@pytest.mark.parametrize("clamp,kind", [(True, "l1"), (False, "mse")])
+def test_palette_geo_loss_tied_tetrahedra(cuda_ok, clamp, kind):
+    """With two chroma colours the two tetrahedra (black, white, c0, c1) and
+    (black, white, c1, c0) are the same solid, so every pixel's errors tie and
+    the kernel takes its general (non-one-hot) path everywhere; achromatic and
+    white pixels are mixed in.  The target is the same whatever the softmax
+    weights, so loss, target weights and dL/dlayer match the FP64 oracle.
+    (dL/dpalette is not compared: on exact ties the softmax term divides
+    FP32 rounding differences by the 1e-9 temperature.)"""
+    from oracle import oracle as orc
+    from palette_b200.loss import barycentric_target, palette_geo_loss
+    g = torch.Generator().manual_seed(4)
+    H, W = 64, 96
+    chroma = torch.rand((2, 3), generator=g) * 0.8 + 0.1
+    target = torch.rand((3, H, W), generator=g)
+    grey = torch.rand((H, W), generator=g) < 0.3
+    target[:, grey] = target[0, grey]
+    target[:, :3, :] = 1.0
+    layer = torch.randn((4, H, W), generator=g) * 0.3 + 0.2
+    ref = orc.palette_geo_loss(layer.double().numpy(), target.double().numpy(),
+                               chroma.double().numpy(), clamp=clamp, kind=kind)
+    L = layer.cuda().requires_grad_(True)
+    P = chroma.cuda().requires_grad_(True)
+    loss = palette_geo_loss(L, P, target.cuda(), clamp=clamp, lambda_pos=0.5, kind=kind)
+    loss.backward()
+    assert abs(float(loss) - ref["loss"]) < 1e-5 * max(1.0, abs(ref["loss"]))
+    wb = barycentric_target(target.cuda(), chroma.cuda(), clamp=clamp)
+    assert np.abs(np_of(wb) - ref["target_weights"]).max() < 1e-4
+    assert rel_err(L.grad, ref["dlayer"]) < 1e-4
+    assert bool(torch.isfinite(P.grad).all())
