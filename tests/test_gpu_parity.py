@@ -389,3 +389,32 @@ def test_backward_reuses_forward_records_only_when_inputs_unchanged(cuda_ok):
                               *out[1:], g)
     assert rel_err(dW[:, 0], np_of(dW2[:, 0]).astype(np.float64)) < 1e-6
     assert rel_err(dW[:, 0], np_of(fresh[:, 0]).astype(np.float64)) > 0.05
+
+
+@pytest.mark.parametrize("K", [1, 2, 4, 6, 7, 8])
+def test_splat_weight_channel_counts(cuda_ok, K):
+    """Compositing and its weights adjoint for every channel count the
+    kernels are built for other than the 5 of the benchmark and the 3 of the
+    colour path (records take two overlapping Gaussians per step, and the
+    adjoint sums their K-vectors in one half-warp transposition padded to a
+    power of two): image, contributor indices and weight gradients against
+    the oracle."""
+    n, W, H, eye = CASES[2]
+    sc, st = _scene(n, seed=40 + K)
+    cam = _cam(W, H, eye)
+    pre = _gpu_pre(st, cam)
+    w = torch.rand((n, K), device="cuda", generator=torch.Generator("cuda").manual_seed(K)) - 0.3
+    ref = _oracle_splat(H, W, K, {k: v.clone() for k, v in pre.items()}, st["alphas"], w, 0.0)
+    layer, contrib, ft, ranges, gsid = gsc.splat_weight(H, W, K, pre["us"], pre["cinv"], st["alphas"],
+                                                        pre["depths"], w, pre["areas"])
+    assert np.array_equal(np_of(gsid), ref["b"]["gsid"])
+    same = np_of(contrib) == ref["contrib"]
+    assert same.mean() > 1 - 1e-4
+    assert max_abs(np_of(layer)[:, same], ref["out"][:, same]) < IMG_TOL
+    g = torch.randn((K, H, W), device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+    dW, = gsc.splat_weight_B(H, W, K, pre["us"], pre["cinv"], st["alphas"], pre["depths"], w,
+                             contrib, ft, ranges, gsid, g)
+    r = orc.draw_backward(H, W, K, np_of(ranges), np_of(gsid), np_of(pre["us"]), np_of(pre["cinv"]),
+                          np_of(st["alphas"]), np_of(w), np_of(ft), np_of(contrib), np_of(g))
+    assert dW.shape == (n, 1, K)
+    assert rel_err(dW[:, 0], r["dfeat"]) < GRAD_REL
