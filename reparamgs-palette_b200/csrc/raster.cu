@@ -255,7 +255,7 @@ __device__ __forceinline__ float warp_transpose_sum(float (&x)[NV], int lane, in
 #pragma unroll
   for (int o = off; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   *idx = id;
-  *owner = (lane & (2 * off - 1)) == 0;
+  *owner = off == 0 || (lane & (2 * off - 1)) == 0;  // NV == group size: every lane
   return v;
 }
 
@@ -395,6 +395,85 @@ __device__ __forceinline__ void adjoint_weights_pair(BwdPixel<K> (&p)[2], int ba
   }
 }
 
+// Destination of gradient value `v` of Gaussian g: x[0..K) features, then
+// alpha, u (2), conic (3).
+template <int K>
+__device__ __forceinline__ float* grad_slot(int v, int64_t g, float* dfeat, float* dalpha,
+                                            float* du, float* dconic) {
+  if (v < K) return dfeat + g * K + v;
+  if (v == K) return dalpha + g;
+  if (v < K + 3) return du + 2 * g + (v - K - 1);
+  return dconic + 3 * g + (v - K - 3);
+}
+
+// Full adjoint (GEOM) of two contributors at once, slot ja behind slot jb:
+// the per-pixel terms are adjoint_pixel's, in the same order (ja then jb for
+// each pixel).  The two gradient vectors (K + 6 values each) are summed
+// together: one exchange at lane offset 16 leaves ja's partial sums on lanes
+// 0-15 and jb's on lanes 16-31, then each half-warp transposes its values
+// (K + 6 + 15 shuffles for the pair instead of 2 x 16 for K = 3..8).
+template <int K, bool DTAU>
+__device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base, int ja, int jb,
+                                                  const float4* srec, const int32_t* sgid,
+                                                  float fx, float fy0, float fy1, int lane,
+                                                  float* __restrict__ dfeat,
+                                                  float* __restrict__ dalpha,
+                                                  float* __restrict__ du,
+                                                  float* __restrict__ dconic) {
+  constexpr int NREAL = K + 6;
+  constexpr int NV = Pow2<NREAL>::value;
+  static_assert(NV <= 16, "half-warp transposition holds at most 16 values");
+  const float4 a0 = srec[ja], a1 = srec[kBatch + ja];
+  const float4 b0 = srec[jb], b1 = srec[kBatch + jb];
+  float xa[NV], xb[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) xa[v] = xb[v] = 0.f;
+  const float dxa = a0.x - fx, dya0 = a0.y - fy0, dya1 = a0.y - fy1;
+  const float dxb = b0.x - fx, dyb0 = b0.y - fy0, dyb1 = b0.y - fy1;
+  const float ma0 = fmaxf(0.f, maha_sq(a0.z, a0.w, a1.x, dxa, dya0));
+  const float ma1 = fmaxf(0.f, maha_sq(a0.z, a0.w, a1.x, dxa, dya1));
+  const float mb0 = fmaxf(0.f, maha_sq(b0.z, b0.w, b1.x, dxb, dyb0));
+  const float mb1 = fmaxf(0.f, maha_sq(b0.z, b0.w, b1.x, dxb, dyb1));
+  bool ha = adjoint_pixel<K, true, DTAU>(p[0], base + ja, ma0, a0, a1, dxa, dya0, srec, ja, xa);
+  bool hb = adjoint_pixel<K, true, DTAU>(p[0], base + jb, mb0, b0, b1, dxb, dyb0, srec, jb, xb);
+  ha |= adjoint_pixel<K, true, DTAU>(p[1], base + ja, ma1, a0, a1, dxa, dya1, srec, ja, xa);
+  hb |= adjoint_pixel<K, true, DTAU>(p[1], base + jb, mb1, b0, b1, dxb, dyb1, srec, jb, xb);
+  const unsigned ca = __ballot_sync(0xffffffffu, ha), cb = __ballot_sync(0xffffffffu, hb);
+  if (!(ca | cb)) return;
+  if (__popc(ca) <= 1 && __popc(cb) <= 1) {
+    if (ha) {
+      const int64_t g = sgid[ja];
+#pragma unroll
+      for (int v = 0; v < NREAL; ++v) atomicAdd(grad_slot<K>(v, g, dfeat, dalpha, du, dconic), xa[v]);
+    }
+    if (hb) {
+      const int64_t g = sgid[jb];
+#pragma unroll
+      for (int v = 0; v < NREAL; ++v) atomicAdd(grad_slot<K>(v, g, dfeat, dalpha, du, dconic), xb[v]);
+    }
+    return;
+  }
+  const bool hi = (lane & 16) != 0;
+  float y[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    if (v < NREAL) {
+      const float send = hi ? xa[v] : xb[v];
+      const float keep = hi ? xb[v] : xa[v];
+      y[v] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    } else {
+      y[v] = 0.f;
+    }
+  }
+  int vidx;
+  bool owner;
+  const float tot = warp_transpose_sum<NV, 8>(y, lane, &vidx, &owner);
+  if (owner && vidx < NREAL && (hi ? cb : ca) != 0u) {
+    const int64_t g = sgid[hi ? jb : ja];
+    atomicAdd(grad_slot<K>(vidx, g, dfeat, dalpha, du, dconic), tot);
+  }
+}
+
 // Walks each pixel's contributors back to front from its `contrib` index,
 // recovering T by division by (1 - alpha') from the saved final T.  The
 // per-pixel skip decisions use the forward's exact expressions, so the walk
@@ -469,11 +548,15 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
       while (mask) {
         const int msb = 31 - __clz(mask);
         mask &= ~(1u << msb);
-        if (!GEOM && mask) {
+        if (mask) {
           const int msb2 = 31 - __clz(mask);
           mask &= ~(1u << msb2);
-          adjoint_weights_pair<K>(p, base, s_lo + msb, s_lo + msb2, srec, sgid, fx, fy0, fy1,
-                                  lane, dfeat);
+          if constexpr (GEOM)
+            adjoint_geom_pair<K, DTAU>(p, base, s_lo + msb, s_lo + msb2, srec, sgid, fx, fy0, fy1,
+                                       lane, dfeat, dalpha, du, dconic);
+          else
+            adjoint_weights_pair<K>(p, base, s_lo + msb, s_lo + msb2, srec, sgid, fx, fy0, fy1,
+                                    lane, dfeat);
           continue;
         }
         const int jj = s_lo + msb;
