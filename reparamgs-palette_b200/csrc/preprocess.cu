@@ -161,14 +161,59 @@ __global__ void __launch_bounds__(kThreads)
 // sh2Weight / sh2Color -- gsplatcu/kernel.cu:670-870, 1040-1169.  Both are the
 // same map feat_k = sum_l Y_l(dir) c[l*K + k] (band-major); colours are K = 3.
 // All Gaussians are evaluated (no depth test), as in the reference.
+// A Gaussian's coefficient row is nb*K values (up to 128); read one row per
+// thread straight from global memory, a warp's loads would be strided by the
+// row length and thrash L1.  The block's rows, one contiguous span, are
+// therefore copied first (coalesced, kShCopy loads in flight per thread) into
+// shared memory at an odd row stride, where each thread reads its own row
+// without bank conflicts.
+constexpr int kShThreads = 64;  // 64 rows of at most 129 floats: 33 KB of shared memory
+constexpr int kShCopy = 8;
+
 template <int K, typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kShThreads)
     k_sh2feat(int64_t n, const T* __restrict__ shs, int nb, const float* __restrict__ pws,
               const float* __restrict__ twc, float* __restrict__ feat, float* __restrict__ dshs,
               float* __restrict__ dpws) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ float srows[];
+  const int rl = nb * K, stride = rl | 1;
+  const int64_t row0 = (int64_t)blockIdx.x * kShThreads;
+  const int rows = (int)min((int64_t)kShThreads, n - row0);
+  // BF16 rows (half the bytes) are read in place: their 2-byte element copies
+  // would cost more than the strided reads they replace (measured)
+  constexpr bool kStage = sizeof(T) == 4;
+  if constexpr (kStage) {
+    const T* src = shs + row0 * rl;
+    const int total = rows * rl;
+    // (row, column) of element e, advanced by kShThreads elements per step
+    int r = threadIdx.x / rl, q = threadIdx.x - r * rl;
+    const int dr = kShThreads / rl, dq = kShThreads - dr * rl;
+    for (int e0 = threadIdx.x; e0 < total; e0 += kShCopy * kShThreads) {
+      float v[kShCopy];
+      int at[kShCopy];
+#pragma unroll
+      for (int u = 0; u < kShCopy; ++u) {
+        const int e = e0 + u * kShThreads;
+        v[u] = e < total ? ld(src, e) : 0.f;
+        at[u] = r * stride + q;
+        q += dq;
+        r += dr;
+        if (q >= rl) {
+          q -= rl;
+          ++r;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kShCopy; ++u)
+        if (e0 + u * kShThreads < total) srows[at[u]] = v[u];
+    }
+  }
+  __syncthreads();
+  const int64_t i = row0 + threadIdx.x;
   if (i >= n) return;
-  const T* c = shs + i * (int64_t)nb * K;
+  const float* srow = srows + threadIdx.x * stride;
+  const T* grow = shs + i * (int64_t)rl;
+  const auto c = [&](int idx) { return kStage ? srow[idx] : ld(grow, idx); };
   float dir[3] = {0.f, 0.f, 0.f}, nd[3] = {0.f, 0.f, 0.f}, ninv = 0.f;
   float Y[16];
   if (nb > 1) {
@@ -178,7 +223,7 @@ __global__ void __launch_bounds__(kThreads)
   }
   sh_basis(dir, nb, Y);
   float acc[K];
-  sh_weights_full<K>([&](int idx) { return ld(c, idx); }, nb, Y, acc);
+  sh_weights_full<K>(c, nb, Y, acc);
 #pragma unroll
   for (int k = 0; k < K; ++k) feat[i * K + k] = acc[k];
   if (dshs) {
@@ -190,7 +235,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int k = 0; k < K; ++k) {
       float dd[3] = {0.f, 0.f, 0.f};
       for (int l = 1; l < nb; ++l) {
-        const float cv = ld(c, l * K + k);
+        const float cv = c(l * K + k);
         dd[0] += G[3 * l] * cv;
         dd[1] += G[3 * l + 1] * cv;
         dd[2] += G[3 * l + 2] * cv;
@@ -240,10 +285,13 @@ template <typename T>
 static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws, const float* twc,
                      float* feat, float* dshs, float* dpws, cudaStream_t st) {
   const T* s = (const T*)shs;
-  const int g = grid_for(n);
+  const int g = div_up(n > 0 ? n : 1, kShThreads);
+  const size_t smem = sizeof(T) == 4 ? (size_t)kShThreads * ((nb * K) | 1) * sizeof(float) : 0;
   switch (K) {
-#define GSB_K(KK) \
-  case KK: k_sh2feat<KK, T><<<g, kThreads, 0, st>>>(n, s, nb, pws, twc, feat, dshs, dpws); break;
+#define GSB_K(KK)                                                                            \
+  case KK:                                                                                   \
+    k_sh2feat<KK, T><<<g, kShThreads, smem, st>>>(n, s, nb, pws, twc, feat, dshs, dpws);    \
+    break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K
     default: return GSB_ERR_INVALID_ARGUMENT;
