@@ -11,7 +11,10 @@
 // within a batch every warp first tests 32 records at a time against its
 // pixel block (one record per lane, ballot) using the record's conservative
 // support box and then its cut ellipse, then walks only the overlapping
-// records in list order.  Per
+// records in list order, two at a time: both records' opacity terms are
+// evaluated before the two blends (or, in the adjoint, the two transmittance
+// recoveries) so that their exp() chains overlap, and the adjoint sums the
+// two records' gradient vectors in one warp reduction.  Per
 // pixel, a record whose Mahalanobis distance exceeds its cut is skipped
 // without evaluating exp() -- the reference would skip it too
 // (alpha' < 0.002) -- and every other record is evaluated with the
