@@ -179,33 +179,47 @@ __global__ void __launch_bounds__(kShThreads)
   const int rl = nb * K, stride = rl | 1;
   const int64_t row0 = (int64_t)blockIdx.x * kShThreads;
   const int rows = (int)min((int64_t)kShThreads, n - row0);
-  // BF16 rows (half the bytes) are read in place: their 2-byte element copies
-  // would cost more than the strided reads they replace (measured)
-  constexpr bool kStage = sizeof(T) == 4;
-  if constexpr (kStage) {
-    const T* src = shs + row0 * rl;
-    const int total = rows * rl;
-    // (row, column) of element e, advanced by kShThreads elements per step
-    int r = threadIdx.x / rl, q = threadIdx.x - r * rl;
-    const int dr = kShThreads / rl, dq = kShThreads - dr * rl;
+  // FP32 rows are copied element by element; BF16 rows of even length
+  // (4-byte aligned) as element pairs, one 32-bit load each (2-byte element
+  // loads cost more than the strided reads they replace); other BF16 rows are
+  // read in place.
+  constexpr bool kF32 = sizeof(T) == 4;
+  const bool pairs = !kF32 && (rl & 1) == 0 && (reinterpret_cast<uintptr_t>(shs) & 3) == 0;
+  const bool staged = kF32 || pairs;
+  if (staged) {
+    // G elements per load; (row, column) of load e advanced by kShThreads
+    // loads per step
+    const int G = kF32 ? 1 : 2;
+    const int rlg = rl / G, total = rows * rlg;
+    int r = threadIdx.x / rlg, q = threadIdx.x - r * rlg;
+    const int dr = kShThreads / rlg, dq = kShThreads - dr * rlg;
     for (int e0 = threadIdx.x; e0 < total; e0 += kShCopy * kShThreads) {
-      float v[kShCopy];
+      float2 v[kShCopy];
       int at[kShCopy];
 #pragma unroll
       for (int u = 0; u < kShCopy; ++u) {
         const int e = e0 + u * kShThreads;
-        v[u] = e < total ? ld(src, e) : 0.f;
-        at[u] = r * stride + q;
+        if constexpr (kF32) {
+          v[u].x = e < total ? ld(shs + row0 * rl, e) : 0.f;
+        } else {
+          const __nv_bfloat162* src = reinterpret_cast<const __nv_bfloat162*>(shs + row0 * rl);
+          v[u] = e < total ? __bfloat1622float2(src[e]) : make_float2(0.f, 0.f);
+        }
+        at[u] = r * stride + q * G;
         q += dq;
         r += dr;
-        if (q >= rl) {
-          q -= rl;
+        if (q >= rlg) {
+          q -= rlg;
           ++r;
         }
       }
 #pragma unroll
-      for (int u = 0; u < kShCopy; ++u)
-        if (e0 + u * kShThreads < total) srows[at[u]] = v[u];
+      for (int u = 0; u < kShCopy; ++u) {
+        if (e0 + u * kShThreads < total) {
+          srows[at[u]] = v[u].x;
+          if constexpr (!kF32) srows[at[u] + 1] = v[u].y;
+        }
+      }
     }
   }
   __syncthreads();
@@ -213,7 +227,7 @@ __global__ void __launch_bounds__(kShThreads)
   if (i >= n) return;
   const float* srow = srows + threadIdx.x * stride;
   const T* grow = shs + i * (int64_t)rl;
-  const auto c = [&](int idx) { return kStage ? srow[idx] : ld(grow, idx); };
+  const auto c = [&](int idx) { return staged ? srow[idx] : ld(grow, idx); };
   float dir[3] = {0.f, 0.f, 0.f}, nd[3] = {0.f, 0.f, 0.f}, ninv = 0.f;
   float Y[16];
   if (nb > 1) {
@@ -286,7 +300,8 @@ static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws
                      float* feat, float* dshs, float* dpws, cudaStream_t st) {
   const T* s = (const T*)shs;
   const int g = div_up(n > 0 ? n : 1, kShThreads);
-  const size_t smem = sizeof(T) == 4 ? (size_t)kShThreads * ((nb * K) | 1) * sizeof(float) : 0;
+  const bool staged = sizeof(T) == 4 || (nb * K) % 2 == 0;  // (as decided in the kernel)
+  const size_t smem = staged ? (size_t)kShThreads * ((nb * K) | 1) * sizeof(float) : 0;
   switch (K) {
 #define GSB_K(KK)                                                                            \
   case KK:                                                                                   \
