@@ -7,7 +7,7 @@ weights-only backward (dL/dlayer random), and the fused preprocess kernel
 alone through the C ABI.  Not collected by pytest; also the command the
 preprocess kernels' ncu summaries are captured from.
 
-    python tests/perf_fused_gpu.py [--mode full|lowrank] [--rank 3] [--dtype f32|bf16]
+    python bench/perf_fused_gpu.py [--mode full|lowrank] [--rank 3] [--dtype f32|bf16]
                                    [--gaussians 1000000] [--width 1920] [--height 1080]
 """
 import argparse

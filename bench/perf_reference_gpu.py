@@ -15,7 +15,7 @@ between one pair of events), where a call's host work overlaps the device
 work of the calls before it.  Not collected by pytest: run it
 on a GPU box and keep the printed JSON.
 
-    python tests/perf_reference_gpu.py [--gaussians 1000000] [--width 1920] [--height 1080]
+    python bench/perf_reference_gpu.py [--gaussians 1000000] [--width 1920] [--height 1080]
 """
 import argparse
 import json

@@ -7,7 +7,7 @@ palette composite and the negative-weight penalty of the finetune loss.  Both
 run on this GPU on the same inputs (K = 5 layer stack at the given size);
 times are CUDA-event medians of forward + backward.  Not collected by pytest.
 
-    python tests/perf_ssim_gpu.py [--width 1920] [--height 1080] [--reps 50]
+    python bench/perf_ssim_gpu.py [--width 1920] [--height 1080] [--reps 50]
 """
 import argparse
 import json

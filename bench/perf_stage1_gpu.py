@@ -10,7 +10,7 @@ over `--rounds` rounds in which the two alternate, after 2 s of GPU load).
 colour path's d/d final T input.  Not collected by pytest: run it on a GPU
 box and keep the printed JSON.
 
-    python tests/perf_stage1_gpu.py [--gaussians 1000000] [--width 1920] [--height 1080]
+    python bench/perf_stage1_gpu.py [--gaussians 1000000] [--width 1920] [--height 1080]
 """
 import argparse
 import json

@@ -17,7 +17,7 @@ rule, with dL/dlayer random on the sampled tiles and zero elsewhere.
 Not collected by pytest (it is a report, minutes of CPU time): run it on a
 GPU box and keep the printed JSON.
 
-    python tests/precision_report.py [--gaussians 3000000] [--poses 32] [--tile-stride 8]
+    python bench/precision_report.py [--gaussians 3000000] [--poses 32] [--tile-stride 8]
 """
 import argparse
 import json

@@ -9,32 +9,46 @@ module name ``gsplatcu_ref`` (so it can be imported beside the drop-in
 ``gsplatcu``), targeting sm_100 SASS exactly as a ``TORCH_CUDA_ARCH_LIST=10.0``
 build of the reference would.  The reference's own ``setup.py`` is not run.
 
-Usage (in the build container, where the reference sources exist)::
+It also stages the reference's unmodified Python caller -- ``gsplat/gsmodel.py``
+and the ``gsplat/utils.py`` it star-imports -- as the package
+``oracle/_ref/gsplat``, so that the drop-in test can run the reference's own
+autograd functions (``WeightGSFunctionTest`` / ``WeightGSFunctionFast``,
+``FinetuneModel``) on either ``gsplatcu`` build.
 
-    python oracle/build_ref.py [--src <reference>/gsplatcu]
+The reference checkout is ``--root``, else ``$GSB_REFERENCE_ROOT``, else the
+build container's copy::
 
-Output: ``oracle/_ref/gsplatcu_ref.so`` and, from the stage-1 sources
-``vanilla_3dgs/gsplatcu``, ``oracle/_ref/vanilla/gsplatcu_vanilla_ref.so``
-(git-ignored; they travel with the tree to the GPU box, where ``load_ref()`` /
-``load_vanilla_ref()`` import them without recompiling).
+    python oracle/build_ref.py [--root <ReparamGS-Palette checkout>]
+
+Output (git-ignored; it travels with the tree to the GPU box, where
+``load_ref()`` / ``load_vanilla_ref()`` / ``reference_caller()`` use it
+without recompiling): ``oracle/_ref/gsplatcu_ref.so``, from the stage-1
+sources ``vanilla_3dgs/gsplatcu`` ``oracle/_ref/vanilla/gsplatcu_vanilla_ref.so``,
+and ``oracle/_ref/gsplat/{gsmodel,utils}.py``.
 """
 import argparse
 import importlib.machinery
 import importlib.util
 import os
+import shutil
 import sys
+import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 REF_SO = os.path.join(REF_DIR, "gsplatcu_ref.so")
-DEFAULT_SRC = "/root/reference/gsplatcu"
-
+CALLER_DIR = os.path.join(REF_DIR, "gsplat")
+CALLER_FILES = ("gsmodel.py", "utils.py")
 
 # The stage-1 (vanilla 3DGS) extension of the same project: its colour splat
 # backward carries the final-transmittance gradient (splat / splatB).
 VANILLA_DIR = os.path.join(REF_DIR, "vanilla")
 VANILLA_SO = os.path.join(VANILLA_DIR, "gsplatcu_vanilla_ref.so")
-DEFAULT_VANILLA_SRC = "/root/reference/vanilla_3dgs/gsplatcu"
+
+
+def reference_root():
+    """Root of the read-only reference checkout (ReparamGS-Palette)."""
+    return os.environ.get("GSB_REFERENCE_ROOT", "/root/reference")
 
 
 def _compile(name, src, out_dir, verbose):
@@ -49,14 +63,29 @@ def _compile(name, src, out_dir, verbose):
          extra_cuda_cflags=["-O3"], verbose=verbose)
 
 
-def build(src=DEFAULT_SRC, verbose=False):
-    _compile("gsplatcu_ref", src, REF_DIR, verbose)
+def build(root=None, verbose=False):
+    _compile("gsplatcu_ref", os.path.join(root or reference_root(), "gsplatcu"), REF_DIR, verbose)
     return REF_SO
 
 
-def build_vanilla(src=DEFAULT_VANILLA_SRC, verbose=False):
-    _compile("gsplatcu_vanilla_ref", src, VANILLA_DIR, verbose)
+def build_vanilla(root=None, verbose=False):
+    _compile("gsplatcu_vanilla_ref", os.path.join(root or reference_root(), "vanilla_3dgs", "gsplatcu"),
+             VANILLA_DIR, verbose)
     return VANILLA_SO
+
+
+def stage_caller(root=None):
+    """Copy the reference's gsplat/gsmodel.py and gsplat/utils.py, byte for
+    byte, into oracle/_ref/gsplat (a namespace package, as in the reference)."""
+    src = os.path.join(root or reference_root(), "gsplat")
+    os.makedirs(CALLER_DIR, exist_ok=True)
+    for f in CALLER_FILES:
+        shutil.copyfile(os.path.join(src, f), os.path.join(CALLER_DIR, f))
+    return CALLER_DIR
+
+
+def caller_staged():
+    return all(os.path.exists(os.path.join(CALLER_DIR, f)) for f in CALLER_FILES)
 
 
 def _load(name, path):
@@ -80,12 +109,55 @@ def load_vanilla_ref():
     return _load("gsplatcu_vanilla_ref", VANILLA_SO)
 
 
+def reference_caller(gsplatcu_module, tag):
+    """The reference's own ``gsplat.gsmodel`` module, executed unchanged with
+    ``import gsplatcu`` resolving to ``gsplatcu_module`` (this build's drop-in
+    or the reference build).  Each call returns a fresh module object named
+    ``gsmodel_<tag>``, so both builds' callers can live in one process.
+    ``gsplat/utils.py`` imports matplotlib for a plotting helper the render
+    path never calls; when matplotlib is absent an empty stand-in is
+    installed.  Returns None when the caller has not been staged."""
+    if not caller_staged():
+        return None
+    if "matplotlib" not in sys.modules:
+        try:
+            import matplotlib  # noqa: F401
+        except ImportError:
+            mpl = types.ModuleType("matplotlib")
+            mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+            sys.modules["matplotlib"], sys.modules["matplotlib.pyplot"] = mpl, mpl.pyplot
+    saved = {k: sys.modules.get(k) for k in ("gsplatcu", "gsplat", "gsplat.utils")}
+    try:
+        sys.modules["gsplatcu"] = gsplatcu_module
+        pkg = types.ModuleType("gsplat")
+        pkg.__path__ = [CALLER_DIR]
+        sys.modules["gsplat"] = pkg
+        sys.modules.pop("gsplat.utils", None)
+        utils_spec = importlib.util.spec_from_file_location(
+            "gsplat.utils", os.path.join(CALLER_DIR, "utils.py"))
+        utils = importlib.util.module_from_spec(utils_spec)
+        sys.modules["gsplat.utils"] = utils
+        utils_spec.loader.exec_module(utils)
+        pkg.utils = utils
+        spec = importlib.util.spec_from_file_location(
+            f"gsmodel_{tag}", os.path.join(CALLER_DIR, "gsmodel.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        return mod
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=DEFAULT_SRC)
-    ap.add_argument("--vanilla-src", default=DEFAULT_VANILLA_SRC)
+    ap.add_argument("--root", default=None, help="reference checkout (default: $GSB_REFERENCE_ROOT)")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
-    print(build(a.src, a.verbose))
-    print(build_vanilla(a.vanilla_src, a.verbose))
+    print(build(a.root, a.verbose))
+    print(build_vanilla(a.root, a.verbose))
+    print(stage_caller(a.root))
     sys.exit(0)

@@ -109,6 +109,31 @@ uint32_t f2u_rz(double v) {
 
 // ================================================================ geometry
 
+// Multiply-add with one rounding in the FP32 instantiation: the reference
+// build's FP32 results follow a fixed pattern of fused multiply-adds (which
+// product of each sum is fused and which is rounded on its own was pinned by
+// reproducing its outputs bit for bit from its inputs); the FP64 oracle
+// evaluates the same expressions unfused (the file is built with
+// -ffp-contract=off, so nothing else is fused).
+inline float fmadd(float a, float b, float c) { return std::fmaf(a, b, c); }
+inline double fmadd(double a, double b, double c) { return a * b + c; }
+
+// a0 b0 + a1 b1 + a2 b2 from zero in index order, each later product fused.
+template <typename R>
+R dot3_fused(R a0, R a1, R a2, R b0, R b1, R b2) {
+  return fmadd(a2, b2, fmadd(a1, b1, a0 * b0));
+}
+
+// Mahalanobis form qa dx^2 + qc dy^2 + 2 qb dx dy (gsplatcu/common.cuh:89-92)
+// in the reference build's FP32 order: the qc term rounded alone, the qa
+// term fused onto it, the cross term fused last.
+template <typename R>
+R maha_form(R qa, R qb, R qc, R dx, R dy) {
+  return fmadd(R(2) * qb * dx, dy, fmadd(qa * dx, dx, qc * dy * dy));
+}
+
+
+
 // gsplatcu/kernel.cu:618-663 (project).  pc = Rcw*pw + tcw; depth = -1 when
 // z < 0.2 (us/pcs are then left untouched); u = f*xy/z + c.
 template <typename R>
@@ -119,7 +144,7 @@ void project(int64_t n, const R* pws, const R* Rcw, const R* tcw, R fx, R fy, R 
       const R* p = pws + 3 * i;
       R pc[3];
       for (int r = 0; r < 3; ++r)
-        pc[r] = Rcw[3 * r] * p[0] + Rcw[3 * r + 1] * p[1] + Rcw[3 * r + 2] * p[2] + tcw[r];
+        pc[r] = dot3_fused(Rcw[3 * r], Rcw[3 * r + 1], Rcw[3 * r + 2], p[0], p[1], p[2]) + tcw[r];
       if (pc[2] < (R)kMinDepth) {
         depths[i] = R(-1);
         continue;
@@ -127,8 +152,8 @@ void project(int64_t n, const R* pws, const R* Rcw, const R* tcw, R fx, R fy, R 
       R zi = R(1) / pc[2];
       R zi2 = zi * zi;
       R xf = pc[0] * fx, yf = pc[1] * fy;
-      us[2 * i] = xf * zi + cx;
-      us[2 * i + 1] = yf * zi + cy;
+      us[2 * i] = fmadd(xf, zi, cx);
+      us[2 * i + 1] = fmadd(yf, zi, cy);
       pcs[3 * i] = pc[0];
       pcs[3 * i + 1] = pc[1];
       pcs[3 * i + 2] = pc[2];
@@ -147,17 +172,16 @@ void project(int64_t n, const R* pws, const R* Rcw, const R* tcw, R fx, R fy, R 
 template <typename R>
 void quat_to_rot(const R* q, R* Rm) {
   R w = q[0], x = q[1], y = q[2], z = q[3];
-  R xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z;
-  R xw = x * w, yw = y * w, zw = z * w;
+  R yy = y * y, zz = z * z, xz = x * z, xw = x * w, zw = z * w;
   Rm[0] = R(1) - R(2) * (yy + zz);
-  Rm[1] = R(2) * (xy - zw);
-  Rm[2] = R(2) * (xz + yw);
-  Rm[3] = R(2) * (xy + zw);
-  Rm[4] = R(1) - R(2) * (xx + zz);
-  Rm[5] = R(2) * (yz - xw);
-  Rm[6] = R(2) * (xz - yw);
-  Rm[7] = R(2) * (yz + xw);
-  Rm[8] = R(1) - R(2) * (xx + yy);
+  Rm[1] = R(2) * fmadd(x, y, -zw);
+  Rm[2] = R(2) * fmadd(y, w, xz);
+  Rm[3] = R(2) * fmadd(x, y, zw);
+  Rm[4] = R(1) - R(2) * fmadd(x, x, zz);
+  Rm[5] = R(2) * fmadd(y, z, -xw);
+  Rm[6] = R(2) * fmadd(-y, w, xz);
+  Rm[7] = R(2) * fmadd(y, z, xw);
+  Rm[8] = R(1) - R(2) * fmadd(x, x, yy);
 }
 
 // d R_ab / d(w,x,y,z) for the map above, as a [9][4] table.
@@ -192,7 +216,8 @@ void cov3d(int64_t n, const R* rots, const R* scales, const R* depths, R* cov3ds
         for (int c = 0; c < 3; ++c) M[3 * a + c] = Rm[3 * a + c] * s[c];
       for (int u = 0; u < 6; ++u) {
         int r = kSym3[u][0], c = kSym3[u][1];
-        cov3ds[6 * i + u] = M[3 * r] * M[3 * c] + M[3 * r + 1] * M[3 * c + 1] + M[3 * r + 2] * M[3 * c + 2];
+        cov3ds[6 * i + u] = dot3_fused(M[3 * r], M[3 * r + 1], M[3 * r + 2], M[3 * c],
+                                       M[3 * c + 1], M[3 * c + 2]);
       }
       if (drot && dscale) {
         R dR[9][4];
@@ -238,15 +263,19 @@ void cov2d(int64_t n, const R* cov3ds, const R* pcs, const R* Rcw, const R* dept
       R M[6];
       for (int r = 0; r < 2; ++r)
         for (int c = 0; c < 3; ++c)
-          M[3 * r + c] = J[3 * r] * Rcw[c] + J[3 * r + 1] * Rcw[3 + c] + J[3 * r + 2] * Rcw[6 + c];
+          M[3 * r + c] = dot3_fused(J[3 * r], J[3 * r + 1], J[3 * r + 2], Rcw[c], Rcw[3 + c],
+                                    Rcw[6 + c]);
       R S[9] = {S6[0], S6[1], S6[2], S6[1], S6[3], S6[4], S6[2], S6[4], S6[5]};
+      // M Sigma: only the last product of entry (0,0) is fused; every other
+      // entry rounds its three products before summing them
       R MS[6];
       for (int r = 0; r < 2; ++r)
         for (int c = 0; c < 3; ++c)
-          MS[3 * r + c] = M[3 * r] * S[c] + M[3 * r + 1] * S[3 + c] + M[3 * r + 2] * S[6 + c];
-      R s00 = MS[0] * M[0] + MS[1] * M[1] + MS[2] * M[2];
-      R s01 = MS[0] * M[3] + MS[1] * M[4] + MS[2] * M[5];
-      R s11 = MS[3] * M[3] + MS[4] * M[4] + MS[5] * M[5];
+          MS[3 * r + c] = (M[3 * r] * S[c] + M[3 * r + 1] * S[3 + c]) + M[3 * r + 2] * S[6 + c];
+      MS[0] = fmadd(M[2], S[6], M[0] * S[0] + M[1] * S[3]);
+      R s00 = dot3_fused(MS[0], MS[1], MS[2], M[0], M[1], M[2]);
+      R s01 = dot3_fused(MS[0], MS[1], MS[2], M[3], M[4], M[5]);
+      R s11 = dot3_fused(MS[3], MS[4], MS[5], M[3], M[4], M[5]);
       cov2ds[3 * i] = s00 + R(0.3);
       cov2ds[3 * i + 1] = s01;
       cov2ds[3 * i + 2] = s11 + R(0.3);
@@ -301,7 +330,7 @@ void inverse_cov2d(int64_t n, const R* cov2ds, R* depths, R* cinv, int32_t* area
     for (int64_t i = b; i < e; ++i) {
       if (depths[i] < (R)kMinDepth) continue;
       R a = cov2ds[3 * i], bb = cov2ds[3 * i + 1], c = cov2ds[3 * i + 2];
-      R det_inv = R(1) / (a * c - bb * bb);
+      R det_inv = R(1) / fmadd(a, c, -(bb * bb));
       if (std::isnan(det_inv)) {
         depths[i] = R(-1);
         continue;
@@ -591,7 +620,7 @@ void draw(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const
             int32_t g = gsid[j];
             R dx = us[2 * g] - (R)px, dy = us[2 * g + 1] - (R)py;
             const R* q = cinv + 3 * g;
-            R maha = std::max(R(0), q[0] * dx * dx + q[2] * dy * dy + R(2) * q[1] * dx * dy);
+            R maha = std::max(R(0), maha_form(q[0], q[1], q[2], dx, dy));
             R ap = std::min((R)kAlphaMax, alphas[g] * std::exp(R(-0.5) * maha));
             if (ap < (R)kAlphaMin) continue;
             R ta = T * ap;
@@ -656,7 +685,7 @@ void draw_backward(int H, int W, int K, const int32_t* ranges, const int32_t* gs
             int32_t g = gsid[j];
             R dx = us[2 * g] - (R)px, dy = us[2 * g + 1] - (R)py;
             const R* q = cinv + 3 * g;
-            R maha = std::max(R(0), q[0] * dx * dx + q[2] * dy * dy + R(2) * q[1] * dx * dy);
+            R maha = std::max(R(0), maha_form(q[0], q[1], q[2], dx, dy));
             R gg = std::exp(R(-0.5) * maha);
             R ap = std::min((R)kAlphaMax, alphas[g] * gg);
             if (ap < (R)kAlphaMin) continue;

@@ -51,19 +51,24 @@ __device__ __forceinline__ float ld(const __nv_bfloat16* p, int64_t i) {
   return __bfloat162float(p[i]);
 }
 
-// Reference Mahalanobis form (gsplatcu/common.cuh:89-92).  The operand order
-// is kept as written there so that the FP32 result, after the compiler's FMA
-// contraction, is the same value the reference computes: the per-pixel skip
-// (alpha' < 0.002) and stop (T < 1e-4) decisions then agree with it exactly.
+// Reference Mahalanobis form qa dx^2 + qc dy^2 + 2 qb dx dy
+// (gsplatcu/common.cuh:89-92), written with explicit round-to-nearest
+// intrinsics in the order the reference build's FP32 results follow: the
+// qc term rounded on its own, the qa term fused onto it, the cross term
+// fused last (pinned by reproducing the reference build's contributor
+// indices and final transmittance bit for bit at 1M Gaussians / 1080p).
+// The intrinsics are never re-contracted, so the forward and the adjoint
+// (separate kernels) take the same skip (alpha' < 0.002) and stop
+// (T < 1e-4) decisions as the reference and as each other.
 __device__ __forceinline__ float maha_sq(float qa, float qb, float qc, float dx, float dy) {
-  return qa * dx * dx + qc * dy * dy + 2 * qb * dx * dy;
+  const float cross = __fmul_rn(__fmul_rn(2.f, qb), dx);
+  return __fmaf_rn(cross, dy, __fmaf_rn(__fmul_rn(qa, dx), dx, __fmul_rn(__fmul_rn(qc, dy), dy)));
 }
 
-// Packed per-Gaussian record read by the compositing kernels.  Vector 0 holds
-// the conservative screen-space support box (pixels outside it give
-// alpha' < 0.002), vector 1 the centre and conic, vector 2 the skip cut,
-// opacity and the first feature, then the remaining features.
-//   v0: xmin xmax ymin ymax | v1: ux uy qa qb | v2: qc cut alpha f0 | v3..: f1..
+// Packed per-Gaussian record read by the compositing kernels (layout in
+// gsb_record.cuh): float4 v0 = centre and conic a, b; v1 = conic c, skip
+// cut, opacity, channel 0; v2 = support half-extents and the conic
+// diagonal's reciprocals; v3.. = channels 1..K-1, zero padded.
 template <int K>
 struct RecordLayout {
   static constexpr int kFloats = ((11 + K) + 3) / 4 * 4;

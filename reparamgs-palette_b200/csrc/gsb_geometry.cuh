@@ -1,30 +1,40 @@
 // Per-Gaussian geometry and spherical-harmonic evaluation (device functions).
 //
-// The FP32 operation order of every value the rasterizer consumes (projected
-// centre, depth, 3D/2D covariance, conic, 3-sigma extents) is kept as the
-// reference computes it (gsplatcu/kernel.cu:379-663), including small matrix
-// products accumulated from zero in (row, column, inner) order.  Compiled with
-// the same FMA contraction rules, the results are then bit-identical, so tile
-// rectangles, sort keys and the per-pixel skip/stop decisions downstream agree
-// with the reference exactly.  Jacobians are written in closed form.
+// Every value the rasterizer's decisions depend on (projected centre, depth,
+// 3D/2D covariance, conic, 3-sigma extents) is computed with explicit
+// round-to-nearest intrinsics (__fmul_rn, __fadd_rn, __fmaf_rn, __fdiv_rn)
+// in the operation order the reference build's FP32 results follow
+// (gsplatcu/kernel.cu:379-663): which product of each sum is fused into a
+// multiply-add and which is rounded on its own was pinned by reproducing the
+// reference build's outputs bit for bit from its inputs (exact FP32
+// emulation, 1M and 3M Gaussians, two cameras).  The intrinsics are never
+// contracted or reordered by the compiler, so the results do not depend on
+// the kernel these functions are inlined into (separate operator kernels,
+// the fused preprocess, the adjoint's recomputation): tile rectangles, sort
+// keys and the per-pixel skip/stop decisions downstream agree with the
+// reference exactly everywhere.  Jacobians are written in closed form.
 #pragma once
 
 #include "gsb_common.cuh"
 
 namespace gsb {
 
-// C[R x Cc] = A[R x In] * B[In x Cc], accumulated from zero in k order.
-template <int Rr, int In, int Cc>
-__device__ __forceinline__ void mat_mul(const float* A, const float* B, float* Cm) {
-#pragma unroll
-  for (int i = 0; i < Rr; ++i)
-#pragma unroll
-    for (int j = 0; j < Cc; ++j) {
-      float acc = 0.f;
-#pragma unroll
-      for (int k = 0; k < In; ++k) acc += A[i * In + k] * B[k * Cc + j];
-      Cm[i * Cc + j] = acc;
-    }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// a0 b0 + a1 b1 + a2 b2 accumulated from zero in index order, each product
+// fused into the running sum (the first rounded on its own).
+__device__ __forceinline__ float dot3_fused(float a0, float a1, float a2, float b0, float b1,
+                                            float b2) {
+  return rfma(a2, b2, rfma(a1, b1, rmul(a0, b0)));
+}
+// The same sum with every product rounded before it is added.
+__device__ __forceinline__ float dot3_plain(float a0, float a1, float a2, float b0, float b1,
+                                            float b2) {
+  return radd(radd(rmul(a0, b0), rmul(a1, b1)), rmul(a2, b2));
 }
 
 // ---------------------------------------------------------------- project
@@ -34,22 +44,18 @@ struct Projected {
   bool valid;     // z >= 0.2
 };
 
+// pc = Rcw pw + t; u = (x fx) / z + c written as (x fx) * (1/z) + c.
 __device__ __forceinline__ Projected project_point(float3 pw, const float* Rcw, float3 t, float fx,
                                                    float fy, float cx, float cy) {
-  float p[3] = {pw.x, pw.y, pw.z};
-  float pc[3];
-  mat_mul<3, 3, 1>(Rcw, p, pc);
   Projected r;
-  r.x = pc[0] + t.x;
-  r.y = pc[1] + t.y;
-  r.z = pc[2] + t.z;
+  r.x = radd(dot3_fused(Rcw[0], Rcw[1], Rcw[2], pw.x, pw.y, pw.z), t.x);
+  r.y = radd(dot3_fused(Rcw[3], Rcw[4], Rcw[5], pw.x, pw.y, pw.z), t.y);
+  r.z = radd(dot3_fused(Rcw[6], Rcw[7], Rcw[8], pw.x, pw.y, pw.z), t.z);
   r.valid = !(r.z < kMinDepth);
   if (r.valid) {
-    const float z_inv = 1.f / r.z;
-    const float x_fx = r.x * fx;
-    const float y_fy = r.y * fy;
-    r.ux = x_fx * z_inv + cx;
-    r.uy = y_fy * z_inv + cy;
+    const float z_inv = rdiv(1.f, r.z);
+    r.ux = rfma(rmul(r.x, fx), z_inv, cx);
+    r.uy = rfma(rmul(r.y, fy), z_inv, cy);
   } else {
     r.ux = r.uy = 0.f;
   }
@@ -57,45 +63,42 @@ __device__ __forceinline__ Projected project_point(float3 pw, const float* Rcw, 
 }
 
 // ------------------------------------------------------------ covariance
-// Rotation of an unnormalised quaternion (w, x, y, z), row-major.
+// Rotation of an unnormalised quaternion (w, x, y, z), row-major:
+// diagonal 1 - 2(.. + ..), off-diagonal 2(.. +- ..), each sum of two
+// products with the fused product the reference's results show.
 __device__ __forceinline__ void quat_rotation(float4 q, float* R) {
   const float w = q.x, x = q.y, y = q.z, z = q.w;
-  const float xx = x * x, yy = y * y, zz = z * z;
-  const float xy = x * y, xz = x * z, yz = y * z;
-  const float xw = x * w, yw = y * w, zw = z * w;
-  R[0] = 1.f - 2.f * (yy + zz);
-  R[1] = 2.f * (xy - zw);
-  R[2] = 2.f * (xz + yw);
-  R[3] = 2.f * (xy + zw);
-  R[4] = 1.f - 2.f * (xx + zz);
-  R[5] = 2.f * (yz - xw);
-  R[6] = 2.f * (xz - yw);
-  R[7] = 2.f * (yz + xw);
-  R[8] = 1.f - 2.f * (xx + yy);
+  const float xx = rmul(x, x), yy = rmul(y, y), zz = rmul(z, z);
+  const float xz = rmul(x, z), zw = rmul(z, w), xw = rmul(x, w);
+  R[0] = rsub(1.f, rmul(2.f, radd(yy, zz)));
+  R[1] = rmul(2.f, rfma(x, y, -zw));
+  R[2] = rmul(2.f, rfma(y, w, xz));
+  R[3] = rmul(2.f, rfma(x, y, zw));
+  R[4] = rsub(1.f, rmul(2.f, rfma(x, x, zz)));
+  R[5] = rmul(2.f, rfma(y, z, -xw));
+  R[6] = rmul(2.f, rfma(-y, w, xz));
+  R[7] = rmul(2.f, rfma(y, z, xw));
+  R[8] = rsub(1.f, rmul(2.f, rfma(x, x, yy)));
 }
 
 // Sigma = M M^T, M = R(q) diag(s); out = 6 upper entries (00,01,02,11,12,22).
-// Also returns M (row-major) for the Jacobians.
+// Also returns M (row-major) and R for the Jacobians.
 __device__ __forceinline__ void covariance_3d(float4 q, float3 s, float* cov, float* Mout,
                                               float* Rout) {
-  float R[9], M[9], Mt[9], S[9];
+  float R[9], M[9];
   quat_rotation(q, R);
   const float sv[3] = {s.x, s.y, s.z};
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) M[3 * r + c] = R[3 * r + c] * sv[c];
+    for (int c = 0; c < 3; ++c) M[3 * r + c] = rmul(R[3 * r + c], sv[c]);
+  const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
 #pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) Mt[3 * c + r] = M[3 * r + c];
-  mat_mul<3, 3, 3>(M, Mt, S);
-  cov[0] = S[0];
-  cov[1] = S[1];
-  cov[2] = S[2];
-  cov[3] = S[4];
-  cov[4] = S[5];
-  cov[5] = S[8];
+  for (int u = 0; u < 6; ++u) {
+    const float* a = M + 3 * sym[u][0];
+    const float* b = M + 3 * sym[u][1];
+    cov[u] = dot3_fused(a[0], a[1], a[2], b[0], b[1], b[2]);
+  }
   if (Mout)
 #pragma unroll
     for (int k = 0; k < 9; ++k) Mout[k] = M[k];
@@ -111,27 +114,34 @@ __device__ __forceinline__ void covariance_3d(float4 q, float3 s, float* cov, fl
 __device__ __forceinline__ void covariance_2d(const float* cov3, float px, float py, float pz,
                                               const float* Rcw, float fx, float fy, float tanx,
                                               float tany, float* cov2, float* Mout, float* xy) {
-  float x = px, y = py;
   const float z = pz;
-  const float limx = 1.3f * tanx;
-  const float limy = 1.3f * tany;
-  x = fminf(limx, fmaxf(-limx, x / z)) * z;
-  y = fminf(limy, fmaxf(-limy, y / z)) * z;
-  const float z2 = z * z;
-  const float J[6] = {fx / z, 0.0f, -(fx * x) / z2, 0.0f, fy / z, -(fy * y) / z2};
+  const float limx = rmul(1.3f, tanx);
+  const float limy = rmul(1.3f, tany);
+  const float x = rmul(fminf(limx, fmaxf(-limx, rdiv(px, z))), z);
+  const float y = rmul(fminf(limy, fmaxf(-limy, rdiv(py, z))), z);
+  const float z2 = rmul(z, z);
+  // J = [[fx/z, 0, -(fx x)/z^2], [0, fy/z, -(fy y)/z^2]]
+  const float J0[3] = {rdiv(fx, z), 0.0f, -rdiv(rmul(fx, x), z2)};
+  const float J1[3] = {0.0f, rdiv(fy, z), -rdiv(rmul(fy, y), z2)};
+  float M[6];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    M[j] = dot3_fused(J0[0], J0[1], J0[2], Rcw[j], Rcw[3 + j], Rcw[6 + j]);
+    M[3 + j] = dot3_fused(J1[0], J1[1], J1[2], Rcw[j], Rcw[3 + j], Rcw[6 + j]);
+  }
   const float a = cov3[0], b = cov3[1], c = cov3[2], d = cov3[3], e = cov3[4], f = cov3[5];
-  const float Sg[9] = {a, b, c, b, d, e, c, e, f};
-  float M[6], MS[6], Mt[6], Sp[4];
-  mat_mul<2, 3, 3>(J, Rcw, M);
-  mat_mul<2, 3, 3>(M, Sg, MS);
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int c2 = 0; c2 < 3; ++c2) Mt[2 * c2 + r] = M[3 * r + c2];
-  mat_mul<2, 3, 2>(MS, Mt, Sp);
-  cov2[0] = Sp[0] + 0.3f;
-  cov2[1] = Sp[1];
-  cov2[2] = Sp[3] + 0.3f;
+  // (M Sigma): row 0 fuses only the last product of its first entry; the
+  // other entries round every product
+  const float m00 = rfma(M[2], c, radd(rmul(M[0], a), rmul(M[1], b)));
+  const float m01 = dot3_plain(M[0], M[1], M[2], b, d, e);
+  const float m02 = dot3_plain(M[0], M[1], M[2], c, e, f);
+  const float m10 = dot3_plain(M[3], M[4], M[5], a, b, c);
+  const float m11 = dot3_plain(M[3], M[4], M[5], b, d, e);
+  const float m12 = dot3_plain(M[3], M[4], M[5], c, e, f);
+  // (M Sigma) M^T
+  cov2[0] = radd(dot3_fused(m00, m01, m02, M[0], M[1], M[2]), 0.3f);
+  cov2[1] = dot3_fused(m00, m01, m02, M[3], M[4], M[5]);
+  cov2[2] = radd(dot3_fused(m10, m11, m12, M[3], M[4], M[5]), 0.3f);
   if (Mout)
 #pragma unroll
     for (int k = 0; k < 6; ++k) Mout[k] = M[k];
@@ -145,13 +155,13 @@ __device__ __forceinline__ void covariance_2d(const float* cov3, float px, float
 // when 1/det is NaN (the Gaussian is then dropped).
 __device__ __forceinline__ bool conic_and_extent(float a, float b, float c, float* conic,
                                                  int* ext, float* det_inv_out) {
-  const float det_inv = 1.f / (a * c - b * b);
+  const float det_inv = rdiv(1.f, rfma(a, c, -rmul(b, b)));
   if (isnan(det_inv)) return false;
-  conic[0] = det_inv * c;
-  conic[1] = -det_inv * b;
-  conic[2] = det_inv * a;
-  ext[0] = (int)ceilf(3 * sqrtf(fabsf(a)));
-  ext[1] = (int)ceilf(3 * sqrtf(fabsf(c)));
+  conic[0] = rmul(det_inv, c);
+  conic[1] = rmul(-det_inv, b);
+  conic[2] = rmul(det_inv, a);
+  ext[0] = (int)ceilf(rmul(3.f, sqrtf(fabsf(a))));
+  ext[1] = (int)ceilf(rmul(3.f, sqrtf(fabsf(c))));
   if (det_inv_out) *det_inv_out = det_inv;
   return true;
 }

@@ -9,7 +9,7 @@ without a GPU.  Cases follow the reference's own call sequences
 without Jacobians, sh2Weight / sh2Weight_fast(_B) / sh2Color, splat_weight(_B)
 and splat_color(_B), plus the 4-Gaussian fixture of gsplat/gau_io.py:180-204.
 
-    python tests/golden/make_golden.py [--out gpurun_out/golden]
+    python tests/golden/make_golden.py --out <directory for the .npz files>
 """
 import argparse
 import os
@@ -98,7 +98,7 @@ def case_color(ref, pws, rots, scales, alphas, shs, W, H, eye, target, seed):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory the .npz files are written to")
     a = ap.parse_args()
     ref = load_ref()
     if ref is None:

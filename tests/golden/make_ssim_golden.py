@@ -9,6 +9,9 @@ tests/golden/ssim_gau_loss.npz.  tests/test_oracle_ssim.py pins the CPU oracle
 to it.
 
     python tests/golden/make_ssim_golden.py [--reference /path/to/ReparamGS-Palette]
+
+The reference checkout defaults to $GSB_REFERENCE_ROOT, else the location
+oracle/build_ref.py uses.
 """
 import argparse
 import importlib.util
@@ -23,7 +26,10 @@ CASES = [(3, 23, 37, 0), (3, 40, 33, 1), (3, 7, 5, 2), (3, 36, 44, 3)]
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")  # the sources, read-only
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.build_ref import reference_root
+    ap.add_argument("--reference", default=reference_root())  # the sources, read-only
     ap.add_argument("--out", default=os.path.join(HERE, "ssim_gau_loss.npz"))
     a = ap.parse_args()
     path = os.path.join(a.reference, "vanilla_3dgs", "gsplat", "pytorch_ssim.py")

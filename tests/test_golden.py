@@ -1,7 +1,11 @@
 """Pin the CPU oracle to golden vectors produced by the reference extension
 itself (tests/golden/make_golden.py, run on a B200 against the reference
-build).  CPU only.  Float outputs: FP32 tolerances; tile lists, ranges and
-in-place updates: bit-exact given the reference's own projected inputs."""
+build).  CPU only.  Geometry (centres, camera-space points, 3D and 2D
+covariances, conics, extents, depth updates): bit-exact, the oracle's FP32
+instantiation follows the reference build's operation order including its
+fused multiply-adds; tile lists, ranges, contributor indices and in-place
+updates: bit-exact; images within 1e-5; Jacobians and SH values (the
+reference evaluates SH with FP64 constants): FP32 tolerances."""
 import glob
 import os
 
@@ -20,6 +24,15 @@ class _Cam:
         self.width, self.height = int(w), int(h)
 
 
+def _bits(a, b, live=None):
+    """Bitwise equality of FP32 arrays (on the rows in `live`)."""
+    a, b = np.asarray(a, np.float32), np.asarray(b, np.float32)
+    if live is not None:
+        a, b = a[live], b[live]
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), \
+        float(np.mean(a.view(np.uint32) == b.view(np.uint32)))
+
+
 def _close(a, b, rtol, atol, frac=1.0):
     ok = np.isclose(a, b, rtol=rtol, atol=atol)
     assert ok.mean() >= frac, (float(ok.mean()), float(np.max(np.abs(a - b))))
@@ -35,25 +48,26 @@ def _check_geometry(z):
     cam = _Cam(z)
     Rcw, tcw = z["Rcw"].astype(np.float32), z["tcw"].astype(np.float32)
     us, pcs, d, du = orc.project(z["pws"], Rcw, tcw, cam.fx, cam.fy, cam.cx, cam.cy, True)
-    _close(us, z["us"], 1e-6, 1e-4)
-    _close(pcs, z["pcs"], 1e-6, 1e-6)
-    assert np.array_equal(d < 0.2, z["depths_proj"] < 0.2)
+    live = z["depths_proj"] >= 0.2
+    _bits(us, z["us"], live)
+    _bits(pcs, z["pcs"], live)
+    _bits(d, z["depths_proj"])
     assert _rel(du, z["du_dpcs"]) < 1e-6
     c3, dr, ds = orc.cov3d(z["rots"], z["scales"], z["depths_proj"], True)
-    _close(c3, z["cov3ds"], 1e-5, 1e-10)
+    _bits(c3, z["cov3ds"], live)
     # Jacobians: norm-wise (entries with cancellation round differently with FMA)
     assert _rel(dr, z["dcov3d_drots"]) < 1e-5
     assert _rel(ds, z["dcov3d_dscales"]) < 1e-5
     c2, d3, dp = orc.cov2d(z["cov3ds"], z["pcs"], Rcw, z["depths_proj"], cam.fx, cam.fy, cam.width,
                            cam.height, True)
-    _close(c2, z["cov2ds"], 1e-5, 1e-6)
+    _bits(c2, z["cov2ds"], live)
     assert _rel(d3, z["dcov2d_dcov3ds"]) < 1e-5
     assert _rel(dp, z["dcov2d_dpcs"]) < 1e-4
     d2 = z["depths_proj"].copy()
     ci, ar, dci = orc.inverse_cov2d(z["cov2ds"], d2, True)
     assert np.array_equal(d2, z["depths_pre"])
-    _close(ci, z["cinv2ds"], 1e-5, 1e-7)
-    assert np.mean(ar != z["areas_pre"]) < 1e-3
+    _bits(ci, z["cinv2ds"], live)
+    assert np.array_equal(ar[live], z["areas_pre"][live])
     assert _rel(dci, z["dcinv2d_dcov2ds"]) < 1e-5
     return cam
 
@@ -68,10 +82,9 @@ def _check_splat(z, K, feats, out_key, dkey, tau_init):
     assert np.array_equal(d, z["depths_post"]) and np.array_equal(a, z["areas_post"])
     out, contrib, ft = orc.draw(H, W, K, z["ranges"], z["gsid"], z["us"], z["cinv2ds"], z["alphas"],
                                 feats, tau_init)
-    same = contrib == z["contrib"]
-    assert same.mean() > 0.999
-    assert np.max(np.abs(out - z[out_key])[:, same]) < 1e-5
-    assert np.max(np.abs(ft - z["final_tau"])[same]) < 1e-5
+    assert np.array_equal(contrib, z["contrib"])
+    assert np.max(np.abs(out - z[out_key])) < 1e-5
+    assert np.max(np.abs(ft - z["final_tau"])) < 1e-5
     return out, contrib, ft
 
 
