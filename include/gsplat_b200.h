@@ -6,7 +6,9 @@
  * (cudaStream_t passed as void*; NULL is the legacy default stream), enqueues
  * its kernels on that stream and returns a status code (GSB_OK == 0).  No
  * entry point allocates device memory: callers pass every output buffer and
- * every scratch buffer, sized with the *_workspace_bytes() queries.  On error
+ * every scratch buffer, sized with the *_bytes() queries (gsb_splat_state_bytes,
+ * gsb_splat_sort_bytes, ...), except gsb_splat_sort_static, which sorts in a
+ * fixed file-scope device array.  On error
  * gsb_last_error() returns a message for the calling thread.
  *
  * The functions under "reference operators" are the kernels behind the 13
@@ -53,6 +55,24 @@ int gsb_version(void);
 #define GSB_STATUS_PATCH_OVERFLOW 2u     /* more patches than the capacity       */
 #define GSB_STATUS_DEPTH_KEY_OVERFLOW 4u /* a depth key above max_depth_key      */
 int gsb_device_status(uint32_t* status, int clear, void* stream);
+/* Asynchronous form: enqueues on `stream` one-thread kernels that OR the
+ * device status bits into *out (device memory, or pinned host memory mapped
+ * into the device's address space) without synchronising or clearing; the
+ * caller reads *out once the stream has passed that point.  Callers enqueue
+ * it after the entry points whose kernels stage through bounded bulk-copy
+ * waits (gsb_sh2weight_fast, gsb_sh2weight_fast_backward,
+ * gsb_render_preprocess, gsb_render_backward(_accumulate)) and raise
+ * GSB_ERR_DEVICE_TIMEOUT when a bit is set.  No counterpart in the
+ * reference, whose CUDA errors are printed and ignored
+ * (gsplatcu/common.cuh:19-25). */
+int gsb_device_status_fetch(uint32_t* out, void* stream);
+/* Test hook for that error path: launches one block that arms an mbarrier
+ * for a transaction no copy delivers and waits on it at most `poll_limit`
+ * times (1..65536); the wait runs out and GSB_STATUS_BULK_TIMEOUT is set, as
+ * when a real bulk copy never completes.  No copy is in flight when the
+ * kernel returns, so the context stays usable.  No counterpart in the
+ * reference. */
+int gsb_debug_expire_bulk_wait(uint32_t poll_limit, void* stream);
 /* Number of kernels this library has launched in the process so far
  * (diagnostic; used to report how many of the library's kernels a timed
  * region ran). */
@@ -176,8 +196,10 @@ int gsb_splat_sort(int64_t n, int height, int width, const gsb_splat_plan* plan,
  * 32-bit keys, 1.3M with 64-bit keys), which every GPU that loads the library
  * holds until the process exits.  Plans needing more return GSB_ERR_CAPACITY
  * with a message; use gsb_splat_sort then.  Allocates nothing; the first
- * call on each device looks up the array's device address (once, with that
- * device current), so make that first call before any stream capture.  All
+ * call on each device looks up the array's device address (once per device
+ * and CUDA context, with that device current: after a device reset or a
+ * re-created primary context the next call looks it up again), so make the
+ * first call in each context before any stream capture.  All
  * calls on a device share the array and it keeps the last call's contents
  * (nothing needs to start at zero), so calls that overlap on the GPU race:
  * order them on one stream.  Inputs, outputs and results as gsb_splat_sort. */
@@ -342,6 +364,18 @@ int gsb_render_preprocess(int64_t n, const gsb_camera* cam, const float* pws, co
                           const float* scales, const float* alphas,
                           const gsb_palette_params* params, void* state, float* depths_out,
                           void* stream);
+
+/* The weight-parameter half of the reference backward in one kernel: from
+ * dloss_dweights [n,K] (splat_weight_B's output) to dw0 (shs [n,16K] for
+ * full weights, dc [n,K] for low-rank) and dA [n,P,rank], dB [n,rank,Q]
+ * (FP32, overwritten), recomputing the view direction and SH basis from
+ * pws and cam->twc.  Replaces, on the GPU, the reference backward's
+ * batched outer product dW x dweight_dshs (gsplat/gsmodel.py:140-143) and
+ * its dW * dweight_ddc + sh2Weight_fast_B pair (gsmodel.py:194-198), so the
+ * forward needs no Jacobian outputs.  Shapes as gsb_render_preprocess. */
+int gsb_palette_weights_backward(int64_t n, const gsb_camera* cam, const float* pws,
+                                 const gsb_palette_params* params, const float* dloss_dweights,
+                                 float* dw0, float* dA, float* dB, void* stream);
 
 /* Scratch bytes gsb_render_backward needs for the per-Gaussian screen-space
  * gradients. */

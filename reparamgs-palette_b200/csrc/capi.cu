@@ -87,6 +87,19 @@ GSB_API int gsb_device_status(uint32_t* status, int clear, void* stream) {
   return GSB_OK;
 }
 
+GSB_API int gsb_device_status_fetch(uint32_t* out, void* stream) {
+  GSB_CHECK_ARG(out, "device_status_fetch: null pointer");
+  int rc = lowrank_status_fetch(out, ST(stream));
+  if (rc) return rc;
+  return fused_status_fetch(out, ST(stream));
+}
+
+GSB_API int gsb_debug_expire_bulk_wait(uint32_t poll_limit, void* stream) {
+  GSB_CHECK_ARG(poll_limit >= 1 && poll_limit <= (1u << 16),
+                "debug_expire_bulk_wait: poll_limit must be in [1, 65536]");
+  return expire_bulk_wait(poll_limit, ST(stream));
+}
+
 GSB_API unsigned long long gsb_launch_count(void) {
   return g_launches.load(std::memory_order_relaxed);
 }
@@ -531,6 +544,34 @@ static int render_backward(int64_t n, const gsb_camera* cam, const float* pws, c
   f.accumulate = acc;
   return launch_render(params->mode, params->dtype, K, params->P, params->Q, params->rank, f, true,
                        ST(stream));
+}
+
+GSB_API int gsb_palette_weights_backward(int64_t n, const gsb_camera* cam, const float* pws,
+                                         const gsb_palette_params* params,
+                                         const float* dloss_dweights, float* dw0, float* dA,
+                                         float* dB, void* stream) {
+  GSB_CHECK_ARG(cam && cam->twc, "palette_weights_backward: null camera");
+  GSB_CHECK_ARG(n >= 0, "palette_weights_backward: n < 0");
+  int rc = check_params("palette_weights_backward", n, params);
+  if (rc) return rc;
+  GSB_CHECK_ARG(!params->palette, "palette_weights_backward: palette-colour parameters have no adjoint here");
+  GSB_CHECK_ARG(n == 0 || (pws && dloss_dweights && dw0), "palette_weights_backward: null pointer");
+  GSB_CHECK_ARG(params->mode == GSB_WEIGHTS_FULL || n == 0 || (dA && dB),
+                "palette_weights_backward: null low-rank gradient outputs");
+  if (n == 0) return GSB_OK;
+  FusedArgs f{};
+  f.n = n;
+  f.cam = cam_args(cam);
+  f.pws = pws;
+  f.w0 = params->w0;
+  f.wa = params->A;
+  f.wb = params->B;
+  f.g_feat = dloss_dweights;  // g_u null: the weights-only chain
+  f.d_w0 = dw0;
+  f.d_wa = dA;
+  f.d_wb = dB;
+  return launch_render(params->mode, params->dtype, params->K, params->P, params->Q, params->rank,
+                       f, true, ST(stream));
 }
 
 GSB_API int gsb_render_backward(int64_t n, const gsb_camera* cam, const float* pws,

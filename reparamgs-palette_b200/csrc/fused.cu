@@ -828,6 +828,37 @@ int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedAr
                                  : dispatch_fused<float>(mode, K, P, Q, R, f, bwd, st);
 }
 
+// ORs this file's status word into *out (see k_lowrank_status_fetch).
+__global__ void k_fused_status_fetch(uint32_t* out) {
+  pdl_wait();
+  const uint32_t v = *(volatile uint32_t*)&g_fused_status;
+  if (v) *(volatile uint32_t*)out |= v;
+}
+
+int fused_status_fetch(uint32_t* out, cudaStream_t st) {
+  launch_pdl(k_fused_status_fetch, dim3(1), dim3(1), 0, st, out);
+  return check_launch("device_status_fetch");
+}
+
+// Error-path check: one block arms an mbarrier for a 16-byte transaction
+// that no copy will ever deliver and waits on it with the given poll limit;
+// the wait runs out, the kernel sets the bulk-timeout bit exactly as the
+// staging kernels do, and returns.  Nothing is in flight when it exits.
+__global__ void k_expire_bulk_wait(uint32_t poll_limit) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, 16);
+    if (!mbar_wait(&bar, 0, poll_limit)) atomicOr(&g_fused_status, kStatusBulkTimeout);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar)) : "memory");
+  }
+}
+
+int expire_bulk_wait(uint32_t poll_limit, cudaStream_t st) {
+  k_expire_bulk_wait<<<1, 32, 0, st>>>(poll_limit);
+  return check_launch("debug_expire_bulk_wait");
+}
+
 int fused_status(uint32_t* out, bool clear, cudaStream_t st) {
   if (cudaMemcpyFromSymbolAsync(out, g_fused_status, sizeof(uint32_t), 0, cudaMemcpyDeviceToHost,
                                 st) != cudaSuccess)

@@ -28,6 +28,7 @@ int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtyp
                                int L, float* dA, float* dB, cudaStream_t st);
 int launch_lab2rgb(int H, int W, const float* lab, float* rgb, cudaStream_t st);
 int lowrank_status(uint32_t* out, bool clear, cudaStream_t st);
+int lowrank_status_fetch(uint32_t* out, cudaStream_t st);
 
 // loss.cu
 int launch_palette_l1(int K, int H, int W, const float* layer, const float* palette,
@@ -128,5 +129,7 @@ struct FusedArgs {
 int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedArgs& f, bool backward,
                   cudaStream_t st);
 int fused_status(uint32_t* out, bool clear, cudaStream_t st);
+int fused_status_fetch(uint32_t* out, cudaStream_t st);
+int expire_bulk_wait(uint32_t poll_limit, cudaStream_t st);
 
 }  // namespace gsb

@@ -13,7 +13,7 @@ namespace gsb {
 
 constexpr uint32_t kMbarPollLimit = 1u << 22;
 
-// Device status bits (read with gsb_device_status).
+// Device status bits (read with gsb_device_status / gsb_device_status_fetch).
 constexpr uint32_t kStatusBulkTimeout = 1u;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -43,10 +43,11 @@ __device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t
       : "memory");
 }
 
-// true once the barrier's phase `parity` has completed; false after the poll
-// limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < kMbarPollLimit; ++it) {
+// true once the barrier's phase `parity` has completed; false after `limit`
+// polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t limit = kMbarPollLimit) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"

@@ -172,20 +172,19 @@ constexpr int kShCopy = 8;
 
 template <int K, typename T>
 __global__ void __launch_bounds__(kShThreads)
-    k_sh2feat(int64_t n, const T* __restrict__ shs, int nb, const float* __restrict__ pws,
-              const float* __restrict__ twc, float* __restrict__ feat, float* __restrict__ dshs,
-              float* __restrict__ dpws) {
+    k_sh2feat(int64_t n, const T* __restrict__ shs, int nb, bool staged,
+              const float* __restrict__ pws, const float* __restrict__ twc,
+              float* __restrict__ feat, float* __restrict__ dshs, float* __restrict__ dpws) {
   extern __shared__ float srows[];
   const int rl = nb * K, stride = rl | 1;
   const int64_t row0 = (int64_t)blockIdx.x * kShThreads;
   const int rows = (int)min((int64_t)kShThreads, n - row0);
-  // FP32 rows are copied element by element; BF16 rows of even length
-  // (4-byte aligned) as element pairs, one 32-bit load each (2-byte element
-  // loads cost more than the strided reads they replace); other BF16 rows are
-  // read in place.
+  // FP32 rows are copied element by element; BF16 rows of even length from a
+  // 4-byte aligned base as element pairs, one 32-bit load each (2-byte
+  // element loads cost more than the strided reads they replace); other BF16
+  // rows are read in place.  The host makes that decision (`staged`) and
+  // sizes the shared memory by it.
   constexpr bool kF32 = sizeof(T) == 4;
-  const bool pairs = !kF32 && (rl & 1) == 0 && (reinterpret_cast<uintptr_t>(shs) & 3) == 0;
-  const bool staged = kF32 || pairs;
   if (staged) {
     // G elements per load; (row, column) of load e advanced by kShThreads
     // loads per step
@@ -300,12 +299,15 @@ static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws
                      float* feat, float* dshs, float* dpws, cudaStream_t st) {
   const T* s = (const T*)shs;
   const int g = div_up(n > 0 ? n : 1, kShThreads);
-  const bool staged = sizeof(T) == 4 || (nb * K) % 2 == 0;  // (as decided in the kernel)
+  // BF16 rows are staged as 32-bit element pairs: only rows of even length
+  // from a 4-byte aligned base
+  const bool staged = sizeof(T) == 4 ||
+                      ((nb * K) % 2 == 0 && (reinterpret_cast<uintptr_t>(shs) & 3) == 0);
   const size_t smem = staged ? (size_t)kShThreads * ((nb * K) | 1) * sizeof(float) : 0;
   switch (K) {
-#define GSB_K(KK)                                                                            \
-  case KK:                                                                                   \
-    k_sh2feat<KK, T><<<g, kShThreads, smem, st>>>(n, s, nb, pws, twc, feat, dshs, dpws);    \
+#define GSB_K(KK)                                                                              \
+  case KK:                                                                                     \
+    k_sh2feat<KK, T><<<g, kShThreads, smem, st>>>(n, s, nb, staged, pws, twc, feat, dshs, dpws); \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K

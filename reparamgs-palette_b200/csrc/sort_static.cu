@@ -19,6 +19,8 @@
 // that overlap on the GPU -- on different streams, or from different host
 // threads without ordering -- use the same bytes and race; order them on one
 // stream or with events.
+#include <cuda.h>  // CUcontext / CUresult types only: the two driver calls below are
+                   // resolved at run time through the runtime's entry-point query
 #include <mutex>
 
 #include "gsb_common.cuh"
@@ -32,10 +34,46 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortBytes];
 
 // Host code may not take the address of g_sort_scratch (that would be a
 // host-side stand-in, not device memory); the device address comes from
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress, with the device current.  It is looked up once per
+// device and CUDA context: the cache is keyed by the context's process-unique
+// id (cuCtxGetId), so after a device reset or a re-created primary context
+// the next call looks the address up again instead of reusing a stale one.
 constexpr int kMaxStaticDevices = 64;
-static void* g_scratch_addr[kMaxStaticDevices];
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  void* addr;
+};
+static ScratchEntry g_scratch[kMaxStaticDevices];
 static std::mutex g_scratch_mutex;
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Process-unique id of the calling thread's current context (0 if unknown).
+static unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {  // (called with g_scratch_mutex held)
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) !=
+            cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2) !=
+            cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+    (void)cudaGetLastError();
+    resolved = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+      get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 static int static_scratch(void** out) {
   int dev = 0;
@@ -45,18 +83,23 @@ static int static_scratch(void** out) {
     return GSB_ERR_UNSUPPORTED;
   }
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
+  // (no context current yet: id 0, the address is looked up, which makes the
+  // device's primary context current for the launch)
+  const unsigned long long ctx = current_context_id();
+  ScratchEntry& e = g_scratch[dev];
+  if (!e.addr || ctx == 0 || e.ctx_id != ctx) {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
-    if (e != cudaSuccess || !p) {
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (err != cudaSuccess || !p) {
       (void)cudaGetLastError();
       set_error("splat_sort_static: cudaGetSymbolAddress failed on device %d: %s", dev,
-                cudaGetErrorString(e));
+                cudaGetErrorString(err));
       return GSB_ERR_CUDA;
     }
-    g_scratch_addr[dev] = p;
+    e.addr = p;
+    e.ctx_id = ctx;
   }
-  *out = g_scratch_addr[dev];
+  *out = e.addr;
   return GSB_OK;
 }
 

@@ -34,7 +34,7 @@ from ._lib import GsplatError, call, ptr, stream_of
 __all__ = [
     "project", "computeCov3D", "computeCov2D", "inverseCov2D", "sh2Weight", "sh2Weight_fast",
     "sh2Weight_fast_B", "sh2Color", "splat_weight", "splat_weight_B", "splat_color",
-    "splat_color_B", "lab2rgb", "splat_weight_B_full", "GsplatError",
+    "splat_color_B", "lab2rgb", "splat_weight_B_full", "GsplatError", "check_device_status",
 ]
 
 TILE = 16
@@ -211,8 +211,10 @@ def sh2Weight_fast(shs_dc, shs_A, shs_B, pws, twc, calc_J, num_palette, Q):
     ddc = _empty((n, K), pws) if calc_J else None
     ylm = _empty((n, L), pws) if calc_J else None
     with torch.cuda.device(pws.device):
+        st = stream_of(pws)
         call(op, "gsb_sh2weight_fast", n, ptr(dc), ptr(A), ptr(B), _sh_dtype(A), K, P, Q, rank,
-             ptr(pws), ptr(twc), ptr(w), ptr(ddc), ptr(ylm), stream_of(pws))
+             ptr(pws), ptr(twc), ptr(w), ptr(ddc), ptr(ylm), st)
+        _lib.fetch_device_status(pws.device, st)
     return [w, ddc, ylm] if calc_J else [w]
 
 
@@ -229,9 +231,25 @@ def sh2Weight_fast_B(shs_A, shs_B, Ylm_stored, dloss_dw, num_palette, Q):
         raise ValueError(f"gsplatcu.{op}: Ylm has {int(ylm.shape[1])} bands but P*Q/K = {P * Q // K}")
     dA, dB = _empty(tuple(A.shape), A), _empty(tuple(B.shape), A)
     with torch.cuda.device(A.device):
+        st = stream_of(A)
         call(op, "gsb_sh2weight_fast_backward", n, ptr(A), ptr(B), _sh_dtype(A), ptr(ylm), ptr(dw),
-             K, P, Q, rank, ptr(dA), ptr(dB), stream_of(A))
+             K, P, Q, rank, ptr(dA), ptr(dB), st)
+        _lib.fetch_device_status(A.device, st)
     return [dA, dB]
+
+
+def check_device_status(device=None):
+    """Wait for the current stream of `device` and raise
+    ``GsplatError`` (``status == GSB_ERR_DEVICE_TIMEOUT``) if a bounded
+    device-side wait of an earlier call on this thread ran out.  The forward
+    operators check at their own patch-count read-back; call this after a
+    backward pass or a batch of calls whose results are used without one."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else \
+        torch.device(device)
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    torch.cuda.current_stream(dev).synchronize()
+    _lib.raise_if_timed_out(dev, "check_device_status")
 
 
 # --------------------------------------------------------------- splatting
@@ -241,18 +259,7 @@ _CAPACITY = {}
 _READBACK = {}
 
 
-def _mapped_address(host):
-    """Device address of a pinned host tensor, or None when the runtime does
-    not map it into the device's address space."""
-    try:
-        from cuda.bindings import runtime as rt
-        err, dptr = rt.cudaHostGetDevicePointer(host.data_ptr(), 0)
-        if err == rt.cudaError_t.cudaSuccess:
-            return int(dptr)
-        rt.cudaGetLastError()  # a refused query must not surface at the next launch check
-    except Exception:
-        pass
-    return None
+_mapped_address = _lib.mapped_address
 
 
 def _readback_buffers(dev):
@@ -300,10 +307,12 @@ def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_
         call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(full), ptr(state),
              float(tau_init), ptr(out), ptr(contrib), ptr(final_tau), st)
         counted.synchronize()
+        _lib.raise_if_timed_out(dev, op)
         if int(host[0]) == 0:
             return full[:int(host[1]) | (int(host[2]) << 32)]
     plan = _lib.SplatPlan()
     call(op, "gsb_splat_counts", n, H, W, ptr(state), C.byref(plan), st)
+    _lib.raise_if_timed_out(dev, op)
     M = int(plan.patches)
     ws = torch.empty(max(1, int(L.gsb_splat_sort_bytes(n, H, W, C.byref(plan)))),
                      dtype=torch.uint8, device=dev)

@@ -6,6 +6,7 @@ anything another way.
 """
 import ctypes as C
 import os
+import threading
 
 import torch
 
@@ -37,6 +38,8 @@ _SIGS = {
     "gsb_version": (_i32, []),
     "gsb_launch_count": (C.c_ulonglong, []),
     "gsb_device_status": (_i32, [_p, _i32, _p]),
+    "gsb_device_status_fetch": (_i32, [_p, _p]),
+    "gsb_debug_expire_bulk_wait": (_i32, [_u32, _p]),
     "gsb_project": (_i32, [_i64, _p, _p, _p, _f32, _f32, _f32, _f32, _p, _p, _p, _p, _p]),
     "gsb_compute_cov3d": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_compute_cov2d": (_i32, [_i64, _p, _p, _p, _p, _f32, _f32, _f32, _f32, _p, _p, _p, _p]),
@@ -70,6 +73,7 @@ _SIGS = {
                                          _p, _p, _p, _p]),
     "gsb_render_preprocess": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_render_backward_bytes": (_sz, [_i64, _i32]),
+    "gsb_palette_weights_backward": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_render_backward": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
                                    _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_render_backward_accumulate": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
@@ -100,7 +104,12 @@ class PaletteParams(C.Structure):
 
 
 class GsplatError(RuntimeError):
-    """A CUDA-side failure reported by libgsplat_b200."""
+    """A CUDA-side failure reported by libgsplat_b200; ``status`` is the
+    library's status code (GSB_ERR_*)."""
+
+    def __init__(self, msg, status=GSB_ERR_CUDA):
+        super().__init__(msg)
+        self.status = status
 
 
 def lib():
@@ -130,7 +139,7 @@ def call(op, name, *args):
         msg = (lib().gsb_last_error() or b"").decode(errors="replace")
         if rc == GSB_ERR_INVALID_ARGUMENT:
             raise ValueError(f"gsplatcu.{op}: {msg}")
-        raise GsplatError(f"gsplatcu.{op}: {msg} (status {rc})")
+        raise GsplatError(f"gsplatcu.{op}: {msg} (status {rc})", rc)
 
 
 def ptr(t):
@@ -139,3 +148,72 @@ def ptr(t):
 
 def stream_of(t):
     return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def mapped_address(host):
+    """Device address of a pinned host tensor, or None when the runtime does
+    not map it into the device's address space."""
+    try:
+        from cuda.bindings import runtime as rt
+        err, dptr = rt.cudaHostGetDevicePointer(host.data_ptr(), 0)
+        if err == rt.cudaError_t.cudaSuccess:
+            return int(dptr)
+        rt.cudaGetLastError()  # a refused query must not surface at the next launch check
+    except Exception:
+        pass
+    return None
+
+
+# ------------------------------------------------- bounded device waits
+# Kernels that stage through bulk copies wait on them a bounded number of
+# times; when a wait runs out the kernel sets a device status bit and returns
+# without its results.  After every call that launches such kernels the
+# operators enqueue gsb_device_status_fetch into a pinned host word of the
+# calling thread; wherever the host waits for the stream anyway (the patch
+# count read-back of splat_weight / render_palette, check_device_status) the
+# word is read and a set bit raises GsplatError(GSB_ERR_DEVICE_TIMEOUT).
+_TIMEOUT_WORDS = {}
+
+
+def _timeout_word(dev):
+    key = (dev.index, threading.get_ident())
+    w = _TIMEOUT_WORDS.get(key)
+    if w is None:
+        host = torch.zeros((1,), dtype=torch.int32, pin_memory=True)
+        addr = mapped_address(host)
+        dword = None if addr is not None else torch.zeros((1,), dtype=torch.int32, device=dev)
+        w = _TIMEOUT_WORDS[key] = (host, addr, dword)
+    return w
+
+
+def fetch_device_status(dev, stream):
+    """Enqueue, on `stream` (a c_void_p), the copy of the device status bits
+    into this thread's host word for `dev`."""
+    host, addr, dword = _timeout_word(dev)
+    if addr is not None:
+        call("device_status_fetch", "gsb_device_status_fetch", C.c_void_p(addr), stream)
+    else:
+        call("device_status_fetch", "gsb_device_status_fetch", ptr(dword), stream)
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream.value, device=dev)):
+            host.copy_(dword, non_blocking=True)
+
+
+def raise_if_timed_out(dev, op):
+    """Call once the stream has passed the fetches of interest: raises
+    GsplatError(GSB_ERR_DEVICE_TIMEOUT) if a bounded wait expired (and
+    clears the bits, so that later calls start clean)."""
+    w = _TIMEOUT_WORDS.get((dev.index, threading.get_ident()))
+    if w is None or int(w[0][0]) == 0:
+        return
+    bits = int(w[0][0])
+    w[0].zero_()
+    if w[2] is not None:
+        w[2].zero_()
+    cleared = C.c_uint32(0)
+    with torch.cuda.device(dev):
+        call("device_status", "gsb_device_status", C.byref(cleared), 1,
+             C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    raise GsplatError(
+        f"gsplatcu.{op}: a bounded device-side wait for a bulk copy ran out (status bits "
+        f"{bits:#x}); the results of the calls since the last check are incomplete "
+        f"(status {GSB_ERR_DEVICE_TIMEOUT})", GSB_ERR_DEVICE_TIMEOUT)

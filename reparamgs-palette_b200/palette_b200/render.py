@@ -122,6 +122,7 @@ def _render_one(pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank):
         _lib.call("render_palette", "gsb_render_preprocess", n, C.byref(camst), _lib.ptr(pws),
                   _lib.ptr(rots), _lib.ptr(scales), _lib.ptr(alphas), C.byref(params),
                   _lib.ptr(state), _lib.ptr(depths), st)
+        _lib.fetch_device_status(dev, st)  # checked at the patch-count read-back below
         gx, gy = (W + 15) // 16, (H + 15) // 16
         ranges = torch.empty((gx * gy, 2), dtype=torch.int32, device=dev)
         layer = torch.empty((K, H, W), dtype=_F32, device=dev)
@@ -176,6 +177,7 @@ class _RenderPalette(torch.autograd.Function):
                       _lib.ptr(scratch), _lib.ptr(dpws), _lib.ptr(drots), _lib.ptr(dscales),
                       _lib.ptr(dalphas), _lib.ptr(dw0), _lib.ptr(dA), _lib.ptr(dB),
                       _lib.stream_of(pws))
+            _lib.fetch_device_status(dev, _lib.stream_of(pws))
         if dalphas is not None:
             dalphas = dalphas.reshape(alphas.shape)
         cast = lambda g, like: None if g is None else g.to(like.dtype)
@@ -277,6 +279,7 @@ class _RenderPaletteViews(torch.autograd.Function):
                           _lib.ptr(dlayer), _lib.ptr(dtau), _lib.ptr(scratch), _lib.ptr(dpws),
                           _lib.ptr(drots), _lib.ptr(dscales), _lib.ptr(dalphas), _lib.ptr(dw0),
                           _lib.ptr(dA), _lib.ptr(dB), st)
+            _lib.fetch_device_status(dev, st)
         if dalphas is not None:
             dalphas = dalphas.reshape(alphas.shape)
         cast = lambda g, like: None if g is None else g.to(like.dtype)

@@ -126,15 +126,20 @@ class _Bucket:
 
 
 class _Slot:
-    """One execution slot: stream, input buffers, workspaces, graphs."""
+    """One execution slot: stream, input buffers, workspaces, graphs.
+    `alloc(shape, dtype)` allocates its device buffers (torch.empty on the
+    slot's device unless the server was given another allocator)."""
 
-    def __init__(self, device, K_max):
+    def __init__(self, device, K_max, alloc=None):
         self.device = device
+        self.alloc = alloc or (lambda shape, dtype: torch.empty(shape, dtype=dtype, device=device))
         self.stream = torch.cuda.Stream(device)
         self.Rcw = torch.zeros((3, 3), dtype=_F32, device=device)
         self.tcw = torch.zeros((3,), dtype=_F32, device=device)
         self.twc = torch.zeros((3,), dtype=_F32, device=device)
         self.palette = torch.zeros((K_max, 3), dtype=_F32, device=device)
+        # words 0-2: overflow bits and patch count of the capacity sort; word 3:
+        # the library's device status bits (a bounded bulk-copy wait ran out)
         self.status = torch.zeros((4,), dtype=torch.int32, device=device)
         self.status_host = torch.zeros((4,), dtype=torch.int32).pin_memory()
         self.sizes = dict(state=0, sort=0, gsid=0, tiles=0, pixels=0)
@@ -154,16 +159,18 @@ class _Slot:
                     pixels=b.pixels)
         if all(need[k] <= self.sizes[k] for k in need):
             return False
-        for k in need:
-            self.sizes[k] = max(self.sizes[k], need[k])
-        dev, s = self.device, self.sizes
-        u8 = lambda nb: torch.empty((max(256, nb),), dtype=torch.uint8, device=dev)
-        self.buf = dict(state=u8(s["state"]), sort=u8(s["sort"]),
-                        gsid=torch.empty((max(1, s["gsid"]),), dtype=torch.int32, device=dev),
-                        ranges=torch.empty((s["tiles"], 2), dtype=torch.int32, device=dev),
-                        image=torch.empty((3 * s["pixels"],), dtype=_F32, device=dev),
-                        contrib=torch.empty((s["pixels"],), dtype=torch.int32, device=dev),
-                        final_tau=torch.empty((s["pixels"],), dtype=_F32, device=dev))
+        s = {k: max(self.sizes[k], need[k]) for k in need}
+        a = self.alloc
+        u8 = lambda nb: a((max(256, nb),), torch.uint8)
+        # all new buffers first: if one allocation fails the slot keeps its
+        # old buffers, sizes and graphs
+        buf = dict(state=u8(s["state"]), sort=u8(s["sort"]),
+                   gsid=a((max(1, s["gsid"]),), torch.int32),
+                   ranges=a((s["tiles"], 2), torch.int32),
+                   image=a((3 * s["pixels"],), _F32),
+                   contrib=a((s["pixels"],), torch.int32),
+                   final_tau=a((s["pixels"],), _F32))
+        self.sizes, self.buf = s, buf
         self.graphs.clear()
         return True
 
@@ -187,8 +194,10 @@ class _Slot:
         _lib.call("serve", "gsb_splat_draw", n, H, W, 3, _lib.ptr(bf["ranges"]),
                   _lib.ptr(bf["gsid"]), _lib.ptr(bf["state"]), 1.0, _lib.ptr(bf["image"]),
                   _lib.ptr(bf["contrib"]), _lib.ptr(bf["final_tau"]), st)
-        # overflow status -> pinned host word, read once the render's event fires
-        err, = _rt.cudaMemcpyAsync(self.status_host.data_ptr(), self.status.data_ptr(), 4,
+        # device status bits (bounded waits of the preprocess) into word 3
+        _lib.call("serve", "gsb_device_status_fetch", C.c_void_p(self.status.data_ptr() + 12), st)
+        # status words -> pinned host words, read once the render's event fires
+        err, = _rt.cudaMemcpyAsync(self.status_host.data_ptr(), self.status.data_ptr(), 16,
                                    _rt.cudaMemcpyKind.cudaMemcpyDeviceToHost, st.value)
         if err != _rt.cudaError_t.cudaSuccess:
             raise _lib.GsplatError(f"serve: status copy failed ({err})")
@@ -203,15 +212,16 @@ class PaletteServer:
     copy each finished image out of its slot (off for throughput runs)."""
 
     def __init__(self, hbm_budget, slots=4, device="cuda", use_graphs=True, K_max=8,
-                 capacity_margin=1.5, keep_images=True):
+                 capacity_margin=1.5, keep_images=True, alloc=None):
         self.device = torch.device(device)
+        self.last_admit_error = None
         self.keep_images = keep_images
         self.budget = int(hbm_budget)
         self.use_graphs = use_graphs
         self.margin = capacity_margin
         self.scenes = collections.OrderedDict()
         self.buckets = {}
-        self.slots = [_Slot(self.device, K_max) for _ in range(slots)]
+        self.slots = [_Slot(self.device, K_max, alloc) for _ in range(slots)]
         self.queue = collections.deque()
         self.done = []
         self.graph_captures = 0
@@ -256,12 +266,20 @@ class PaletteServer:
         for sl, s in zip(self.slots, saved):
             sl.sizes = s
         if self.resident_bytes() + scene.bytes + growth > self.budget:
+            self.last_admit_error = "over the HBM budget"
+            return False
+        try:
+            for b in buckets.values():
+                for sl in self.slots:
+                    sl.ensure(b)
+        except torch.OutOfMemoryError as e:
+            # a workspace could not be allocated: the scene is not admitted; slots
+            # that already grew keep their (larger, valid) buffers
+            self.last_admit_error = f"workspace allocation failed: {e}"
             return False
         self.scenes[scene.id] = scene
         self.buckets.update(buckets)
-        for b in buckets.values():
-            for sl in self.slots:
-                sl.ensure(b)
+        self.last_admit_error = None
         return True
 
     def evict_scene(self, scene_id):
@@ -357,6 +375,18 @@ class PaletteServer:
     def _retire(self, sl):
         req, b = sl.req, self.buckets[sl.req.bucket]
         sl.req = None
+        if int(sl.status_host[3]):
+            # a bounded wait of the render's preprocess ran out: its image is
+            # incomplete.  Clear the bits and report.
+            bits = int(sl.status_host[3])
+            sl.status_host[3] = 0
+            sl.status[3:].zero_()
+            cleared = C.c_uint32(0)
+            _lib.call("serve", "gsb_device_status", C.byref(cleared), 1,
+                      C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+            raise _lib.GsplatError(f"serve: request for scene {req.scene_id!r}: a bounded device "
+                                   f"wait ran out (status bits {bits:#x})",
+                                   _lib.GSB_ERR_DEVICE_TIMEOUT)
         status = int(sl.status_host[0])
         if status & (_lib.STATUS_PATCH_OVERFLOW | _lib.STATUS_DEPTH_KEY_OVERFLOW):
             if status & _lib.STATUS_DEPTH_KEY_OVERFLOW:

@@ -274,6 +274,37 @@ def test_bf16_full_weights_match_rounded_oracle(cuda_ok):
     np.testing.assert_allclose(np_of(w), o_w, rtol=1e-5, atol=2e-7)
 
 
+@pytest.mark.parametrize("nb,K,offset", [(9, 5, 0), (9, 3, 0), (16, 5, 1), (16, 3, 1), (4, 5, 1),
+                                         (9, 5, 1)])
+def test_bf16_sh_rows_odd_length_or_misaligned(cuda_ok, nb, K, offset):
+    """BF16 coefficient rows that the SH kernel cannot stage as 32-bit
+    element pairs -- an odd row length (nb*K = 45, 27, 15) or a base
+    address offset by one element (a contiguous view at an odd storage
+    offset) -- are read in place; results match the oracle on the same
+    BF16-rounded values.  FP32 arithmetic: 1e-5 relative."""
+    n = 3000
+    g = torch.Generator().manual_seed(100 + nb * 10 + K + offset)
+    vals = (torch.randn((n, nb * K), generator=g) * 0.2).to(torch.bfloat16)
+    if offset:
+        buf = torch.empty((n * nb * K + 1,), dtype=torch.bfloat16, device="cuda")
+        buf[1:] = vals.reshape(-1).cuda()
+        shs = buf[1:].view(n, nb * K)
+        assert shs.is_contiguous() and shs.data_ptr() % 4 == 2
+    else:
+        shs = vals.cuda()
+    sc, st = _scene(n, seed=41)
+    cam = _cam(64, 64, (1.0, -8.0, 0.5))
+    twc = orc.camera_arrays(cam, np.float32)[2]
+    if K == 3:
+        f, dsh, dpw = gsc.sh2Color(shs, st["pws"], cam.twc, True)
+    else:
+        f, dsh, dpw = gsc.sh2Weight(shs, st["pws"], cam.twc, True, K)
+    o_f, o_dsh, o_dpw = orc.sh2feat(vals.float().numpy(), sc["pws"], twc, K, True)
+    np.testing.assert_allclose(np_of(f), o_f, rtol=1e-5, atol=2e-7)
+    np.testing.assert_allclose(np_of(dsh), o_dsh, rtol=1e-5, atol=2e-7)
+    assert rel_err(dpw, o_dpw) < 1e-4
+
+
 def test_lab2rgb_matches_oracle(cuda_ok):
     g = torch.Generator().manual_seed(0)
     lab = torch.stack([torch.rand(40, 50, generator=g), torch.rand(40, 50, generator=g) * 160 - 80,

@@ -1,6 +1,12 @@
 """Scene files: the finetune checkpoint ``.npy`` and the ``.pply`` + ``.gswp``
-pair round-trip (CPU); on the GPU, a scene loaded from them renders like the
-same parameters passed directly."""
+pair round-trip (CPU); the writers produce the same bytes as the reference's
+converter (convert_npy_ply/palette_npy_to_pply.py:176-272) and the readers
+read its files (golden bytes in tests/golden/scene_formats.npz, made by
+tests/golden/make_scene_golden.py from the reference's own convert());
+on the GPU, a scene loaded from them renders like the same parameters passed
+directly."""
+import os
+import sys
 import numpy as np
 import pytest
 import torch
@@ -44,6 +50,43 @@ def test_checkpoint_and_pply_gswp_round_trip(tmp_path, low_rank):
     assert head[:4] == b"GSWP"
     assert np.frombuffer(head[4:], "<u4").tolist() == \
         [1, 500, 5, 16, int(low_rank), 5 if low_rank else 0, 15 if low_rank else 0]
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scene_formats.npz")
+
+
+def _golden_checkpoints():
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_scene_golden import checkpoints
+    return checkpoints()
+
+
+@pytest.mark.parametrize("name", ["dense", "lowrank"])
+def test_writers_match_reference_converter_bytes(tmp_path, name):
+    z = np.load(GOLDEN)
+    d = _golden_checkpoints()[name]
+    scene_io.write_pply(tmp_path / "s.pply", d)
+    scene_io.write_gswp(tmp_path / "s.gswp", d)
+    assert (tmp_path / "s.pply").read_bytes() == z[f"{name}_pply"].tobytes()
+    assert (tmp_path / "s.gswp").read_bytes() == z[f"{name}_gswp"].tobytes()
+
+
+@pytest.mark.parametrize("name", ["dense", "lowrank"])
+def test_readers_load_reference_converter_files(tmp_path, name):
+    z = np.load(GOLDEN)
+    d = _golden_checkpoints()[name]
+    (tmp_path / "r.pply").write_bytes(z[f"{name}_pply"].tobytes())
+    (tmp_path / "r.gswp").write_bytes(z[f"{name}_gswp"].tobytes())
+    r = scene_io.load_pply_gswp(tmp_path / "r.pply", tmp_path / "r.gswp")
+    assert np.array_equal(r["pw"], d["pw"]) and np.array_equal(r["rot"], d["rot"])
+    assert np.array_equal(r["palette"], d["palette"])
+    np.testing.assert_allclose(r["scale"], d["scale"], rtol=1e-6)
+    a = np.clip(np.asarray(d["alpha"]).reshape(-1), 1e-6, 1 - 1e-6)  # the converter's logit clip
+    np.testing.assert_allclose(r["alpha"], a, rtol=1e-5, atol=1e-6)
+    keys = ("low_shs_w", "high_shs_A", "high_shs_B") if d["low_rank"] else ("shs_w",)
+    for k in keys:
+        assert np.array_equal(r[k], d[k]), k
+    assert bool(r["low_rank"]) == d["low_rank"]
 
 
 def test_malformed_files_are_rejected(tmp_path):

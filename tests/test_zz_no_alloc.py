@@ -92,6 +92,29 @@ def test_static_sort_matches_workspace_sort_twice_in_a_row(cuda_ok):
     assert widths == [False, True]
 
 
+def test_static_sort_allocates_no_device_memory(cuda_ok):
+    """The defining property: after one warm-up call (which looks up the
+    array's address), a further call changes neither the device's free
+    memory nor what torch's caching allocator holds."""
+    n, W, H = 20000, 256, 256
+    state, plan, s = _packed(n, W, H, 11, 1.0)
+    M, tiles = int(plan.patches), ((W + 15) // 16) * ((H + 15) // 16)
+    gsid = torch.empty((M,), dtype=torch.int32, device="cuda")
+    ranges = torch.empty((tiles, 2), dtype=torch.int32, device="cuda")
+    args = (n, H, W, C.byref(plan), _lib.ptr(state), _lib.ptr(gsid), _lib.ptr(ranges), s)
+    _lib.call("sort_static", "gsb_splat_sort_static", *args)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    res0, alloc0 = torch.cuda.memory_reserved(), torch.cuda.memory_allocated()
+    _lib.call("sort_static", "gsb_splat_sort_static", *args)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_reserved() == res0 and torch.cuda.memory_allocated() == alloc0
+    g_ref, r_ref = _sort_with_workspace(n, W, H, state, plan, s)
+    assert torch.equal(gsid, g_ref) and torch.equal(ranges, r_ref)
+
+
 def test_static_sort_refuses_plans_beyond_its_array(cuda_ok):
     L = _lib.lib()
     n, W, H = 1000, 1920, 1080
