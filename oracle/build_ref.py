@@ -9,11 +9,13 @@ module name ``gsplatcu_ref`` (so it can be imported beside the drop-in
 ``gsplatcu``), targeting sm_100 SASS exactly as a ``TORCH_CUDA_ARCH_LIST=10.0``
 build of the reference would.  The reference's own ``setup.py`` is not run.
 
-It also stages the reference's unmodified Python caller -- ``gsplat/gsmodel.py``
-and the ``gsplat/utils.py`` it star-imports -- as the package
-``oracle/_ref/gsplat``, so that the drop-in test can run the reference's own
-autograd functions (``WeightGSFunctionTest`` / ``WeightGSFunctionFast``,
-``FinetuneModel``) on either ``gsplatcu`` build.
+It also stages, unmodified, the reference's Python caller --
+``gsplat/gsmodel.py`` and the ``gsplat/utils.py`` it star-imports -- and its
+numpy rasterizer ``gsplat/gausplat.py`` with the ``gsplat/sh_coef.py`` it
+imports, as the package ``oracle/_ref/gsplat``: the drop-in test runs the
+reference's own autograd functions (``WeightGSFunctionTest`` /
+``WeightGSFunctionFast``, ``FinetuneModel``) on either ``gsplatcu`` build,
+and the benchmark's reference arm times the numpy path on the host cores.
 
 The reference checkout is ``--root``, else ``$GSB_REFERENCE_ROOT``, else the
 build container's copy::
@@ -24,7 +26,7 @@ Output (git-ignored; it travels with the tree to the GPU box, where
 ``load_ref()`` / ``load_vanilla_ref()`` / ``reference_caller()`` use it
 without recompiling): ``oracle/_ref/gsplatcu_ref.so``, from the stage-1
 sources ``vanilla_3dgs/gsplatcu`` ``oracle/_ref/vanilla/gsplatcu_vanilla_ref.so``,
-and ``oracle/_ref/gsplat/{gsmodel,utils}.py``.
+and ``oracle/_ref/gsplat/{gsmodel,utils,gausplat,sh_coef}.py``.
 """
 import argparse
 import importlib.machinery
@@ -38,7 +40,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 REF_SO = os.path.join(REF_DIR, "gsplatcu_ref.so")
 CALLER_DIR = os.path.join(REF_DIR, "gsplat")
-CALLER_FILES = ("gsmodel.py", "utils.py")
+CALLER_FILES = ("gsmodel.py", "utils.py", "gausplat.py", "sh_coef.py")
 
 # The stage-1 (vanilla 3DGS) extension of the same project: its colour splat
 # backward carries the final-transmittance gradient (splat / splatB).
@@ -75,8 +77,9 @@ def build_vanilla(root=None, verbose=False):
 
 
 def stage_caller(root=None):
-    """Copy the reference's gsplat/gsmodel.py and gsplat/utils.py, byte for
-    byte, into oracle/_ref/gsplat (a namespace package, as in the reference)."""
+    """Copy the reference's gsplat/{gsmodel,utils,gausplat,sh_coef}.py, byte
+    for byte, into oracle/_ref/gsplat (a namespace package, as in the
+    reference)."""
     src = os.path.join(root or reference_root(), "gsplat")
     os.makedirs(CALLER_DIR, exist_ok=True)
     for f in CALLER_FILES:
@@ -109,6 +112,51 @@ def load_vanilla_ref():
     return _load("gsplatcu_vanilla_ref", VANILLA_SO)
 
 
+def _stub_matplotlib():
+    """gsplat/utils.py and gsplat/gausplat.py import matplotlib.pyplot for
+    plotting helpers the timed and tested paths never call; when matplotlib
+    is absent an empty stand-in is installed (its pause() is a no-op)."""
+    if "matplotlib" in sys.modules:
+        return
+    try:
+        import matplotlib  # noqa: F401
+    except ImportError:
+        mpl = types.ModuleType("matplotlib")
+        mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+        mpl.pyplot.pause = lambda *a, **k: None
+        sys.modules["matplotlib"], sys.modules["matplotlib.pyplot"] = mpl, mpl.pyplot
+
+
+def reference_numpy_path():
+    """The reference's numpy rasterizer module ``gsplat/gausplat.py``
+    (project, compute_cov_3d, compute_cov_2d, inverse_cov2d, sh2color,
+    splat), executed unchanged; None when it has not been staged."""
+    if not caller_staged():
+        return None
+    _stub_matplotlib()
+    saved = {k: sys.modules.get(k) for k in ("gsplat", "gsplat.sh_coef")}
+    try:
+        pkg = types.ModuleType("gsplat")
+        pkg.__path__ = [CALLER_DIR]
+        sys.modules["gsplat"] = pkg
+        sc_spec = importlib.util.spec_from_file_location(
+            "gsplat.sh_coef", os.path.join(CALLER_DIR, "sh_coef.py"))
+        sh_coef = importlib.util.module_from_spec(sc_spec)
+        sys.modules["gsplat.sh_coef"] = sh_coef
+        sc_spec.loader.exec_module(sh_coef)
+        spec = importlib.util.spec_from_file_location(
+            "gausplat_ref", os.path.join(CALLER_DIR, "gausplat.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        return mod
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
+
+
 def reference_caller(gsplatcu_module, tag):
     """The reference's own ``gsplat.gsmodel`` module, executed unchanged with
     ``import gsplatcu`` resolving to ``gsplatcu_module`` (this build's drop-in
@@ -119,13 +167,7 @@ def reference_caller(gsplatcu_module, tag):
     installed.  Returns None when the caller has not been staged."""
     if not caller_staged():
         return None
-    if "matplotlib" not in sys.modules:
-        try:
-            import matplotlib  # noqa: F401
-        except ImportError:
-            mpl = types.ModuleType("matplotlib")
-            mpl.pyplot = types.ModuleType("matplotlib.pyplot")
-            sys.modules["matplotlib"], sys.modules["matplotlib.pyplot"] = mpl, mpl.pyplot
+    _stub_matplotlib()
     saved = {k: sys.modules.get(k) for k in ("gsplatcu", "gsplat", "gsplat.utils")}
     try:
         sys.modules["gsplatcu"] = gsplatcu_module

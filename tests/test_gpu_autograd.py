@@ -1,12 +1,13 @@
-"""GPU tests of the autograd layer: WeightGSFunctionTest / WeightGSFunctionFast
-(reference semantics, gsplat/gsmodel.py:104-200) and the fused palette L1 loss,
-against torch / the CPU oracle."""
+"""GPU tests of the autograd layer: splat_palette_weights (the operator forward
+with the fused weight-parameter adjoint; the gradients of the reference's
+WeightGSFunctionTest / WeightGSFunctionFast, gsplat/gsmodel.py:104-200) and the
+fused palette L1 loss, against torch / the CPU oracle."""
 import numpy as np
 import pytest
 import torch
 
 from oracle import oracle as orc
-from palette_b200.autograd import WeightGSFunctionFast, WeightGSFunctionTest
+from palette_b200.weights import splat_palette_weights
 from palette_b200.loss import palette_image, palette_l1_loss
 from palette_b200.scene import look_at, synthetic_scene, to_torch
 from helpers import np_of, rel_err
@@ -48,7 +49,7 @@ def _oracle_grads(st, sc, cam, w, layer_grad):
 
 
 @pytest.mark.parametrize("rank", [1, 3])
-def test_weight_function_fast_gradients(cuda_ok, rank):
+def test_splat_palette_weights_lowrank_gradients(cuda_ok, rank):
     sc = synthetic_scene(6000, seed=60 + rank, mode="lowrank", rank=rank)
     st = to_torch(sc)
     cam = look_at((0.5, -7.5, 1.0), width=96, height=80)
@@ -56,8 +57,8 @@ def test_weight_function_fast_gradients(cuda_ok, rank):
     if rank == 1:
         A, B = A[:, :, 0].contiguous(), B[:, 0, :].contiguous()
     dc, A, B = st["dc"].requires_grad_(), A.requires_grad_(), B.requires_grad_()
-    layer, mask = WeightGSFunctionFast.apply(st["pws"], dc, A, B, st["alphas"], st["scales"],
-                                             st["rots"], cam, 5, 15)
+    layer, mask = splat_palette_weights(st["pws"], st["alphas"], st["scales"], st["rots"], cam,
+                                        dc=dc, A=A, B=B)
     G = torch.randn_like(layer)
     (layer * G).sum().backward()
     import gsplatcu as gsc
@@ -70,13 +71,13 @@ def test_weight_function_fast_gradients(cuda_ok, rank):
     assert mask.dtype == torch.bool and mask.shape == (6000,)
 
 
-def test_weight_function_test_gradients(cuda_ok):
+def test_splat_palette_weights_full_sh_gradients(cuda_ok):
     sc = synthetic_scene(6000, seed=70)
     st = to_torch(sc)
     cam = look_at((0.5, -7.5, 1.0), width=96, height=80)
     shs = st["shs"].requires_grad_()
-    layer, mask = WeightGSFunctionTest.apply(st["pws"], shs, st["alphas"], st["scales"], st["rots"],
-                                             cam, 5)
+    layer, mask = splat_palette_weights(st["pws"], st["alphas"], st["scales"], st["rots"], cam,
+                                        shs=shs)
     G = torch.randn_like(layer)
     (layer * G).sum().backward()
     import gsplatcu as gsc

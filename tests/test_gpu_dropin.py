@@ -98,6 +98,39 @@ def test_weight_function_fast_rank1(callers, n, W, H, seed):
         assert rel_err(ga, gb) < GRAD_TOL
 
 
+@pytest.mark.parametrize("mode", ["full", "lowrank"])
+def test_own_autograd_matches_reference_caller(callers, mode):
+    """palette_b200.weights.splat_palette_weights (operator forward, fused
+    weight-parameter adjoint) against the reference's own autograd function
+    on the reference build: same layers, same mask, same gradients."""
+    from palette_b200.weights import splat_palette_weights
+    n, W, H = 200000, 1920, 1080
+    s = _scene(n, 41, mode)
+    cam = look_at((1.5, -7.0, 2.0), width=W, height=H)
+    dl = torch.randn((5, H, W), device="cuda", generator=torch.Generator("cuda").manual_seed(4))
+    theirs = callers[1]
+    if mode == "full":
+        shs_a, shs_b = _leaf(s["shs"]), _leaf(s["shs"])
+        la, ma = splat_palette_weights(s["pws"], s["alphas"], s["scales"], s["rots"], cam, shs=shs_a)
+        lb, mb = theirs.WeightGSFunctionTest.apply(s["pws"], shs_b, s["alphas"], s["scales"],
+                                                   s["rots"], cam, 5)
+        pairs = [(shs_a, shs_b)]
+    else:
+        a = [_leaf(s[k]) for k in ("dc", "A", "B")]
+        b = [_leaf(s[k]) for k in ("dc", "A", "B")]
+        la, ma = splat_palette_weights(s["pws"], s["alphas"], s["scales"], s["rots"], cam,
+                                       dc=a[0], A=a[1], B=a[2])
+        lb, mb = theirs.WeightGSFunctionFast.apply(s["pws"], b[0], b[1], b[2], s["alphas"],
+                                                   s["scales"], s["rots"], cam, 5, 15)
+        pairs = list(zip(a, b))
+    la.backward(dl)
+    lb.backward(dl)
+    assert torch.equal(ma, mb)
+    assert max_abs(la, lb) < IMG_TOL
+    for x, y in pairs:
+        assert rel_err(x.grad, y.grad) < GRAD_TOL
+
+
 def _finetune_params(gm, s, low_rank):
     """The reference's own parameter set-up (get_finetune_params), then the
     synthetic scene's weights written into its leaf tensors, so that renders

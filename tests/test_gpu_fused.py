@@ -220,22 +220,39 @@ def test_fused_weights_only_backward(cuda_ok, mode, rank):
 
 @pytest.mark.parametrize("rank", [1, 3])
 def test_fused_weight_gradients_match_reference_backward(cuda_ok, rank):
-    """d dc, dA, dB equal the reference backward's (WeightGSFunctionFast,
-    gsplat/gsmodel.py:172-200, run through gsplatcu) up to FP32 summation order."""
-    from palette_b200.autograd import WeightGSFunctionFast
+    """d dc, dA, dB of the fused path equal the reference backward's formula
+    (gsplat/gsmodel.py:182-200: splat_weight_B, dc' = dW * dweight_ddc,
+    sh2Weight_fast_B) evaluated with the gsplatcu operators, and those of
+    splat_palette_weights, up to FP32 summation order."""
+    from palette_b200.weights import splat_palette_weights
     sc, st, cam = _setup("lowrank", rank, torch.float32, seed=40 + rank)
     (layer, ft, _), leaf = _render(st, cam, "lowrank", requires_grad=True,
                                    grad_names=["dc", "A", "B"])
     g = torch.randn(layer.shape, device="cuda", generator=torch.Generator("cuda").manual_seed(9))
     (layer * g).sum().backward()
-    ref_in = {k: st[k].detach().clone().requires_grad_(True) for k in ("dc", "A", "B")}
-    ref_layer, _ = WeightGSFunctionFast.apply(st["pws"], ref_in["dc"], ref_in["A"], ref_in["B"],
-                                             st["alphas"], st["scales"], st["rots"], cam, 5, 15)
-    ref_layer = ref_layer.reshape(layer.shape)
-    assert max_abs(ref_layer, layer) < IMG_TOL
-    (ref_layer * g).sum().backward()
+    # the reference's backward, written out with the operators
+    H, W = cam.height, cam.width
+    us, pcs, d = gsc.project(st["pws"], cam.Rcw, cam.tcw, cam.fx, cam.fy, cam.cx, cam.cy, False)
+    c3, = gsc.computeCov3D(st["rots"], st["scales"], d, False)
+    c2, = gsc.computeCov2D(c3, pcs, cam.Rcw, d, cam.fx, cam.fy, W, H, False)
+    w, ddc, ylm = gsc.sh2Weight_fast(st["dc"], st["A"], st["B"], st["pws"], cam.twc, True, 5, 15)
+    cinv, areas = gsc.inverseCov2D(c2, d, False)
+    ref_layer, contrib, rft, ranges, gsid = gsc.splat_weight(H, W, 5, us, cinv, st["alphas"], d, w,
+                                                             areas)
+    assert max_abs(ref_layer.reshape(layer.shape), layer) < IMG_TOL
+    dW, = gsc.splat_weight_B(H, W, 5, us, cinv, st["alphas"], d, w, contrib, rft, ranges, gsid,
+                             g.reshape(ref_layer.shape).contiguous())
+    dw = dW.squeeze(1)
+    dA, dB = gsc.sh2Weight_fast_B(st["A"], st["B"], ylm, dw, 5, 15)
+    expect = dict(dc=dw * ddc, A=dA, B=dB)
     for k in ("dc", "A", "B"):
-        assert rel_err(leaf[k].grad, ref_in[k].grad) < 1e-5, k
+        assert rel_err(leaf[k].grad, expect[k]) < 1e-5, k
+    ops_in = {k: st[k].detach().clone().requires_grad_(True) for k in ("dc", "A", "B")}
+    ol, _ = splat_palette_weights(st["pws"], st["alphas"], st["scales"], st["rots"], cam,
+                                  dc=ops_in["dc"], A=ops_in["A"], B=ops_in["B"])
+    (ol.reshape(layer.shape) * g).sum().backward()
+    for k in ("dc", "A", "B"):
+        assert rel_err(ops_in[k].grad, expect[k]) < 1e-5, k
 
 
 def test_fused_forward_overlapped_count_and_overflow(cuda_ok):
