@@ -1,28 +1,35 @@
 #!/usr/bin/env python
 """Benchmark of the palette-weight rasterizer on B200.
 
-Workload (one step): a finetune step of ReparamGS-Palette's low-rank fused
-path (WeightGSFunctionFast, gsplat/gsmodel.py:151-200) over 1,000,000
-synthetic Gaussians at 1920x1080 with rank-3 factors A [N,5,3], B [N,3,15]
-(P=5, Q=15, K=5, SH order 3, FP32 storage): forward through the gsplatcu
-operators (project, computeCov3D, computeCov2D, sh2Weight_fast, inverseCov2D,
-splat_weight), the finetune loss (finetune.py:356-389) against a seeded random
-target image -- L1 between the rendered weights and the target's barycentric
-weights in the palette, clamped to non-negative and renormalised, plus
-0.5 * mean(relu(-weights)) (one fused kernel, palette_b200.loss) -- and the
-backward (splat_weight_B, sh2Weight_fast_B; dc, A, B and palette gradients).
-`value` is whole-job fwd+bwd iterations per second with the scene resident
-in HBM; `frames_per_s` is the forward alone.  `multiview` is the
-differentiation workload on the same scene: steps of 8 views at 1920x1080
-from BF16 rank-3 factors, loss 0.8 L1 + 0.2 (1 - SSIM) + 0.5 mean(relu(-W))
-per view (fused render + fused loss kernel).
+Workload (one step): a finetune step of ReparamGS-Palette's low-rank path
+(WeightGSFunctionFast, gsplat/gsmodel.py:151-200) over 1,000,000 synthetic
+Gaussians at 1920x1080 with rank-3 factors A [N,5,3], B [N,3,15] (P=5, Q=15,
+K=5, SH order 3, FP32 storage): forward through the gsplatcu operators
+(project, computeCov3D, computeCov2D, sh2Weight_fast, inverseCov2D,
+splat_weight; palette_b200.weights.splat_palette_weights), the finetune loss
+(finetune.py:356-389) against a seeded random target image -- L1 between the
+rendered weights and the target's barycentric weights in the palette,
+clamped to non-negative and renormalised, plus 0.5 * mean(relu(-weights))
+(one fused kernel, palette_b200.loss) -- and the backward (splat_weight_B,
+then one kernel from dL/dweights to the dc, A, B gradients; palette
+gradient).  `value` is whole-job fwd+bwd iterations per second with the
+scene resident in HBM; `frames_per_s` is the forward alone; `fused_path` the
+same step through the one-kernel preprocess (palette_b200.render).
+`multiview` is the differentiation workload on the same scene: steps of 8
+views at 1920x1080 from BF16 rank-3 factors, loss 0.8 L1 + 0.2 (1 - SSIM) +
+0.5 mean(relu(-W)) per view (fused render + fused loss kernel).
+`gpu_baseline` times the reference's own gsplatcu extension (built from its
+sources) on the same GPU through the reference's own autograd functions,
+beside this build's paths on the same scenes, in a subprocess.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 N > 1 (under torchrun): independent replicas, one per GPU (the path has no
 exchange step); rank 0 prints the line with the max-over-ranks time.
 --impl reference times the reference algorithm's CPU implementation (the
-CPU oracle port) on this host's cores on a bounded sample of the same step.
+CPU oracle port, every tile of every step composited) on this host's cores,
+and, as a labelled extra, the reference's own numpy rasterizer
+(gsplat/gausplat.py) on the 20k-Gaussian 256x256 workload.
 """
 import argparse
 import datetime
@@ -49,7 +56,6 @@ METRIC = "1080p frames/s & fwd+bwd iters/s at 1M Gaussians; p50/p99 palette-edit
 # against the barycentric target of the target image in the palette, clamped
 # to non-negative and renormalised, plus the negative-weight penalty.
 LOSS = dict(clamp=True, lambda_pos=0.5, kind="l1")
-SAMPLE_TILE_STRIDE = 8  # CPU baseline composites every 8th tile and scales
 
 
 def parse():
@@ -64,8 +70,11 @@ def parse():
     ap.add_argument("--rank", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="length of the palette-edit serving stream (0: skip)")
+    ap.add_argument("--no-gpu-baseline", action="store_true",
+                    help="skip the reference-extension timing leg")
+    ap.add_argument("--gpu-baseline-leg", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-rate", type=float, default=400.0)
     ap.add_argument("--serve-scale", type=float, default=1.0,
                     help="scale of the resident scene sizes (1: 100k..3M)")
@@ -92,14 +101,14 @@ def make_workload(a, device):
 
 
 def step(wl, cam=None, target=None, backward=True):
-    from palette_b200.autograd import WeightGSFunctionFast
     from palette_b200.loss import palette_geo_loss
+    from palette_b200.weights import splat_palette_weights
     cam = cam or wl["cam"]
     target = wl["target"] if target is None else target
     for p in (wl["dc"], wl["A"], wl["B"], wl["chroma"]):
         p.grad = None
-    layer, _ = WeightGSFunctionFast.apply(wl["pws"], wl["dc"], wl["A"], wl["B"], wl["alphas"],
-                                          wl["scales"], wl["rots"], cam, wl["K"], wl["Q"])
+    layer, _ = splat_palette_weights(wl["pws"], wl["alphas"], wl["scales"], wl["rots"], cam,
+                                     dc=wl["dc"], A=wl["A"], B=wl["B"])
     loss = palette_geo_loss(layer, wl["chroma"], target, **LOSS)
     if backward:
         loss.backward()
@@ -300,11 +309,11 @@ def stage_breakdown(wl, reps=5):
             us, pcs, d = gsc.project(wl["pws"], cam.Rcw, cam.tcw, cam.fx, cam.fy, cam.cx, cam.cy, False)
             c3, = gsc.computeCov3D(wl["rots"], wl["scales"], d, False)
             c2, = gsc.computeCov2D(c3, pcs, cam.Rcw, d, cam.fx, cam.fy, W, H, False)
-            w, ddc, ylm = gsc.sh2Weight_fast(dc, A, B, wl["pws"], cam.twc, True, K, Q)
+            w, = gsc.sh2Weight_fast(dc, A, B, wl["pws"], cam.twc, False, K, Q)
             cinv, areas = gsc.inverseCov2D(c2, d, False)
-            return us, cinv, d, areas, w, ylm
+            return us, cinv, d, areas, w
         out["preprocess"] = timed(pre, reps, st) / reps
-        us, cinv, d, areas, w, ylm = pre()
+        us, cinv, d, areas, w = pre()
         n = us.shape[0]
         state = torch.empty(int(L.gsb_splat_state_bytes(n, K, H, W)), dtype=torch.uint8,
                             device=us.device)
@@ -343,13 +352,16 @@ def stage_breakdown(wl, reps=5):
             "bench", "gsb_splat_backward_packed", n, H, W, K, _lib.ptr(ranges), _lib.ptr(gsid),
             _lib.ptr(contrib), _lib.ptr(ft), _lib.ptr(g), None, _lib.ptr(state), _lib.ptr(dW), None,
             None, None, sp), reps, st) / reps
-        out["lowrank_backward"] = timed(lambda: gsc.sh2Weight_fast_B(A, B, ylm, dW[:, 0], K, Q),
-                                        reps, st) / reps
-        # fused path: one preprocess kernel (+ count scan), weights-only backward
         from palette_b200.render import camera_struct
         camst, _keep = camera_struct(cam)
         params = _lib.PaletteParams(_lib.WEIGHTS_LOWRANK, _lib.DTYPE_F32, K, 5, Q, int(A.shape[2]),
                                     dc.data_ptr(), A.data_ptr(), B.data_ptr())
+        gdc, gA, gB = torch.empty_like(dc), torch.empty_like(A), torch.empty_like(B)
+        out["weights_backward"] = timed(lambda: _lib.call(
+            "bench", "gsb_palette_weights_backward", n, C.byref(camst), _lib.ptr(wl["pws"]),
+            C.byref(params), _lib.ptr(dW), _lib.ptr(gdc), _lib.ptr(gA), _lib.ptr(gB), sp),
+            reps, st) / reps
+        # fused path: one preprocess kernel (+ count scan), weights-only backward
         fstate = torch.empty_like(state)
         out["fused_preprocess"] = timed(lambda: _lib.call(
             "bench", "gsb_render_preprocess", n, C.byref(camst), _lib.ptr(wl["pws"]),
@@ -357,7 +369,6 @@ def stage_breakdown(wl, reps=5):
             _lib.ptr(fstate), None, sp), reps, st) / reps
         scratch = torch.empty(int(L.gsb_render_backward_bytes(n, K)), dtype=torch.uint8,
                               device=us.device)
-        gdc, gA, gB = torch.empty_like(dc), torch.empty_like(A), torch.empty_like(B)
         out["fused_backward"] = timed(lambda: _lib.call(
             "bench", "gsb_render_backward", n, C.byref(camst), _lib.ptr(wl["pws"]),
             _lib.ptr(wl["rots"]), _lib.ptr(wl["scales"]), _lib.ptr(wl["alphas"]), C.byref(params),
@@ -417,7 +428,7 @@ def serve_bench(a, device):
     probes = [(c.Rcw.numpy(), c.tcw.numpy()) for c in
               (look_at(e, device="cpu") for e in sphere_poses(8, 6.0, seed=3))]
     free, _ = torch.cuda.mem_get_info(device)
-    srv = PaletteServer(hbm_budget=int(0.8 * free), slots=4, device=device, keep_images=False)
+    srv = PaletteServer(hbm_budget=int(0.8 * free), slots=8, device=device, keep_images=False)
     t0 = time.perf_counter()
     for sc in scenes:
         if not srv.admit_scene(sc, res, probes):
@@ -437,7 +448,9 @@ def serve_bench(a, device):
     t1 = time.perf_counter()
     srv.prepare(reqs)
     prep_s = time.perf_counter() - t1
+    n_batches0 = len(srv.batch_sizes)
     st = srv.run_open_loop(reqs, rate=a.serve_rate, seed=a.seed)
+    st["mean_batch"] = round(float(np.mean(srv.batch_sizes[n_batches0:])), 2)
     lat = {}
     for r in srv.done:
         for key in (r.tag[0], f"{r.tag[1]}px"):
@@ -445,11 +458,26 @@ def serve_bench(a, device):
     st["by_form"] = {k: dict(n=len(v), p50_ms=round(float(np.percentile(v, 50)), 3),
                              p99_ms=round(float(np.percentile(v, 99)), 3))
                      for k, v in sorted(lat.items())}
+    # saturation (closed loop): every request of one storage form queued at
+    # once, per form
+    sat = {}
+    for form in ("fp32", "bf16"):
+        sub = [Request(r.scene_id, r.Rcw.numpy(), r.tcw.numpy(), r.fx, r.fy, r.cx, r.cy, r.width,
+                       r.height, r.palette.numpy(), tag=r.tag)
+               for r in reqs if r.tag[0] == form][:600]
+        srv.run_closed_loop(sub[:50])  # warm
+        res = srv.run_closed_loop(sub)
+        sat[form] = dict(requests=res["requests"], frames_per_s=round(res["frames_per_s"], 1),
+                         mean_batch=round(res["mean_batch"], 2), reruns=res["reruns"])
+    st["saturation"] = sat
     st.update(scenes=len(scenes), gaussians=int(sum(s.n for s in scenes)),
               resident_gb=round(srv.resident_bytes() / 1e9, 2), slots=len(srv.slots),
               graphs=srv.graph_captures, seconds=a.serve_seconds, admit_s=round(admit_s, 1),
               capture_s=round(prep_s, 1),
-              latency="arrival to image complete in HBM; camera/palette H2D per request")
+              latency="arrival to image complete in HBM; camera/palette H2D per request",
+              path=("per-request preparation graphs (fused preprocess + capacity sort) on 8 "
+                    "slot streams; prepared requests composited together by one persistent "
+                    "kernel per batch (captured graph, up to 3 batches in flight on their own streams)"))
     for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "frames_per_s"):
         st[k] = round(st[k], 3)
     del srv, scenes
@@ -458,63 +486,80 @@ def serve_bench(a, device):
 
 
 # ----------------------------------------------------------- CPU baseline
-def cpu_step(wl, orc, stride):
-    """One bounded sample of the step on the host cores (CPU oracle, FP32;
-    the loss in FP64): full preprocess and binning of all Gaussians; forward
-    compositing, loss and adjoint compositing of every `stride`-th tile.  Returns extrapolated seconds for
-    one full step and the sample's own seconds."""
+def cpu_step(wl, orc):
+    """One full step on the host cores (CPU oracle, FP32; the loss in FP64):
+    preprocess and binning of all Gaussians, compositing of every tile, the
+    loss on every pixel, the compositing adjoint and the factor gradients.
+    Returns its seconds."""
     sc, cam, K, Q = wl["sc"], wl["cam"], wl["K"], wl["Q"]
     H, W = cam.height, cam.width
     t0 = time.perf_counter()
     pre = orc.preprocess(sc["pws"], sc["rots"], sc["scales"], cam, np.float32)
     w, _, ylm = orc.sh2weight_fast(sc["dc"], sc["A"], sc["B"], sc["pws"], pre["twc"], K, Q, True)
     b = orc.bin_gaussians(pre["us"], pre["areas"], pre["depths"], H, W)
-    t1 = time.perf_counter()
-    ranges = b["ranges"].copy()
-    keep = np.zeros(len(ranges), bool)
-    keep[::stride] = True
-    ranges[~keep] = 0
-    out, contrib, ft = orc.draw(H, W, K, ranges, b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w, 0.0)
-    # the loss and its gradients on the composited tiles' pixels
-    gx = (W + 15) // 16
-    mask = np.zeros((H, W), bool)
-    for t in np.flatnonzero(keep):
-        ty, tx = divmod(int(t), gx)
-        mask[ty * 16:(ty + 1) * 16, tx * 16:(tx + 1) * 16] = True
+    out, contrib, ft = orc.draw(H, W, K, b["ranges"], b["gsid"], pre["us"], pre["cinv"],
+                                sc["alphas"], w, 0.0)
     tgt = wl["target_host"].numpy()
-    lo = orc.palette_geo_loss(out[:, mask][:, None, :], tgt[:, mask][:, None, :],
-                              sc["palette"][2:], **LOSS)
-    dlayer = np.zeros_like(out)
-    dlayer[:, mask] = lo["dlayer"][:, 0, :]
-    g = orc.draw_backward(H, W, K, ranges, b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w, ft,
-                          contrib, dlayer)
-    t2 = time.perf_counter()
+    lo = orc.palette_geo_loss(out, tgt, sc["palette"][2:], **LOSS)
+    g = orc.draw_backward(H, W, K, b["ranges"], b["gsid"], pre["us"], pre["cinv"], sc["alphas"], w,
+                          ft, contrib, lo["dlayer"].astype(np.float32))
     orc.sh2weight_fast_b(sc["A"], sc["B"], ylm, g["dfeat"], K, Q)
-    t3 = time.perf_counter()
-    frac = keep.sum() / len(keep)
-    full = (t1 - t0) + (t2 - t1) / frac + (t3 - t2)
-    return full, t3 - t0
+    return time.perf_counter() - t0
 
 
 def cpu_baseline(wl, steps, warmup):
     from oracle import oracle as orc
     orc.set_threads(os.cpu_count() or 1)
     for _ in range(max(0, warmup)):
-        cpu_step(wl, orc, SAMPLE_TILE_STRIDE)
-    fulls, samples = [], []
-    for _ in range(max(1, steps)):
-        f, s = cpu_step(wl, orc, SAMPLE_TILE_STRIDE)
-        fulls.append(f)
-        samples.append(s)
-    v = 1.0 / statistics.median(fulls)
+        cpu_step(wl, orc)
+    secs = [cpu_step(wl, orc) for _ in range(max(1, steps))]
+    v = len(secs) / sum(secs)
     return dict(value=v, unit="iters/s", cores=orc.get_threads(), kind="port",
                 sample=(f"CPU oracle (FP32, from-scratch restatement of gsplatcu's kernels) on "
-                        f"{orc.get_threads()} host threads: full preprocess + binning of all "
-                        f"{wl['sc']['pws'].shape[0]} Gaussians, forward+adjoint compositing of every "
-                        f"{SAMPLE_TILE_STRIDE}th tile scaled x{SAMPLE_TILE_STRIDE}; "
-                        f"{len(fulls)} timed samples, median; sample wall "
-                        f"{statistics.median(samples):.1f}s"),
-                ms_per_step=1000.0 / v)
+                        f"{orc.get_threads()} host threads: {len(secs)} full steps (all "
+                        f"{wl['sc']['pws'].shape[0]} Gaussians preprocessed and binned, every "
+                        f"tile composited forward and backward, the loss on every pixel), "
+                        f"{sum(secs):.1f} s timed after {max(0, warmup)} warm-up steps"),
+                ms_per_step=1000.0 * sum(secs) / len(secs), seconds=sum(secs))
+
+
+def numpy_reference_forward(seed=0):
+    """The reference's own numpy rasterizer (gsplat/gausplat.py, executed
+    unchanged from oracle/_ref) on the 20k-Gaussian, 256x256 workload: project
+    -> compute_cov_3d -> compute_cov_2d -> inverse_cov2d, the SH weights by its
+    sh2color (3 channels at a time, so twice for K = 5; it adds its +0.5 bias),
+    then splat twice (it is fixed at 3 channels).  Single-threaded numpy; its
+    maths differs from the CUDA extension (a timing baseline, not an oracle).
+    Returns None when the numpy path is not staged."""
+    import contextlib
+    import io
+    from oracle.build_ref import reference_numpy_path
+    from palette_b200.scene import look_at, synthetic_scene
+    gp = reference_numpy_path()
+    if gp is None:
+        return None
+    n, W, H = 20000, 256, 256
+    sc = synthetic_scene(n, seed=seed, mode="full")
+    cam = look_at((0.0, -8.0, 0.0), width=W, height=H, device="cpu")
+    R, t = cam.Rcw.numpy().astype(np.float64), cam.tcw.numpy().astype(np.float64)
+    twc = -R.T @ t
+    shs = sc["shs"].reshape(n, 16, 5).astype(np.float64)
+    # the numpy path's colour layout: band b, channel c at 3 b + c
+    groups = [shs[:, :, 0:3], np.concatenate([shs[:, :, 3:5], np.zeros((n, 16, 1))], 2)]
+    t0 = time.perf_counter()
+    with contextlib.redirect_stdout(io.StringIO()):
+        u, pc = gp.project(sc["pws"].astype(np.float64), R, t, cam.fx, cam.fy, cam.cx, cam.cy)
+        cov3 = gp.compute_cov_3d(sc["scales"].astype(np.float64), sc["rots"].astype(np.float64))
+        cov2 = gp.compute_cov_2d(pc, cam.fx, cam.fy, W, H, cov3, R)
+        cinv, areas = gp.inverse_cov2d(cov2)
+        alpha = sc["alphas"].reshape(-1).astype(np.float64)
+        for g in groups:
+            col = gp.sh2color(g.reshape(n, 48), sc["pws"].astype(np.float64), twc)
+            gp.splat(H, W, u, cinv, alpha, pc[:, 2], col, areas)
+    sec = time.perf_counter() - t0
+    return dict(workload=f"{n} Gaussians, {W}x{H}, full SH weights K=5 (forward only)",
+                forward_s=round(sec, 3), frames_per_s=round(1.0 / sec, 4), threads=1,
+                source="gsplat/gausplat.py of the reference, unchanged")
 
 
 # ------------------------------------------------------------------- arms
@@ -524,14 +569,144 @@ def run_reference(a):
         return
     wl = make_workload(a, torch.device("cpu"))
     cb = cpu_baseline(wl, a.steps, a.warmup)
+    try:
+        npy = numpy_reference_forward(a.seed)
+    except Exception as e:  # a labelled extra: report, never fail the arm
+        npy = dict(error=f"{type(e).__name__}: {e}")
     line = dict(metric=METRIC, value=cb["value"], unit="iters/s", n_gpus=a.gpus, steps=a.steps,
                 warmup=a.warmup, ms_per_step=cb["ms_per_step"], higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
                 config=config(a), impl="reference",
                 cpu_baseline={k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                timed_seconds=round(cb["seconds"], 2),
                 e2e=dict(value=cb["value"], unit="iters/s", h2d_bytes_per_step=0,
-                         d2h_bytes_per_step=0))
+                         d2h_bytes_per_step=0),
+                numpy_reference=npy)
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------- reference extension leg
+def _per_call_ms(fn, warmup=20, reps=200):
+    """Median device time (ms) of one call of fn, CUDA events around each call
+    on the current stream, synchronised after each call (the reference's
+    operators synchronise inside every call anyway)."""
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = []
+    for _ in range(reps):
+        s.record(st)
+        fn()
+        e.record(st)
+        e.synchronize()
+        out.append(s.elapsed_time(e))
+    return statistics.median(out)
+
+
+def gpu_baseline_leg(a):
+    """Run in a subprocess of the b200 arm (so that the reference extension is
+    never loaded into the timed process): time the reference's own gsplatcu
+    extension, built from its sources, through the reference's own autograd
+    functions (gsplat/gsmodel.py WeightGSFunctionTest for full SH weights,
+    WeightGSFunctionFast for rank-1 factors -- the only rank it supports),
+    forward and forward + backward (dL/dlayer a fixed random image), on the
+    bench scene's Gaussians and camera; beside it, on the same scenes and with
+    the same method, this build through the same reference caller (drop-in),
+    through palette_b200.weights (operator forward, fused weight adjoint) and
+    through palette_b200.render (fused preprocess, weights-only adjoint).
+    Prints one JSON line."""
+    import gsplatcu
+    from oracle.build_ref import load_ref, reference_caller
+    from palette_b200.render import render_palette
+    from palette_b200.scene import look_at, synthetic_scene
+    from palette_b200.weights import splat_palette_weights
+    ref = load_ref()
+    gm_ref = reference_caller(ref, "ref") if ref is not None else None
+    if gm_ref is None:
+        print(json.dumps(dict(unavailable="reference build or caller missing under oracle/_ref")))
+        return
+    gm_b200 = reference_caller(gsplatcu, "b200")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    W, H, n = a.width, a.height, a.gaussians
+    cam = look_at((0.0, -8.0, 0.0), width=W, height=H, device=dev)
+    G = torch.randn((5, H, W), device=dev, generator=torch.Generator(dev).manual_seed(a.seed))
+    clocks = ClockSampler(0)
+    clocks.start()
+    res = {}
+    for form in ("full_sh", "rank1"):
+        sc = synthetic_scene(n, seed=a.seed, mode="full" if form == "full_sh" else "lowrank",
+                             rank=1)
+        t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        geo = (t(sc["pws"]), t(sc["alphas"]), t(sc["scales"]), t(sc["rots"]))
+        pws, alphas, scales, rots = geo
+        if form == "full_sh":
+            shs = t(sc["shs"]).requires_grad_()
+            leaves = [shs]
+            calls = {
+                "reference": lambda gm=gm_ref: gm.WeightGSFunctionTest.apply(
+                    pws, shs, alphas, scales, rots, cam, 5)[0],
+                "dropin": lambda gm=gm_b200: gm.WeightGSFunctionTest.apply(
+                    pws, shs, alphas, scales, rots, cam, 5)[0],
+                "ops": lambda: splat_palette_weights(pws, alphas, scales, rots, cam, shs=shs)[0],
+                "fused": lambda: render_palette(pws, rots, scales, alphas, cam, shs=shs)[0],
+            }
+        else:
+            dc, A, B = (t(sc["dc"]).requires_grad_(), t(sc["A"][:, :, 0]).requires_grad_(),
+                        t(sc["B"][:, 0, :]).requires_grad_())
+            leaves = [dc, A, B]
+            calls = {
+                "reference": lambda gm=gm_ref: gm.WeightGSFunctionFast.apply(
+                    pws, dc, A, B, alphas, scales, rots, cam, 5, 15)[0],
+                "dropin": lambda gm=gm_b200: gm.WeightGSFunctionFast.apply(
+                    pws, dc, A, B, alphas, scales, rots, cam, 5, 15)[0],
+                "ops": lambda: splat_palette_weights(pws, alphas, scales, rots, cam, dc=dc, A=A,
+                                                     B=B)[0],
+                "fused": lambda: render_palette(pws, rots, scales, alphas, cam, dc=dc, A=A,
+                                                B=B)[0],
+            }
+        out = {}
+        for name, fwd in calls.items():
+            def fwd_only(fwd=fwd):
+                with torch.no_grad():
+                    fwd()
+
+            def fwd_bwd(fwd=fwd):
+                for x in leaves:
+                    x.grad = None
+                fwd().backward(G.reshape(5, H, W))
+            out[name] = dict(forward_ms=round(_per_call_ms(fwd_only), 4),
+                             fwd_bwd_ms=round(_per_call_ms(fwd_bwd), 4))
+        r = out["reference"]
+        for name in ("dropin", "ops", "fused"):
+            out[name]["forward_speedup"] = round(r["forward_ms"] / out[name]["forward_ms"], 2)
+            out[name]["fwd_bwd_speedup"] = round(r["fwd_bwd_ms"] / out[name]["fwd_bwd_ms"], 2)
+        res[form] = out
+        del sc, geo, leaves, calls
+        torch.cuda.empty_cache()
+    res["clocks"] = clocks.stop()
+    res["method"] = ("median of 200 per-call CUDA-event times after 20 warm-up calls; forward: "
+                     "layer under no_grad; fwd_bwd: layer.backward(fixed random dL/dlayer)")
+    res["workload"] = f"{n} Gaussians, {W}x{H}, K=5, camera at distance 8"
+    print(json.dumps(res), flush=True)
+
+
+def run_gpu_baseline(a):
+    """The reference-extension leg in a subprocess; its JSON, or a reason."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--gpu-baseline-leg",
+           "--gaussians", str(a.gaussians), "--width", str(a.width), "--height", str(a.height),
+           "--seed", str(a.seed)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return dict(unavailable="reference-extension leg timed out")
+    lines = [x for x in r.stdout.strip().splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return dict(unavailable=f"reference-extension leg failed (rc {r.returncode}): "
+                                f"{r.stderr.strip().splitlines()[-1:] }")
+    return json.loads(lines[-1])
 
 
 def config(a):
@@ -661,8 +836,11 @@ def run_b200(a):
 
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cb = cpu_baseline(wl, steps=8, warmup=1)
+        cb = cpu_baseline(wl, steps=3, warmup=1)
         cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    gb = None
+    if rank == 0 and world == 1 and not a.no_gpu_baseline:
+        gb = run_gpu_baseline(a)
     if rank == 0:
         line = dict(metric=METRIC, value=round(value, 3), unit="iters/s", n_gpus=world,
                     steps=a.steps, warmup=a.warmup, ms_per_step=round(ms_per_step, 4),
@@ -682,7 +860,7 @@ def run_b200(a):
                                    steps=mv_reps, ms_per_step=round(mv_ms, 4),
                                    iters_per_s=round(world * 1000.0 / mv_ms, 3),
                                    views_per_s=round(world * VIEWS * 1000.0 / mv_ms, 2)),
-                    serving=serving,
+                    serving=serving, gpu_baseline=gb,
                     stages_ms={k: round(v, 4) for k, v in stages.items()},
                     patches=alg["M"],
                     # sort throughput and the compositing's nominal pixel work
@@ -697,7 +875,9 @@ def run_b200(a):
 
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.gpu_baseline_leg:
+        gpu_baseline_leg(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_b200(a)

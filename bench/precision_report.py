@@ -12,7 +12,14 @@ errors are taken over those tiles: max / mean abs error of the K-channel
 weight image and of the palette colour image, and PSNR (peak 1).  Gradients:
 for the first `--grad-poses` poses, every parameter group's relative error
 ||g - g64|| / ||g64|| of the full adjoint against the oracle's FP64 chain
-rule, with dL/dlayer random on the sampled tiles and zero elsewhere.
+rule, with dL/dlayer random on the sampled tiles and zero elsewhere -- and
+split in two: pixels where the FP32 render and the FP64 oracle take a
+different discrete decision (a Gaussian skipped at alpha' < 0.002 in one and
+blended in the other, or the T < 1e-4 stop at a different Gaussian: the
+contributor index differs, or the final transmittance differs by more than
+1e-4 relative, far above FP32 rounding) are found, dL/dlayer is zeroed on
+them, and the relative error recomputed: that is the arithmetic part, the
+rest is the decision (threshold-flip) part.
 
 Not collected by pytest (it is a report, minutes of CPU time): run it on a
 GPU box and keep the printed JSON.
@@ -106,18 +113,37 @@ def main():
                                                   lists=lists, dout=dout)
                 pairs = dict(pws="dpws", rots="drots", scales="dscales", alphas="dalphas",
                              shs="dshs")
+                # pixels whose discrete decisions differ between the FP32 render
+                # and the FP64 oracle
+                from palette_b200.render import _render_one, _weight_args
+                w0, A_, B_, md, K_, P_, Q_, rk = _weight_args(st32["shs"], None, None, None, K)
+                with torch.no_grad():
+                    _l, ft32, _d, _s, _r, _g, c32 = _render_one(
+                        st32["pws"], st32["rots"], st32["scales"], st32["alphas"], w0, A_, B_,
+                        cam, md, K_, P_, Q_, rk)
+                c32, ft32 = c32.cpu().numpy(), ft32.double().cpu().numpy()
+                flip = (c32 != o["contrib"]) | (np.abs(ft32 - o["final_tau"]) >
+                                                1e-4 * np.maximum(np.abs(o["final_tau"]), 1e-6))
+                flip &= mask
+                dout_ar = dout * ~flip
+                g64_ar = orc.render_weights_backward(f64["pws"], f64["rots"], f64["scales"],
+                                                     f64["alphas"], cam, twc, K, shs=f64["shs"],
+                                                     lists=lists, dout=dout_ar)
                 for name, st in (("fp32", st32), ("bf16", st16)):
-                    leaves = {k: st[k].detach().clone().requires_grad_(True) for k in pairs}
-                    layer, _, _ = render_palette(leaves["pws"], leaves["rots"], leaves["scales"],
-                                                 leaves["alphas"], cam, shs=leaves["shs"])
-                    layer.backward(torch.from_numpy(dout.astype(np.float32)).cuda())
-                    rel = {}
-                    for k, gk in pairs.items():
-                        g = leaves[k].grad.double().cpu().numpy().reshape(len(g64[gk]), -1)
-                        r = g64[gk].reshape(len(g), -1)
-                        rel[k] = float(np.linalg.norm(g - r) / max(np.linalg.norm(r), 1e-300))
-                    report["gradients"].append(dict(storage=name, width=W, height=H, pose=pi,
-                                                    rel_err=rel))
+                    rel, rel_ar = {}, {}
+                    for d_out, ref, out in ((dout, g64, rel), (dout_ar, g64_ar, rel_ar)):
+                        leaves = {k: st[k].detach().clone().requires_grad_(True) for k in pairs}
+                        layer, _, _ = render_palette(leaves["pws"], leaves["rots"], leaves["scales"],
+                                                     leaves["alphas"], cam, shs=leaves["shs"])
+                        layer.backward(torch.from_numpy(d_out.astype(np.float32)).cuda())
+                        for k, gk in pairs.items():
+                            g = leaves[k].grad.double().cpu().numpy().reshape(len(ref[gk]), -1)
+                            r = ref[gk].reshape(len(g), -1)
+                            out[k] = float(np.linalg.norm(g - r) / max(np.linalg.norm(r), 1e-300))
+                    report["gradients"].append(dict(
+                        storage=name, width=W, height=H, pose=pi, rel_err=rel,
+                        rel_err_arithmetic=rel_ar, flipped_pixels=int(flip.sum()),
+                        sampled_pixels=int(mask.sum())))
         summ = {}
         for name, rs in rows.items():
             summ[name] = {

@@ -377,6 +377,39 @@ int gsb_palette_weights_backward(int64_t n, const gsb_camera* cam, const float* 
                                  const gsb_palette_params* params, const float* dloss_dweights,
                                  float* dw0, float* dA, float* dB, void* stream);
 
+/* ------------------------------------------------ batched compositing
+ * Several images' compositing in one persistent kernel (the serving loop's
+ * batches of palette-edit renders; no counterpart in the reference, which
+ * renders one request per call).  Each image is described by its packed
+ * state (gsb_render_preprocess or gsb_splat_pack), sorted tile lists and
+ * output buffers; all images of a batch carry the same channel count.  The
+ * caller packs a batch into a host table (gsb_draw_batch_pack, host code
+ * only), copies it to a device buffer of gsb_draw_batch_bytes(max_jobs)
+ * bytes (16-byte aligned) and launches gsb_draw_batch on that buffer.  The
+ * kernel's blocks claim (image, tile) items from the table's queue with an
+ * atomic counter, so tiles of large and small images share the SMs; each
+ * tile is composited exactly as gsb_splat_draw composites it (results are
+ * bit-identical to rendering the images one by one).  The copy and the
+ * launch can be captured in a CUDA graph: replaying the graph copies the
+ * host table's current contents.  A device buffer must not be reused for
+ * another batch before the kernel reading it has finished. */
+typedef struct gsb_draw_job {
+  const void* state;      /* packed state: gsb_splat_state_bytes(n, channels, height, width) */
+  int64_t n;              /* Gaussians of the image                                        */
+  int height, width;
+  int channels;           /* record channels (equal for every job of a batch)              */
+  const int32_t* ranges;  /* [tiles,2] tile ranges of the sorted lists                     */
+  const int32_t* gsid;    /* sorted Gaussian ids                                           */
+  float tau_init;         /* final_tau of empty tiles: 0 (weights) or 1 (colours)          */
+  float* out;             /* [channels,height,width]                                       */
+  int32_t* contrib;       /* [height,width]                                                */
+  float* final_tau;       /* [height,width]                                                */
+} gsb_draw_job;
+size_t gsb_draw_batch_bytes(int max_jobs);
+int gsb_draw_batch_pack(const gsb_draw_job* jobs, int njobs, void* host_table,
+                        size_t table_bytes);
+int gsb_draw_batch(const void* dev_table, int channels, void* stream);
+
 /* Scratch bytes gsb_render_backward needs for the per-Gaussian screen-space
  * gradients. */
 size_t gsb_render_backward_bytes(int64_t n, int K);

@@ -603,7 +603,8 @@ namespace {
 // the caller's initial values (final_tau is 0 for weights, 1 for colours).
 template <typename R>
 void draw(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const R* us,
-          const R* cinv, const R* alphas, const R* feat, R* out, int32_t* contrib, R* final_tau) {
+          const R* cinv, const R* alphas, const R* feat, R* out, int32_t* contrib, R* final_tau,
+          int32_t* blends = nullptr) {
   int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   parallel_for((int64_t)gx * gy, [&](int64_t b, int64_t e) {
     std::vector<R> acc(K);
@@ -615,7 +616,7 @@ void draw(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const
         for (int px = tx * kTile; px < std::min(W, tx * kTile + kTile); ++px) {
           std::fill(acc.begin(), acc.end(), R(0));
           R T = 1;
-          int32_t cont = 0;
+          int32_t cont = 0, nblend = 0;
           for (int32_t j = s; j < en; ++j) {
             int32_t g = gsid[j];
             R dx = us[2 * g] - (R)px, dy = us[2 * g + 1] - (R)py;
@@ -626,6 +627,7 @@ void draw(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const
             R ta = T * ap;
             for (int k = 0; k < K; ++k) acc[k] += ta * feat[(int64_t)g * K + k];
             cont = j - s + 1;
+            ++nblend;
             T *= (R(1) - ap);
             if (T < (R)kTransMin) break;
           }
@@ -633,6 +635,7 @@ void draw(int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const
           for (int k = 0; k < K; ++k) out[(int64_t)k * H * W + pix] = acc[k];
           contrib[pix] = cont;
           final_tau[pix] = T;
+          if (blends) blends[pix] = nblend;
         }
     }
   }, 1);
@@ -770,6 +773,15 @@ DEF_BOTH(oracle_sh2weight_lowrank_b, SIG_LRB, CALL_LRB)
    const R* alphas, const R* feat, R* out, int32_t* contrib, R* final_tau)
 #define CALL_DRAW(R) draw<R>(H, W, K, ranges, gsid, us, cinv, alphas, feat, out, contrib, final_tau);
 DEF_BOTH(oracle_draw, SIG_DRAW, CALL_DRAW)
+
+// Forward compositing (FP32) that also counts, per pixel, the Gaussians
+// blended into it (the (pixel, Gaussian) pairs the adjoint revisits).
+ORACLE_EXPORT void oracle_draw_count_f32(int H, int W, int K, const int32_t* ranges,
+                                         const int32_t* gsid, const float* us, const float* cinv,
+                                         const float* alphas, const float* feat, float* out,
+                                         int32_t* contrib, float* final_tau, int32_t* blends) {
+  draw<float>(H, W, K, ranges, gsid, us, cinv, alphas, feat, out, contrib, final_tau, blends);
+}
 
 #define SIG_DRAWB(R)                                                                             \
   (int H, int W, int K, const int32_t* ranges, const int32_t* gsid, const R* us, const R* cinv, \

@@ -225,6 +225,22 @@ def draw(H, W, K, ranges, gsid, us, cinv, alphas, feat, tau_init, dtype=np.float
     return [out, contrib, ft]
 
 
+def draw_count(H, W, K, ranges, gsid, us, cinv, alphas, feat, tau_init):
+    """draw() in FP32 plus the per-pixel number of blended Gaussians; returns
+    [out, contrib, final_tau, blends [H,W] int32]."""
+    us, cinv, feat = (_arr(x, np.float32) for x in (us, cinv, feat))
+    alphas = _arr(alphas, np.float32).reshape(-1)
+    ranges, gsid = _arr(ranges, np.int32), _arr(gsid, np.int32)
+    out = np.zeros((K, H, W), np.float32)
+    contrib = np.zeros((H, W), np.int32)
+    ft = np.full((H, W), tau_init, np.float32)
+    blends = np.zeros((H, W), np.int32)
+    lib().oracle_draw_count_f32(C.c_int(H), C.c_int(W), C.c_int(K), _p(ranges), _p(gsid), _p(us),
+                                _p(cinv), _p(alphas), _p(feat), _p(out), _p(contrib), _p(ft),
+                                _p(blends))
+    return [out, contrib, ft, blends]
+
+
 def draw_backward(H, W, K, ranges, gsid, us, cinv, alphas, feat, final_tau, contrib, dout,
                   dT=None, dtype=np.float32):
     """Adjoint of draw(); returns dict(dfeat [N,K], dalpha [N], du [N,2], dconic [N,3])."""

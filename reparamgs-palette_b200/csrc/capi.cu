@@ -2,6 +2,7 @@
 // argument validation, workspace carving and kernel launches.  No entry point
 // allocates device memory or synchronises, except gsb_splat_counts, which
 // must return the patch count to the host.
+#include <mutex>
 #include <cmath>
 #include <atomic>
 #include <cstdarg>
@@ -78,20 +79,70 @@ GSB_API const char* gsb_last_error(void) { return g_err; }
 GSB_API int gsb_version(void) { return 100; }
 GSB_API int gsb_device_status(uint32_t* status, int clear, void* stream) {
   GSB_CHECK_ARG(status, "device_status: null pointer");
-  uint32_t a = 0, b = 0;
+  uint32_t a = 0, b = 0, c = 0;
   int rc = lowrank_status(&a, clear != 0, ST(stream));
   if (rc) return rc;
   rc = fused_status(&b, clear != 0, ST(stream));
   if (rc) return rc;
-  *status = a | b;
+  rc = raster_status(&c, clear != 0, ST(stream));
+  if (rc) return rc;
+  *status = a | b | c;
   return GSB_OK;
+}
+
+// The device addresses of the status words of the files whose kernels wait
+// on bulk copies (low-rank weights, fused preprocess / adjoint, compositing),
+// looked up once per device and CUDA context.
+struct StatusWords {
+  unsigned long long ctx;
+  const uint32_t* w[3];
+};
+static StatusWords g_status_words[64];
+static std::mutex g_status_mutex;
+
+static int status_words(const uint32_t** w) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("device_status_fetch", 0);
+  if (dev < 0 || dev >= 64) {
+    set_error("device_status_fetch: device %d beyond the 64 supported", dev);
+    return GSB_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_status_mutex);
+  const unsigned long long ctx = current_context_id();
+  StatusWords& e = g_status_words[dev];
+  if (!e.w[0] || ctx == 0 || e.ctx != ctx) {
+    e.w[0] = lowrank_status_word();
+    e.w[1] = fused_status_word();
+    e.w[2] = raster_status_word();
+    e.ctx = ctx;
+    if (!e.w[0] || !e.w[1] || !e.w[2]) {
+      e.w[0] = nullptr;
+      set_error("device_status_fetch: cudaGetSymbolAddress failed on device %d", dev);
+      return GSB_ERR_CUDA;
+    }
+  }
+  for (int k = 0; k < 3; ++k) w[k] = e.w[k];
+  return GSB_OK;
+}
+
+// ORs the three status words into *out (device memory or mapped host
+// memory; one thread, so the read-modify-write of *out is not shared).  The
+// words themselves are left set: only gsb_device_status clears them.
+__global__ void k_status_fetch(const uint32_t* a, const uint32_t* b, const uint32_t* c,
+                               uint32_t* out) {
+  pdl_wait();
+  const uint32_t v = *(const volatile uint32_t*)a | *(const volatile uint32_t*)b |
+                     *(const volatile uint32_t*)c;
+  if (v) *(volatile uint32_t*)out |= v;
 }
 
 GSB_API int gsb_device_status_fetch(uint32_t* out, void* stream) {
   GSB_CHECK_ARG(out, "device_status_fetch: null pointer");
-  int rc = lowrank_status_fetch(out, ST(stream));
+  const uint32_t* w[3];
+  const int rc = status_words(w);
   if (rc) return rc;
-  return fused_status_fetch(out, ST(stream));
+  launch_pdl(k_status_fetch, dim3(1), dim3(1), 0, ST(stream), w[0], w[1], w[2], out);
+  return check_launch("device_status_fetch");
 }
 
 GSB_API int gsb_debug_expire_bulk_wait(uint32_t poll_limit, void* stream) {
@@ -544,6 +595,38 @@ static int render_backward(int64_t n, const gsb_camera* cam, const float* pws, c
   f.accumulate = acc;
   return launch_render(params->mode, params->dtype, K, params->P, params->Q, params->rank, f, true,
                        ST(stream));
+}
+
+GSB_API size_t gsb_draw_batch_bytes(int max_jobs) { return draw_queue_bytes(max_jobs); }
+
+GSB_API int gsb_draw_batch_pack(const gsb_draw_job* jobs, int njobs, void* host_table,
+                                size_t table_bytes) {
+  GSB_CHECK_ARG(njobs >= 0 && (njobs == 0 || jobs) && host_table, "draw_batch_pack: null pointer");
+  for (int i = 0; i < njobs; ++i) {
+    const gsb_draw_job& j = jobs[i];
+    int rc = check_image("draw_batch_pack", j.n, j.height, j.width, j.channels);
+    if (rc) return rc;
+    GSB_CHECK_ARG(j.channels == jobs[0].channels, "draw_batch_pack: job %d has %d channels, job 0 %d",
+                  i, j.channels, jobs[0].channels);
+    GSB_CHECK_ARG(j.state && ((uintptr_t)j.state & 255) == 0 && j.ranges && j.out && j.contrib &&
+                      j.final_tau,
+                  "draw_batch_pack: job %d: null or misaligned pointer", i);
+  }
+  const int rc = draw_queue_pack(jobs, njobs, host_table, table_bytes);
+  if (rc) set_error("draw_batch_pack: %d jobs need %zu table bytes, %zu given", njobs,
+                    draw_queue_bytes(njobs), table_bytes);
+  return rc;
+}
+
+GSB_API int gsb_draw_batch(const void* dev_table, int channels, void* stream) {
+  GSB_CHECK_ARG(dev_table && ((uintptr_t)dev_table & 15) == 0,
+                "draw_batch: table must be a 16-byte aligned device buffer");
+  GSB_CHECK_ARG(channels >= 1 && channels <= GSB_MAX_CHANNELS, "draw_batch: bad channel count");
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return check_launch("draw_batch (device query)", 0);
+  return launch_draw_queue(channels, dev_table, 4 * sms, ST(stream));
 }
 
 GSB_API int gsb_palette_weights_backward(int64_t n, const gsb_camera* cam, const float* pws,

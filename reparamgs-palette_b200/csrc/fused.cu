@@ -828,16 +828,13 @@ int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedAr
                                  : dispatch_fused<float>(mode, K, P, Q, R, f, bwd, st);
 }
 
-// ORs this file's status word into *out (see k_lowrank_status_fetch).
-__global__ void k_fused_status_fetch(uint32_t* out) {
-  pdl_wait();
-  const uint32_t v = *(volatile uint32_t*)&g_fused_status;
-  if (v) *(volatile uint32_t*)out |= v;
-}
-
-int fused_status_fetch(uint32_t* out, cudaStream_t st) {
-  launch_pdl(k_fused_status_fetch, dim3(1), dim3(1), 0, st, out);
-  return check_launch("device_status_fetch");
+const uint32_t* fused_status_word() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_fused_status) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return nullptr;
+  }
+  return (const uint32_t*)p;
 }
 
 // Error-path check: one block arms an mbarrier for a 16-byte transaction

@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "gsplat_b200.h"
+
 namespace gsb {
 
 // preprocess.cu
@@ -28,7 +30,9 @@ int launch_sh2weight_lowrank_b(int64_t n, const void* A, const void* B, int dtyp
                                int L, float* dA, float* dB, cudaStream_t st);
 int launch_lab2rgb(int H, int W, const float* lab, float* rgb, cudaStream_t st);
 int lowrank_status(uint32_t* out, bool clear, cudaStream_t st);
-int lowrank_status_fetch(uint32_t* out, cudaStream_t st);
+// Device address of this file's status word (cudaGetSymbolAddress, with the
+// current device and context), null on failure.
+const uint32_t* lowrank_status_word();
 
 // loss.cu
 int launch_palette_l1(int K, int H, int W, const float* layer, const float* palette,
@@ -44,6 +48,10 @@ int launch_palette_l1_ssim(int K, int H, int W, const float* layer, const float*
                            const float* target, float lambda_ssim, float lambda_pos,
                            float data_range, float* image, float* loss, float* dlayer,
                            float* dpal, cudaStream_t st);
+
+// sort_static.cu -- process-unique id of the calling thread's current CUDA
+// context (0 if unknown).
+unsigned long long current_context_id();
 
 // binning.cu -- clears a[0, na) and b[0, nb) (32-bit words; either may be
 // null) in one kernel launched in the programmatic-dependent-launch chain.
@@ -100,6 +108,14 @@ int launch_sort_capacity(const SortPlan& p, int64_t n, int H, int W, const Splat
 int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, const int32_t* gsid,
                 const SplatState& s, float tau_init, float* out, int32_t* contrib,
                 float* final_tau, cudaStream_t st);
+// Batched compositing (raster.cu): one image of a batch as the host
+// describes it (gsb_draw_job of the C ABI).
+using DrawJobDesc = gsb_draw_job;
+size_t draw_queue_bytes(int max_jobs);
+int draw_queue_pack(const DrawJobDesc* jobs, int njobs, void* host_table, size_t table_bytes);
+int launch_draw_queue(int channels, const void* dev_table, int grid, cudaStream_t st);
+int raster_status(uint32_t* out, bool clear, cudaStream_t st);
+const uint32_t* raster_status_word();
 int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* ranges,
                          const int32_t* gsid, const SplatState& s, const int32_t* contrib,
                          const float* final_tau, const float* dout, const float* dtau,
@@ -129,7 +145,7 @@ struct FusedArgs {
 int launch_render(int mode, int dtype, int K, int P, int Q, int R, const FusedArgs& f, bool backward,
                   cudaStream_t st);
 int fused_status(uint32_t* out, bool clear, cudaStream_t st);
-int fused_status_fetch(uint32_t* out, cudaStream_t st);
+const uint32_t* fused_status_word();
 int expire_bulk_wait(uint32_t poll_limit, cudaStream_t st);
 
 }  // namespace gsb

@@ -275,19 +275,13 @@ __global__ void __launch_bounds__(kLrThreads)
   }
 }
 
-// ORs this file's status word into *out (device or mapped host memory; one
-// thread, so the read-modify-write of *out is not shared with other threads
-// of this launch).  The word itself is left set: only gsb_device_status
-// clears it.
-__global__ void k_lowrank_status_fetch(uint32_t* out) {
-  pdl_wait();
-  const uint32_t v = *(volatile uint32_t*)&g_lowrank_status;
-  if (v) *(volatile uint32_t*)out |= v;
-}
-
-int lowrank_status_fetch(uint32_t* out, cudaStream_t st) {
-  launch_pdl(k_lowrank_status_fetch, dim3(1), dim3(1), 0, st, out);
-  return check_launch("device_status_fetch");
+const uint32_t* lowrank_status_word() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_lowrank_status) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return nullptr;
+  }
+  return (const uint32_t*)p;
 }
 
 int lowrank_status(uint32_t* out, bool clear, cudaStream_t st) {

@@ -49,12 +49,20 @@ static std::mutex g_scratch_mutex;
 using CtxGetCurrentFn = CUresult (*)(CUcontext*);
 using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
+}  // namespace gsb
+
+namespace gsb {
+
 // Process-unique id of the calling thread's current context (0 if unknown).
-static unsigned long long current_context_id() {
+// Callers hold their own lock; the one-time resolution of the two driver
+// entry points is guarded here.
+unsigned long long current_context_id() {
   static CtxGetCurrentFn get_current = nullptr;
   static CtxGetIdFn get_id = nullptr;
   static bool resolved = false;
-  if (!resolved) {  // (called with g_scratch_mutex held)
+  static std::mutex resolve_mutex;
+  std::lock_guard<std::mutex> guard(resolve_mutex);
+  if (!resolved) {
     cudaDriverEntryPointQueryResult q1, q2;
     if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) !=
             cudaSuccess ||

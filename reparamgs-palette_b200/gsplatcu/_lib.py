@@ -74,6 +74,9 @@ _SIGS = {
     "gsb_render_preprocess": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_render_backward_bytes": (_sz, [_i64, _i32]),
     "gsb_palette_weights_backward": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "gsb_draw_batch_bytes": (_sz, [_i32]),
+    "gsb_draw_batch_pack": (_i32, [_p, _i32, _p, _sz]),
+    "gsb_draw_batch": (_i32, [_p, _i32, _p]),
     "gsb_render_backward": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
                                    _p, _p, _p, _p, _p, _p, _p, _p]),
     "gsb_render_backward_accumulate": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
@@ -101,6 +104,14 @@ class PaletteParams(C.Structure):
     _fields_ = [("mode", C.c_int), ("dtype", C.c_int), ("K", C.c_int), ("P", C.c_int),
                 ("Q", C.c_int), ("rank", C.c_int), ("w0", C.c_void_p), ("A", C.c_void_p),
                 ("B", C.c_void_p), ("palette", C.c_void_p)]
+
+
+class DrawJob(C.Structure):
+    """gsb_draw_job: one image of a batched compositing launch."""
+    _fields_ = [("state", C.c_void_p), ("n", C.c_int64), ("height", C.c_int),
+                ("width", C.c_int), ("channels", C.c_int), ("ranges", C.c_void_p),
+                ("gsid", C.c_void_p), ("tau_init", C.c_float), ("out", C.c_void_p),
+                ("contrib", C.c_void_p), ("final_tau", C.c_void_p)]
 
 
 class GsplatError(RuntimeError):
@@ -206,13 +217,16 @@ def raise_if_timed_out(dev, op):
     if w is None or int(w[0][0]) == 0:
         return
     bits = int(w[0][0])
-    w[0].zero_()
-    if w[2] is not None:
-        w[2].zero_()
+    # clear the device bits (this synchronises the stream, so fetches enqueued
+    # before it -- which may still OR the old bits into the host word -- have
+    # run), then the host word
     cleared = C.c_uint32(0)
     with torch.cuda.device(dev):
         call("device_status", "gsb_device_status", C.byref(cleared), 1,
              C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    w[0].zero_()
+    if w[2] is not None:
+        w[2].zero_()
     raise GsplatError(
         f"gsplatcu.{op}: a bounded device-side wait for a bulk copy ran out (status bits "
         f"{bits:#x}); the results of the calls since the last check are incomplete "

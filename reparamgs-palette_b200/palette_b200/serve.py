@@ -6,23 +6,31 @@ image -- with continuous batching:
 
 * Scenes are admitted by their HBM footprint (parameters plus the growth of
   the per-slot render workspaces they need) against a byte budget, and can be
-  evicted to make room.
-* A request renders in one of ``slots`` execution slots.  A slot owns a CUDA
-  stream, device buffers for the camera and palette, and render workspaces
-  sized for the largest (scene, resolution) bucket it serves.  Each bucket's
-  render -- fused preprocess with palette-colour records
+  evicted to make room.  Admission survives a failed workspace allocation
+  (the scene is refused, the slots stay whole).
+* A request is prepared in one of ``slots`` execution slots.  A slot owns a
+  CUDA stream, device buffers for the camera and palette, and render
+  workspaces sized for the largest (scene, resolution) bucket it serves.
+  Each bucket's preparation -- fused preprocess with palette-colour records
   (gsb_render_preprocess), capacity-sized tile sort with no host read-back
-  (gsb_splat_sort_capacity), compositing (gsb_splat_draw, 3 channels, final
-  transmittance starting at 1 as splat_color) and the copy of the overflow
-  status word to pinned host memory -- is captured once per slot as a CUDA
-  graph; a request copies its camera and palette into the slot's buffers and
-  replays the graph on the slot's stream.
-* Requests that arrive while others run are started as soon as a slot is
-  free, so several renders of different scenes and resolutions overlap on
-  the device; a finished slot takes the next queued request at once.
+  (gsb_splat_sort_capacity) and the copy of the sort's overflow words to
+  pinned host memory -- is captured once per slot as a CUDA graph; a request
+  copies its camera and palette into the slot's buffers and replays it on
+  the slot's stream, so the preparations of different requests overlap.
+* Prepared requests are composited together: a batch packs their images
+  into a job table (gsb_draw_batch_pack) and one persistent kernel
+  (gsb_draw_batch) claims (image, tile) items from all of them until every
+  tile is done, so tiles of large and small images, of different scenes
+  and resolutions, share the SMs.  The table copy, the kernel and the fetch
+  and copy of the device status bits are one captured CUDA graph per batch
+  table, replayed on the table's own stream after it waits for the members'
+  preparations.  Up to ``batches`` batches are in flight and overlap on the
+  device; requests that arrive meanwhile are prepared at once and join the
+  next batch.
 * A render whose patch count or depth key exceeded the bucket's capacity
-  (status word) is re-run after the bucket's capacity grows (its graphs are
-  recaptured); its latency includes the re-run.
+  (status words) is re-run after the bucket's capacity grows (its graphs are
+  recaptured); its latency includes the re-run.  A bounded device wait that
+  ran out (status bits) raises GsplatError(GSB_ERR_DEVICE_TIMEOUT).
 
 The palette-edit image equals the reference's bake-and-render path
 (gsplat/gsmodel.py:488-509 bakes palette colours into RGB SH coefficients,
@@ -138,15 +146,15 @@ class _Slot:
         self.tcw = torch.zeros((3,), dtype=_F32, device=device)
         self.twc = torch.zeros((3,), dtype=_F32, device=device)
         self.palette = torch.zeros((K_max, 3), dtype=_F32, device=device)
-        # words 0-2: overflow bits and patch count of the capacity sort; word 3:
-        # the library's device status bits (a bounded bulk-copy wait ran out)
+        # overflow bits and patch count of the capacity sort
         self.status = torch.zeros((4,), dtype=torch.int32, device=device)
         self.status_host = torch.zeros((4,), dtype=torch.int32).pin_memory()
         self.sizes = dict(state=0, sort=0, gsid=0, tiles=0, pixels=0)
         self.buf = {}
         self.graphs = {}
         self.req = None
-        self.event = None
+        self.event = None  # the preparation's completion
+        self.batch = None  # the batch compositing the request, once launched
 
     def bytes(self):
         s = self.sizes
@@ -177,8 +185,9 @@ class _Slot:
     def image_view(self, W, H):
         return self.buf["image"][:3 * W * H].view(3, H, W)
 
-    def launch(self, b, fx, fy, cx, cy):
-        """Enqueue one render of bucket b on the current stream (capturable)."""
+    def launch_prep(self, b, fx, fy, cx, cy):
+        """Enqueue one request's preparation for bucket b on the current
+        stream (capturable): preprocess, capacity sort, status words."""
         sc, W, H = b.scene, b.W, b.H
         cam = _lib.Camera(self.Rcw.data_ptr(), self.tcw.data_ptr(), self.twc.data_ptr(), fx, fy,
                           cx, cy, W, H)
@@ -191,13 +200,62 @@ class _Slot:
         _lib.call("serve", "gsb_splat_sort_capacity", n, H, W, b.capacity, MAX_DEPTH_KEY,
                   _lib.ptr(bf["state"]), _lib.ptr(bf["sort"]), _lib.ptr(bf["gsid"]),
                   _lib.ptr(bf["ranges"]), _lib.ptr(self.status), st)
-        _lib.call("serve", "gsb_splat_draw", n, H, W, 3, _lib.ptr(bf["ranges"]),
-                  _lib.ptr(bf["gsid"]), _lib.ptr(bf["state"]), 1.0, _lib.ptr(bf["image"]),
-                  _lib.ptr(bf["contrib"]), _lib.ptr(bf["final_tau"]), st)
-        # device status bits (bounded waits of the preprocess) into word 3
-        _lib.call("serve", "gsb_device_status_fetch", C.c_void_p(self.status.data_ptr() + 12), st)
-        # status words -> pinned host words, read once the render's event fires
-        err, = _rt.cudaMemcpyAsync(self.status_host.data_ptr(), self.status.data_ptr(), 16,
+        # overflow status -> pinned host words, read once the request's batch is
+        # done (the device status bits are fetched by the batch, after its
+        # members' preparations and the compositing)
+        err, = _rt.cudaMemcpyAsync(self.status_host.data_ptr(), self.status.data_ptr(), 12,
+                                   _rt.cudaMemcpyKind.cudaMemcpyDeviceToHost, st.value)
+        if err != _rt.cudaError_t.cudaSuccess:
+            raise _lib.GsplatError(f"serve: status copy failed ({err})")
+
+    def job(self, b):
+        """The slot's image as an entry of a batched compositing launch."""
+        bf = self.buf
+        return _lib.DrawJob(bf["state"].data_ptr(), b.scene.n, b.H, b.W, 3,
+                            bf["ranges"].data_ptr(), bf["gsid"].data_ptr(), 1.0,
+                            bf["image"].data_ptr(), bf["contrib"].data_ptr(),
+                            bf["final_tau"].data_ptr())
+
+
+class _Batch:
+    """One batch table: pinned host table, device table, status words and
+    the captured graph (table copy, persistent compositing, status copy)."""
+
+    def __init__(self, device, max_jobs):
+        L = _lib.lib()
+        self.device = device
+        self.max_jobs = max_jobs
+        self.nbytes = int(L.gsb_draw_batch_bytes(max_jobs))
+        self.host = torch.zeros((self.nbytes,), dtype=torch.uint8).pin_memory()
+        self.dev = torch.zeros((self.nbytes,), dtype=torch.uint8, device=device)
+        self.status = torch.zeros((1,), dtype=torch.int32, device=device)
+        self.status_host = torch.zeros((1,), dtype=torch.int32).pin_memory()
+        self.stream = torch.cuda.Stream(device)  # batches overlap on the device
+        self.graph = None
+        self.event = None
+        self.slots = []
+
+    def pack(self, jobs):
+        arr = (_lib.DrawJob * max(1, len(jobs)))(*jobs)
+        _lib.call("serve", "gsb_draw_batch_pack", arr, len(jobs), C.c_void_p(self.host.data_ptr()),
+                  self.nbytes)
+
+    def enqueue(self):
+        """Table copy, batched compositing, status fetch and copy on the
+        current stream (capturable: a replay copies the host table's
+        contents at that time)."""
+        st = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        err, = _rt.cudaMemcpyAsync(self.dev.data_ptr(), self.host.data_ptr(), self.nbytes,
+                                   _rt.cudaMemcpyKind.cudaMemcpyHostToDevice, st.value)
+        if err != _rt.cudaError_t.cudaSuccess:
+            raise _lib.GsplatError(f"serve: table copy failed ({err})")
+        _lib.call("serve", "gsb_draw_batch", _lib.ptr(self.dev), 3, st)
+        # the library's device status bits (a bounded wait of the members'
+        # preprocess or of the compositing ran out), fetched into a word
+        # cleared first
+        self.status.zero_()
+        _lib.call("serve", "gsb_device_status_fetch", _lib.ptr(self.status), st)
+        err, = _rt.cudaMemcpyAsync(self.status_host.data_ptr(), self.status.data_ptr(), 4,
                                    _rt.cudaMemcpyKind.cudaMemcpyDeviceToHost, st.value)
         if err != _rt.cudaError_t.cudaSuccess:
             raise _lib.GsplatError(f"serve: status copy failed ({err})")
@@ -211,8 +269,8 @@ class PaletteServer:
     (False: launch the same kernels directly, for comparison).  keep_images:
     copy each finished image out of its slot (off for throughput runs)."""
 
-    def __init__(self, hbm_budget, slots=4, device="cuda", use_graphs=True, K_max=8,
-                 capacity_margin=1.5, keep_images=True, alloc=None):
+    def __init__(self, hbm_budget, slots=8, device="cuda", use_graphs=True, K_max=8,
+                 capacity_margin=1.5, keep_images=True, alloc=None, batches=3):
         self.device = torch.device(device)
         self.last_admit_error = None
         self.keep_images = keep_images
@@ -222,9 +280,11 @@ class PaletteServer:
         self.scenes = collections.OrderedDict()
         self.buckets = {}
         self.slots = [_Slot(self.device, K_max, alloc) for _ in range(slots)]
+        self.batches = [_Batch(self.device, slots) for _ in range(batches)]
         self.queue = collections.deque()
         self.done = []
         self.graph_captures = 0
+        self.batch_sizes = []
 
     # ------------------------------------------------------------ memory
     def resident_bytes(self):
@@ -285,10 +345,8 @@ class PaletteServer:
     def evict_scene(self, scene_id):
         """Drop a scene (waits for its in-flight renders).  Slot workspaces
         keep their size until the server is rebuilt."""
-        for sl in self.slots:
-            if sl.req is not None and sl.req.scene_id == scene_id:
-                sl.event.synchronize()
-                self._retire(sl)
+        if any(sl.req is not None and sl.req.scene_id == scene_id for sl in self.slots):
+            self.drain()
         self.scenes.pop(scene_id)
         for key in [k for k in self.buckets if k[0] == scene_id]:
             del self.buckets[key]
@@ -323,18 +381,35 @@ class PaletteServer:
         key = req.bucket
         g = sl.graphs.get(key)
         if g is None:
-            sl.launch(b, req.fx, req.fy, req.cx, req.cy)  # warm (function attributes)
+            with torch.cuda.stream(sl.stream):
+                sl.launch_prep(b, req.fx, req.fy, req.cx, req.cy)  # warm (function attributes)
             torch.cuda.synchronize(self.device)
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=sl.stream):
-                sl.launch(b, req.fx, req.fy, req.cx, req.cy)
+                sl.launch_prep(b, req.fx, req.fy, req.cx, req.cy)
             sl.graphs[key] = g
             self.graph_captures += 1
         return g
 
+    def _batch_graph(self, bt):
+        """The batch table's graph, captured on first use (with an empty table:
+        call it before packing the batch)."""
+        if bt.graph is None:
+            bt.pack([])
+            with torch.cuda.stream(bt.stream):
+                bt.enqueue()  # warm (function attributes, status-word addresses)
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=bt.stream):
+                bt.enqueue()
+            bt.graph = g
+            self.graph_captures += 1
+        return bt.graph
+
     def prepare(self, requests):
-        """Capture every (bucket, slot) graph these requests need, before a
-        timed run (a service does this at start-up)."""
+        """Capture every (bucket, slot) preparation graph these requests need
+        and the batch graphs, before a timed run (a service does this at
+        start-up)."""
         if not self.use_graphs:
             return
         seen = set()
@@ -344,8 +419,9 @@ class PaletteServer:
             seen.add(r.bucket)
             b = self.buckets[r.bucket]
             for sl in self.slots:
-                with torch.cuda.stream(sl.stream):
-                    self._graph(sl, b, r)
+                self._graph(sl, b, r)
+        for bt in self.batches:
+            self._batch_graph(bt)
         torch.cuda.synchronize(self.device)
 
     def _start(self, sl, req):
@@ -353,40 +429,75 @@ class PaletteServer:
         if b is None:
             raise KeyError(f"no render bucket for scene {req.scene_id!r} at "
                            f"{req.width}x{req.height}; admit the scene with this resolution")
-        if sl.ensure(b):
-            pass  # workspaces grew: graphs are recaptured below
+        sl.ensure(b)  # (workspaces grew: graphs are recaptured below)
         K = b.scene.K
+        g = self._graph(sl, b, req) if self.use_graphs else None
         with torch.cuda.stream(sl.stream):
             sl.Rcw.copy_(req.Rcw, non_blocking=True)
             sl.tcw.copy_(req.tcw, non_blocking=True)
             sl.twc.copy_(req.twc, non_blocking=True)
             sl.palette[:K].copy_(req.palette, non_blocking=True)
-            if self.use_graphs:
-                self._graph(sl, b, req).replay()
+            if g is not None:
+                g.replay()
             else:
-                sl.launch(b, req.fx, req.fy, req.cx, req.cy)
+                sl.launch_prep(b, req.fx, req.fy, req.cx, req.cy)
             sl.event = torch.cuda.Event()
             sl.event.record(sl.stream)
         if req.start is None:
             req.start = time.perf_counter()
         req.slot = self.slots.index(sl)
         sl.req = req
+        sl.batch = None
+
+    def _launch_batch(self):
+        """Composite every prepared request not yet in a batch in one
+        persistent kernel, if a batch table is free."""
+        ready = [sl for sl in self.slots if sl.req is not None and sl.batch is None]
+        if not ready:
+            return False
+        bt = next((b for b in self.batches if not b.slots), None)
+        if bt is None:
+            return False
+        ready = ready[:bt.max_jobs]
+        g = self._batch_graph(bt) if self.use_graphs else None  # (captured before packing)
+        bt.pack([sl.job(self.buckets[sl.req.bucket]) for sl in ready])
+        with torch.cuda.stream(bt.stream):
+            for sl in ready:
+                bt.stream.wait_event(sl.event)
+            if g is not None:
+                g.replay()
+            else:
+                bt.enqueue()
+            bt.event = torch.cuda.Event()
+            bt.event.record(bt.stream)
+        bt.slots = ready
+        for sl in ready:
+            sl.batch = bt
+        self.batch_sizes.append(len(ready))
+        return True
+
+    def _retire_batch(self, bt):
+        members, bt.slots = bt.slots, []
+        bits = int(bt.status_host[0])
+        if bits:
+            # a bounded wait of a member's preprocess or of the compositing ran
+            # out: the batch's images are incomplete.  Clear the bits, report.
+            for sl in members:
+                sl.req, sl.batch = None, None
+            cleared = C.c_uint32(0)
+            _lib.call("serve", "gsb_device_status", C.byref(cleared), 1,
+                      C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+            bt.status_host[0] = 0
+            raise _lib.GsplatError(f"serve: a bounded device wait ran out in a batch of "
+                                   f"{len(members)} request(s) (status bits {bits:#x})",
+                                   _lib.GSB_ERR_DEVICE_TIMEOUT)
+        for sl in members:
+            sl.batch = None
+            self._retire(sl)
 
     def _retire(self, sl):
         req, b = sl.req, self.buckets[sl.req.bucket]
         sl.req = None
-        if int(sl.status_host[3]):
-            # a bounded wait of the render's preprocess ran out: its image is
-            # incomplete.  Clear the bits and report.
-            bits = int(sl.status_host[3])
-            sl.status_host[3] = 0
-            sl.status[3:].zero_()
-            cleared = C.c_uint32(0)
-            _lib.call("serve", "gsb_device_status", C.byref(cleared), 1,
-                      C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
-            raise _lib.GsplatError(f"serve: request for scene {req.scene_id!r}: a bounded device "
-                                   f"wait ran out (status bits {bits:#x})",
-                                   _lib.GSB_ERR_DEVICE_TIMEOUT)
         status = int(sl.status_host[0])
         if status & (_lib.STATUS_PATCH_OVERFLOW | _lib.STATUS_DEPTH_KEY_OVERFLOW):
             if status & _lib.STATUS_DEPTH_KEY_OVERFLOW:
@@ -406,14 +517,16 @@ class PaletteServer:
         return req
 
     def poll(self):
-        """Retire finished renders and start queued requests on free slots.
-        Returns the number of slots busy afterwards."""
-        for sl in self.slots:
-            if sl.req is not None and sl.event.query():
-                self._retire(sl)
+        """Retire finished batches, prepare queued requests on free slots and
+        launch a batch of the prepared ones.  Returns the number of busy
+        slots."""
+        for bt in self.batches:
+            if bt.slots and bt.event.query():
+                self._retire_batch(bt)
         for sl in self.slots:
             if sl.req is None and self.queue:
                 self._start(sl, self.queue.popleft())
+        self._launch_batch()
         return sum(sl.req is not None for sl in self.slots)
 
     def submit(self, req, now=None):
@@ -454,3 +567,21 @@ class PaletteServer:
                     p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
                     max_ms=float(lat.max()), frames_per_s=len(self.done) / (t_end - t0),
                     offered_rate=rate, reruns=int(sum(r.reruns for r in self.done)))
+
+    def run_closed_loop(self, requests):
+        """Saturation: all `requests` queued at once, served as fast as the
+        slots and batches allow.  Returns frames per second and the mean
+        batch size."""
+        self.done = []
+        n0 = len(self.batch_sizes)
+        torch.cuda.synchronize(self.device)
+        t0 = time.perf_counter()
+        for r in requests:
+            self.submit(r, now=t0)
+        self.drain()
+        t1 = time.perf_counter()
+        sizes = self.batch_sizes[n0:]
+        return dict(requests=len(self.done), seconds=t1 - t0,
+                    frames_per_s=len(self.done) / (t1 - t0),
+                    mean_batch=float(np.mean(sizes)) if sizes else 0.0,
+                    reruns=int(sum(r.reruns for r in self.done)))

@@ -152,6 +152,7 @@ def test_serve_admission_survives_allocation_failure(cuda_ok, fail_at):
 
 
 def test_serve_reports_expired_wait(cuda_ok):
+    gsc.check_device_status()  # clean start
     W, H = 320, 180
     scene, sc = _serve_scene("s1", 20000, 8)
     srv = PaletteServer(4 << 30, slots=1)

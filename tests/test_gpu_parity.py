@@ -1,7 +1,17 @@
 """GPU parity: every gsplatcu operator against the CPU oracle on the same
 seeded inputs.  Tolerances: tile lists, ranges, in-place depth/area updates
 and sort order bit-exact; images within 1e-5 abs (FP32 storage); gradients
-within 1e-4 relative (norm-wise); preprocess values within a few FP32 ulps."""
+within 1e-4 relative (norm-wise); preprocess values within a few FP32 ulps.
+
+Compositing decisions: the oracle evaluates exp() with the host C library and
+the GPU with CUDA's expf.  The two may differ by an ulp, which changes a skip
+(alpha' < 0.002) or stop (T < 1e-4) decision only where alpha' or T lies
+within that ulp of its threshold.  Such pixels (a different contributor
+index) are counted, printed and excluded from the image comparison; at most
+``MAX_EXP_FLIPS`` per image are allowed (measured on a B200: 0 such pixels in
+every case of this file).  Against the reference build itself,
+which uses the same expf, contributor indices are compared bit for bit
+(tests/test_gpu_reference.py, tests/test_gpu_fullsize.py)."""
 import numpy as np
 import pytest
 import torch
@@ -15,6 +25,19 @@ pytestmark = pytest.mark.gpu
 
 IMG_TOL = 1e-5
 GRAD_REL = 1e-4
+MAX_EXP_FLIPS = 2
+
+
+def _compare_composite(name, img, contrib, ft, ref):
+    """Contributor indices equal but for at most MAX_EXP_FLIPS pixels (an
+    exp() ulp at a threshold, see the module docstring); images and final
+    transmittance within IMG_TOL on every other pixel."""
+    same = np_of(contrib) == ref["contrib"]
+    flips = int((~same).sum())
+    print(f"{name}: {flips} of {same.size} pixels with a different contributor index")
+    assert flips <= MAX_EXP_FLIPS
+    assert max_abs(np_of(img)[:, same], ref["out"][:, same]) < IMG_TOL
+    assert max_abs(np_of(ft)[same], ref["ft"][same]) < IMG_TOL
 
 CASES = [  # (N, W, H, eye)
     (2000, 64, 64, (0.0, -8.0, 0.0)),
@@ -104,11 +127,7 @@ def test_splat_weight_lists_bitexact_and_image(cuda_ok, case):
     assert np.array_equal(np_of(pre["depths"]), ref["depths"])
     assert np.array_equal(np_of(pre["areas"]), ref["areas"])
     # compositing
-    c_gpu = np_of(contrib)
-    same = c_gpu == ref["contrib"]
-    assert same.mean() > 1 - 1e-4
-    assert max_abs(np_of(layer)[:, same], ref["out"][:, same]) < IMG_TOL
-    assert max_abs(np_of(ft)[same], ref["ft"][same]) < IMG_TOL
+    _compare_composite(f"splat_weight {case}", layer, contrib, ft, ref)
     assert np.mean(np.abs(np_of(layer) - ref["out"])) < 1e-7
 
 
@@ -226,9 +245,7 @@ def test_splat_color_forward_backward_matches_oracle(cuda_ok):
     img, contrib, ft, ranges, gsid = gsc.splat_color(H, W, pre["us"], pre["cinv"], st["alphas"],
                                                      pre["depths"], col, pre["areas"])
     assert np.array_equal(np_of(gsid), ref["b"]["gsid"])
-    same = np_of(contrib) == ref["contrib"]
-    assert same.mean() > 1 - 1e-4
-    assert max_abs(np_of(img)[:, same], ref["out"][:, same]) < IMG_TOL
+    _compare_composite("splat_color", img, contrib, ft, ref)
     g = torch.randn((3, H, W), device="cuda")
     du, dq, da, dc = gsc.splat_color_B(H, W, pre["us"], pre["cinv"], st["alphas"], pre["depths"], col,
                                        contrib, ft, ranges, gsid, g)
@@ -375,9 +392,7 @@ def test_splat_weight_overlapped_count_and_overflow_bitexact(cuda_ok):
         assert np.array_equal(np_of(ranges), ref["b"]["ranges"])
         assert np.array_equal(np_of(pre["depths"]), ref["depths"])
         assert np.array_equal(np_of(pre["areas"]), ref["areas"])
-        same = np_of(contrib) == ref["contrib"]
-        assert same.mean() > 1 - 1e-4
-        assert max_abs(np_of(layer)[:, same], ref["out"][:, same]) < IMG_TOL
+        _compare_composite(f"overlapped count {eye}", layer, contrib, ft, ref)
 
 
 def test_backward_reuses_forward_records_only_when_inputs_unchanged(cuda_ok):

@@ -1,8 +1,9 @@
 """GPU tests of the palette-edit serving path: the capacity-sized tile sort,
 the palette-colour render against the reference's bake-and-render sequence
 (gsplat/gsmodel.py:488-509 + 14-26, run through gsplatcu), continuous
-batching (each image identical alone and in the mix), HBM admission, and
-re-rendering after a capacity overflow.  Tolerances: sort outputs bit-exact;
+batching through the persistent batched compositing kernel (each image
+identical alone and in the mix), HBM admission, and re-rendering after a
+capacity overflow.  Tolerances: sort outputs bit-exact;
 images 1e-5 abs against the bake-and-render sequence (a different FP32
 summation order of the same linear map); mix vs alone bit-exact (same kernels
 and inputs, no atomics in the forward)."""
@@ -170,10 +171,14 @@ def test_continuous_batching_mix_equals_alone(cuda_ok):
     mix = [mk() for mk in reqs]
     for r in mix:  # all arrive at once: slots fill, the rest queue
         srv.submit(r)
+    n0 = len(srv.batch_sizes)
     busy = srv.poll()
     assert busy == 3 and len(srv.queue) == 9
     srv.drain()
     assert len({r.slot for r in mix}) == 3
+    # the mix was composited in shared persistent launches (several requests
+    # of different scenes and resolutions per batch)
+    assert max(srv.batch_sizes[n0:]) > 1
     for r in mix:
         assert torch.equal(r.image, alone[r.tag]), r.tag
 
