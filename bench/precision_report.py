@@ -21,10 +21,22 @@ contributor index differs, or the final transmittance differs by more than
 them, and the relative error recomputed: that is the arithmetic part, the
 rest is the decision (threshold-flip) part.
 
+With ``--serving`` it instead measures the two storage forms of the serving
+benchmark as served: one scene with full SH weights in FP32 and one with
+rank-3 low-rank factors in BF16 (``--serve-gaussians`` each, the serving
+benchmark's generators), palette-edit requests at 1920x1080 (cameras on a
+sphere of radius 6..10, palettes perturbed as in the serving stream) rendered
+through ``PaletteServer`` -- per-slot preparation graphs and the persistent
+batched compositing kernel -- and each image compared with the FP64 oracle's
+palette colour image of the same request, rendered from the FP32 parameters
+(so the BF16 error includes the storage rounding), over every
+``--tile-stride``-th tile: PSNR (peak 1) and max / mean abs error per form.
+
 Not collected by pytest (it is a report, minutes of CPU time): run it on a
 GPU box and keep the printed JSON.
 
     python bench/precision_report.py [--gaussians 3000000] [--poses 32] [--tile-stride 8]
+    python bench/precision_report.py --serving [--serve-gaussians 250000] [--serve-requests 8]
 """
 import argparse
 import json
@@ -65,6 +77,74 @@ def stats(a, b, mask):
                 psnr=float("inf") if mse == 0 else 10 * math.log10(1.0 / mse))
 
 
+def serving_precision(a):
+    """PSNR vs FP64 of the serving path's two storage forms (see module doc)."""
+    from oracle import oracle as orc
+    from palette_b200.scene import look_at, sphere_poses, synthetic_scene, to_torch
+    from palette_b200.serve import PaletteServer, Request, Scene
+    orc.set_threads(os.cpu_count() or 1)
+    W, H, K, Q = 1920, 1080, 5, 15
+    n = a.serve_gaussians
+    forms = {}
+    sc = synthetic_scene(n, seed=100, mode="full")
+    st = to_torch(sc, "cuda", torch.float32)
+    forms["fp32_full"] = (sc, Scene("fp32_full", st["pws"], st["rots"], st["scales"], st["alphas"],
+                                    shs=st["shs"]))
+    sc = synthetic_scene(n, seed=200, mode="lowrank", rank=3)
+    st = to_torch(sc, "cuda", torch.bfloat16)
+    forms["bf16_lowrank"] = (sc, Scene("bf16_lowrank", st["pws"], st["rots"], st["scales"],
+                                       st["alphas"], dc=st["dc"], A=st["A"], B=st["B"]))
+    c0 = look_at((0, -8, 0), width=W, height=H, device="cpu")
+    res = [(W, H, c0.fx, c0.fy, c0.cx, c0.cy)]
+    probes = [(c.Rcw.numpy(), c.tcw.numpy()) for c in
+              (look_at(e, device="cpu") for e in sphere_poses(8, 6.0, seed=3))]
+    srv = PaletteServer(hbm_budget=8 << 30, slots=4, keep_images=True)
+    for _, scene in forms.values():
+        if not srv.admit_scene(scene, res, probes):
+            raise RuntimeError(f"scene {scene.id} not admitted")
+    rng = np.random.default_rng(11)
+    eyes = sphere_poses(a.serve_requests, (6.0, 10.0), seed=12)
+    report = dict(gaussians_per_scene=n, resolution=f"{W}x{H}", requests_per_form=a.serve_requests,
+                  tile_stride=a.tile_stride, host_threads=orc.get_threads(), forms={})
+    t0 = time.time()
+    for form, (sc, scene) in forms.items():
+        reqs, cams = [], []
+        for i in range(a.serve_requests):
+            cam = look_at(eyes[i], width=W, height=H, device="cpu")
+            pal = np.array(sc["palette"], np.float32)
+            pal[2:] = np.clip(pal[2:] + rng.normal(0, 0.15, pal[2:].shape), 0, 1)
+            reqs.append(Request(scene.id, cam.Rcw.numpy(), cam.tcw.numpy(), cam.fx, cam.fy,
+                                cam.cx, cam.cy, W, H, pal))
+            cams.append(cam)
+        srv.run_closed_loop(reqs)  # the batched persistent path
+        rows = []
+        for req, cam in zip(reqs, cams):
+            twc = req.twc.numpy().astype(np.float64)
+            pre32 = orc.preprocess(sc["pws"], sc["rots"], sc["scales"], cam, np.float32)
+            lists, mask = sampled_lists(orc, pre32, H, W, a.tile_stride)
+            f64 = {k: np.asarray(sc[k], np.float64) for k in ("pws", "rots", "scales", "alphas")}
+            if "shs" in sc:
+                w64, = orc.sh2feat(np.asarray(sc["shs"], np.float64), f64["pws"], twc, K, False,
+                                   np.float64, ref_quirk=False)
+            else:
+                w64, = orc.sh2weight_fast(np.asarray(sc["dc"], np.float64),
+                                          np.asarray(sc["A"], np.float64),
+                                          np.asarray(sc["B"], np.float64), f64["pws"], twc, K, Q,
+                                          False, np.float64)
+            o = orc.render_weights(f64["pws"], f64["rots"], f64["scales"], f64["alphas"], w64, cam,
+                                   np.float64, lists=lists)
+            img64 = np.einsum("kc,khw->chw", req.palette.numpy().astype(np.float64), o["layer"])
+            img = req.image.double().cpu().numpy().reshape(3, H, W)
+            rows.append(stats(img, img64, mask))
+        report["forms"][form] = dict(
+            psnr_min=min(r["psnr"] for r in rows), psnr_mean=float(np.mean([r["psnr"] for r in rows])),
+            max_abs=max(r["max_abs"] for r in rows),
+            mean_abs=float(np.mean([r["mean_abs"] for r in rows])),
+            frac_over_1e5=float(np.mean([r["frac_over_1e5"] for r in rows])))
+    report["wall_s"] = round(time.time() - t0, 1)
+    print(json.dumps(report, indent=1))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gaussians", type=int, default=3_000_000)
@@ -72,7 +152,12 @@ def main():
     ap.add_argument("--grad-poses", type=int, default=2)
     ap.add_argument("--tile-stride", type=int, default=8)
     ap.add_argument("--resolutions", default="3840x2160,1920x1080")
+    ap.add_argument("--serving", action="store_true")
+    ap.add_argument("--serve-gaussians", type=int, default=250_000)
+    ap.add_argument("--serve-requests", type=int, default=8)
     a = ap.parse_args()
+    if a.serving:
+        return serving_precision(a)
     from oracle import oracle as orc
     from palette_b200.render import render_palette
     from palette_b200.scene import look_at, sphere_poses, synthetic_scene, to_torch

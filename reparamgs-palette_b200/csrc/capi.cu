@@ -79,23 +79,21 @@ GSB_API const char* gsb_last_error(void) { return g_err; }
 GSB_API int gsb_version(void) { return 100; }
 GSB_API int gsb_device_status(uint32_t* status, int clear, void* stream) {
   GSB_CHECK_ARG(status, "device_status: null pointer");
-  uint32_t a = 0, b = 0, c = 0;
+  uint32_t a = 0, b = 0;
   int rc = lowrank_status(&a, clear != 0, ST(stream));
   if (rc) return rc;
   rc = fused_status(&b, clear != 0, ST(stream));
   if (rc) return rc;
-  rc = raster_status(&c, clear != 0, ST(stream));
-  if (rc) return rc;
-  *status = a | b | c;
+  *status = a | b;
   return GSB_OK;
 }
 
 // The device addresses of the status words of the files whose kernels wait
-// on bulk copies (low-rank weights, fused preprocess / adjoint, compositing),
-// looked up once per device and CUDA context.
+// on bulk copies (low-rank weights, fused preprocess / adjoint), looked up
+// once per device and CUDA context.
 struct StatusWords {
   unsigned long long ctx;
-  const uint32_t* w[3];
+  const uint32_t* w[2];
 };
 static StatusWords g_status_words[64];
 static std::mutex g_status_mutex;
@@ -113,35 +111,32 @@ static int status_words(const uint32_t** w) {
   if (!e.w[0] || ctx == 0 || e.ctx != ctx) {
     e.w[0] = lowrank_status_word();
     e.w[1] = fused_status_word();
-    e.w[2] = raster_status_word();
     e.ctx = ctx;
-    if (!e.w[0] || !e.w[1] || !e.w[2]) {
+    if (!e.w[0] || !e.w[1]) {
       e.w[0] = nullptr;
       set_error("device_status_fetch: cudaGetSymbolAddress failed on device %d", dev);
       return GSB_ERR_CUDA;
     }
   }
-  for (int k = 0; k < 3; ++k) w[k] = e.w[k];
+  for (int k = 0; k < 2; ++k) w[k] = e.w[k];
   return GSB_OK;
 }
 
-// ORs the three status words into *out (device memory or mapped host
-// memory; one thread, so the read-modify-write of *out is not shared).  The
-// words themselves are left set: only gsb_device_status clears them.
-__global__ void k_status_fetch(const uint32_t* a, const uint32_t* b, const uint32_t* c,
-                               uint32_t* out) {
+// ORs the status words into *out (device memory or mapped host memory; one
+// thread, so the read-modify-write of *out is not shared).  The words
+// themselves are left set: only gsb_device_status clears them.
+__global__ void k_status_fetch(const uint32_t* a, const uint32_t* b, uint32_t* out) {
   pdl_wait();
-  const uint32_t v = *(const volatile uint32_t*)a | *(const volatile uint32_t*)b |
-                     *(const volatile uint32_t*)c;
+  const uint32_t v = *(const volatile uint32_t*)a | *(const volatile uint32_t*)b;
   if (v) *(volatile uint32_t*)out |= v;
 }
 
 GSB_API int gsb_device_status_fetch(uint32_t* out, void* stream) {
   GSB_CHECK_ARG(out, "device_status_fetch: null pointer");
-  const uint32_t* w[3];
+  const uint32_t* w[2];
   const int rc = status_words(w);
   if (rc) return rc;
-  launch_pdl(k_status_fetch, dim3(1), dim3(1), 0, ST(stream), w[0], w[1], w[2], out);
+  launch_pdl(k_status_fetch, dim3(1), dim3(1), 0, ST(stream), w[0], w[1], out);
   return check_launch("device_status_fetch");
 }
 

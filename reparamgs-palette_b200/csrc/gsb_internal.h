@@ -114,8 +114,6 @@ using DrawJobDesc = gsb_draw_job;
 size_t draw_queue_bytes(int max_jobs);
 int draw_queue_pack(const DrawJobDesc* jobs, int njobs, void* host_table, size_t table_bytes);
 int launch_draw_queue(int channels, const void* dev_table, int grid, cudaStream_t st);
-int raster_status(uint32_t* out, bool clear, cudaStream_t st);
-const uint32_t* raster_status_word();
 int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* ranges,
                          const int32_t* gsid, const SplatState& s, const int32_t* contrib,
                          const float* final_tau, const float* dout, const float* dtau,

@@ -6,40 +6,29 @@
 // block of pixels, one per lane.  In the adjoint each of the 4 warps owns an
 // 8x8 block and each lane two pixels of one column, four rows apart, so the
 // per-Gaussian loop control and the warp reduction of the gradient terms are
-// shared by 64 pixels.  The tile's Gaussian list is staged through a
-// two-buffer shared-memory ring in batches of packed records, one record per
-// thread of the block (256 in the forward, 128 in the adjoint): each thread
-// issues the 1-D bulk copy (TMA, cp.async.bulk) of its record -- whose
-// Gaussian id it loaded a batch ahead -- and arrives on the buffer's
-// mbarrier with the copy's byte count, so batch b + 1 lands while batch b is
-// composited and one block barrier per batch remains (the one that also
-// decides the block's early exit).  Records sit at an odd stride of float4s,
-// so the lane-parallel culling reads of 32 consecutive records are free of
-// bank conflicts.  Every wait is bounded.
-// Within a batch every warp first tests 32 records at a time against its
-// pixel block (one record per lane, ballot) using the record's conservative
-// support box and then its cut ellipse, then walks only the overlapping
-// records in list order, two at a time: both records' opacity terms are
-// evaluated before the two blends (or, in the adjoint, the two transmittance
-// recoveries) so that their exp() chains overlap, and the adjoint sums the
-// two records' gradient vectors in one warp reduction.  Per
-// pixel, a record whose Mahalanobis distance exceeds its cut is skipped
-// without evaluating exp() -- the reference would skip it too
-// (alpha' < 0.002) -- and every other record is evaluated with the
+// shared by 64 pixels.  The tile's Gaussian list is staged through shared
+// memory in batches of 256 packed records, each thread loading whole records
+// (four 16-byte loads for K <= 5) -- the gather measured faster than a
+// double-buffered ring filled by per-record 1-D bulk copies or by cp.async
+// (the compositing is issue-bound and several blocks per SM already overlap
+// one block's staging with the others' compositing).  Within a batch every
+// warp first tests 32 records at a time against its pixel block (one record
+// per lane, ballot) using the record's conservative support box and then its
+// cut ellipse, then walks only the overlapping records in list order, two at
+// a time: both records' opacity terms are evaluated before the two blends
+// (or, in the adjoint, the two transmittance recoveries) so that their exp()
+// chains overlap, and the adjoint sums the two records' gradient vectors in
+// one warp reduction.  Per pixel, a record whose Mahalanobis distance exceeds
+// its cut is skipped without evaluating exp() -- the reference would skip it
+// too (alpha' < 0.002) -- and every other record is evaluated with the
 // reference's own FP32 expressions, so skip/stop decisions, contributor
 // indices and blended values agree with it.
 #include "gsb_geometry.cuh"
 #include "gsb_internal.h"
-#include "gsb_tma.cuh"
 
 namespace gsb {
 
-constexpr int kBatch = 256;   // forward records per ring buffer
-constexpr int kBatchB = 128;  // adjoint records per ring buffer
-
-// Status word of this file's kernels (kStatusBulkTimeout: a bounded wait for
-// a record batch ran out; the block then wrote no results).
-static __device__ uint32_t g_raster_status;
+constexpr int kBatch = 256;
 constexpr int kDrawFwdThreads = 256;  // forward: one pixel per thread, 8x4 pixels per warp
 constexpr int kDrawThreads = 128;     // adjoint: two pixels per thread, 8x8 pixels per warp
 
@@ -71,37 +60,20 @@ __device__ __forceinline__ void pixel_of_1px(int tile, int gx, int& wx, int& wy,
   py = wy + (lane >> 3);
 }
 
-// Shared-memory ring of record batches: buffer b holds records at
-// ring(b)[slot * S + v], S = V rounded up to an odd count of float4s.
-template <int V>
-struct Ring {
-  static constexpr int S = V | 1;
-};
-
-// Batch filling, one record per thread: `fetch_id` loads the Gaussian id of
-// the thread's record in a batch (or -1 past the batch's end) -- issued a
-// batch ahead, so its latency overlaps the current batch -- and
-// `fill_slot` stores it (when `sgid` is given), arrives on the buffer's
-// mbarrier (initialised with the block's thread count) with the copy's byte
-// count and issues the 1-D bulk copy of the record (V float4s, 16-byte
-// aligned in global and shared memory).  The arrival releases the id store
-// to the threads that wait on the barrier.
-__device__ __forceinline__ int fetch_id(const int32_t* __restrict__ gsid, int first, int cnt) {
-  return (int)threadIdx.x < cnt ? __ldg(gsid + first + threadIdx.x) : -1;
-}
-
-template <int V>
-__device__ __forceinline__ void fill_slot(int g, const float4* __restrict__ records, float4* dst,
-                                          int32_t* sgid, uint64_t* bar) {
-  constexpr int S = Ring<V>::S;
-  const int t = threadIdx.x;
-  if (g < 0) {
-    mbar_arrive(bar);
-    return;
+// Stage records [first, first+cnt) of the tile list into shared memory,
+// vector-major (srec[v * kBatch + slot]) so that per-slot broadcasts and the
+// lane-per-slot box test are both conflict-free.
+template <int V, int NT>
+__device__ __forceinline__ void stage_batch(const int32_t* __restrict__ gsid, int first, int cnt,
+                                            const float4* __restrict__ records, float4* srec,
+                                            int32_t* sgid) {
+  for (int t = threadIdx.x; t < cnt; t += NT) {
+    const int g = gsid[first + t];
+    const float4* src = records + (int64_t)g * V;
+#pragma unroll
+    for (int v = 0; v < V; ++v) srec[v * kBatch + t] = __ldg(src + v);
+    if (sgid) sgid[t] = g;
   }
-  if (sgid) sgid[t] = g;
-  mbar_arrive_expect_tx(bar, V * 16);
-  bulk_load(dst + t * S, records + (int64_t)g * V, V * 16, bar);
 }
 
 // First stage of the warp's record test: does the record's support box
@@ -149,115 +121,67 @@ __device__ __forceinline__ bool ellipse_meets_block(float4 v0, float4 v1, float4
   return !(m > c2);
 }
 
-// Channels of one staged record `r` (its float4s r[0..V)).
 template <int K>
-__device__ __forceinline__ void load_feats(const float4* r, float v1w, float* f) {
-  f[0] = v1w;  // channel 0 sits in v1.w
+__device__ __forceinline__ void load_feats(const float4* srec, int j, float v2w, float* f) {
+  f[0] = v2w;  // channel 0 sits in v1.w
 #pragma unroll
   for (int k = 1; k < K; ++k) {
     const int idx = record_channel(k);  // float index inside the record
-    const float4 q = r[idx >> 2];
+    const float4 q = srec[(idx >> 2) * kBatch + j];
     f[k] = (idx & 3) == 0 ? q.x : (idx & 3) == 1 ? q.y : (idx & 3) == 2 ? q.z : q.w;
   }
 }
 
 // ------------------------------------------------------------- forward
-// Shared memory of one compositing block: the two-buffer record ring, its
-// mbarriers (initialised once per block) and the count of completed fills of
-// each buffer, whose low bit is the parity the next wait on it expects.
-template <int V>
-struct DrawSmem {
-  float4 rec[2][kBatch * Ring<V>::S];
-  uint64_t full[2];
-  uint32_t fills[2];
-  int fail;
-};
-
-template <int V>
-__device__ __forceinline__ void draw_smem_init(DrawSmem<V>& sm) {
-  if (threadIdx.x == 0) {
-    mbar_init(&sm.full[0], blockDim.x);  // one arrival per thread per fill
-    mbar_init(&sm.full[1], blockDim.x);
-    sm.fills[0] = sm.fills[1] = 0;
-    sm.fail = 0;
-  }
-  __syncthreads();
-}
-
-// Waits (bounded) for the next fill of ring buffer `buf`; every thread
-// calls it once per fill.  false when the wait ran out.
-template <int V>
-__device__ __forceinline__ bool ring_wait(DrawSmem<V>& sm, int buf) {
-  return mbar_wait(&sm.full[buf], sm.fills[buf] & 1);
-}
-
 // Composites one 16x16 tile of one image (draw_weight / draw_color,
 // gsplatcu/kernel.cu:283-372): ranges/gsid/records of that image's tile
-// lists, K channels, final_tau of empty tiles = tau_init.  Called by all
-// threads of a block; returns false when a bounded wait ran out (the status
-// bit is set, nothing was written and no copy is left in flight).
+// lists, K channels, final_tau of empty tiles = tau_init, `srec` the block's
+// staging buffer (V x kBatch float4s).  Called by all threads of a block; it
+// starts with a block barrier, so the buffer may still be in use by the
+// block's previous tile when it is called.
 template <int K>
-__device__ __forceinline__ bool draw_tile(int tile, int H, int W, int gx,
+__device__ __forceinline__ void draw_tile(int tile, int H, int W, int gx,
                                           const int2* __restrict__ ranges,
                                           const int32_t* __restrict__ gsid,
                                           const float4* __restrict__ records, float tau_init,
                                           float* __restrict__ out, int32_t* __restrict__ contrib,
-                                          float* __restrict__ final_tau,
-                                          DrawSmem<RecordLayout<K>::kVec4>& sm) {
-  constexpr int V = RecordLayout<K>::kVec4, S = Ring<V>::S;
+                                          float* __restrict__ final_tau, float4* srec) {
+  constexpr int V = RecordLayout<K>::kVec4;
   int wx, wy, px, py;
   pixel_of_1px(tile, gx, wx, wy, px, py);
-  const int lane = threadIdx.x & 31;
   const bool inside = px < W && py < H;
   const int2 rg = ranges[tile];
   const int n = rg.y - rg.x;
-  const int nb = (n + kBatch - 1) / kBatch;
   float acc[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) acc[k] = 0.f;
   float T = 1.f;
   int cont = 0;
   bool done = !inside;
-  static_assert(kBatch == kDrawFwdThreads, "one record per thread per batch");
-  if (nb > 0) {
-    const int g0 = fetch_id(gsid, rg.x, min(kBatch, n));
-    const int g1 = nb > 1 ? fetch_id(gsid, rg.x + kBatch, min(kBatch, n - kBatch)) : -1;
-    fill_slot<V>(g0, records, sm.rec[0], nullptr, &sm.full[0]);
-    if (nb > 1) fill_slot<V>(g1, records, sm.rec[1], nullptr, &sm.full[1]);
-  }
-  for (int b = 0; b < nb; ++b) {
-    const int buf = b & 1, base = b * kBatch, cnt = min(kBatch, n - base);
-    const float4* rs = sm.rec[buf];
-    // the id of this thread's record two batches on, loaded now so that its
-    // latency overlaps the compositing of this batch
-    const int gnext =
-        b + 2 < nb ? fetch_id(gsid, rg.x + base + 2 * kBatch, min(kBatch, n - base - 2 * kBatch))
-                   : -1;
-    const bool landed = ring_wait(sm, buf);
-    if (!landed) sm.fail = 1;
-    // (warp-uniform: a warp with a lane whose wait ran out skips the batch;
-    // the block then stops at the barrier below)
-    if (__all_sync(0xffffffffu, landed) && !__all_sync(0xffffffffu, done)) {
-      for (int s0 = 0; s0 < cnt; s0 += 32) {
-        const int j = s0 + lane;
-        bool ov = j < cnt && box_meets_block(rs[j * S], rs[j * S + 2], wx, wy, 7, 3);
+  for (int base = 0; base < n; base += kBatch) {
+    const int cnt = min(kBatch, n - base);
+    __syncthreads();
+    stage_batch<V, kDrawFwdThreads>(gsid, rg.x + base, cnt, records, srec, nullptr);
+    __syncthreads();
+    if (!__all_sync(0xffffffffu, done)) {
+      for (int s = 0; s < cnt; s += 32) {
+        const int j = s + (threadIdx.x & 31);
+        bool ov = j < cnt && box_meets_block(srec[j], srec[2 * kBatch + j], wx, wy, 7, 3);
         if (ov)
-          ov = ellipse_meets_block(rs[j * S], rs[j * S + 1], rs[j * S + 2], (float)wx, (float)wy,
-                                   (float)(wx + 7), (float)(wy + 3));
+          ov = ellipse_meets_block(srec[j], srec[kBatch + j], srec[2 * kBatch + j], (float)wx,
+                                   (float)wy, (float)(wx + 7), (float)(wy + 3));
         unsigned mask = __ballot_sync(0xffffffffu, ov);
         while (mask) {
-          const int jj = s0 + __ffs(mask) - 1;
+          const int jj = s + __ffs(mask) - 1;
           mask &= mask - 1;
           if (mask) {
             // two records at once: both opacity terms first, so that their
             // exp() chains overlap, then the two blends in list order
-            const int jb = s0 + __ffs(mask) - 1;
+            const int jb = s + __ffs(mask) - 1;
             mask &= mask - 1;
             if (done) continue;
-            const float4* ra = rs + jj * S;
-            const float4* rb = rs + jb * S;
-            const float4 a0 = ra[0], a1 = ra[1];
-            const float4 b0 = rb[0], b1 = rb[1];
+            const float4 a0 = srec[jj], a1 = srec[kBatch + jj];
+            const float4 b0 = srec[jb], b1 = srec[kBatch + jb];
             const float dxa = a0.x - (float)px, dya = a0.y - (float)py;
             const float dxb = b0.x - (float)px, dyb = b0.y - (float)py;
             const float ma = fmaxf(0.0f, maha_sq(a0.z, a0.w, a1.x, dxa, dya));
@@ -266,7 +190,7 @@ __device__ __forceinline__ bool draw_tile(int tile, int H, int W, int gx,
             const float apb = fminf(kAlphaMax, b1.z * expf(-0.5f * mb));
             if (!(ma > a1.y) && !(apa < kAlphaMin)) {
               float f[K];
-              load_feats<K>(ra, a1.w, f);
+              load_feats<K>(srec, jj, a1.w, f);
 #pragma unroll
               for (int k = 0; k < K; ++k) acc[k] += T * apa * f[k];
               cont = base + jj + 1;
@@ -275,7 +199,7 @@ __device__ __forceinline__ bool draw_tile(int tile, int H, int W, int gx,
             }
             if (!done && !(mb > b1.y) && !(apb < kAlphaMin)) {
               float f[K];
-              load_feats<K>(rb, b1.w, f);
+              load_feats<K>(srec, jb, b1.w, f);
 #pragma unroll
               for (int k = 0; k < K; ++k) acc[k] += T * apb * f[k];
               cont = base + jb + 1;
@@ -285,16 +209,15 @@ __device__ __forceinline__ bool draw_tile(int tile, int H, int W, int gx,
             continue;
           }
           if (done) continue;
-          const float4* r = rs + jj * S;
-          const float4 v0 = r[0];  // ux uy qa qb
-          const float4 v1 = r[1];  // qc c2 alpha ch0
+          const float4 v0 = srec[jj];           // ux uy qa qb
+          const float4 v1 = srec[kBatch + jj];  // qc c2 alpha ch0
           const float dx = v0.x - (float)px, dy = v0.y - (float)py;
           const float maha = fmaxf(0.0f, maha_sq(v0.z, v0.w, v1.x, dx, dy));
           if (maha > v1.y) continue;
           const float ap = fminf(kAlphaMax, v1.z * expf(-0.5f * maha));
           if (ap < kAlphaMin) continue;
           float f[K];
-          load_feats<K>(r, v1.w, f);
+          load_feats<K>(srec, jj, v1.w, f);
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] += T * ap * f[k];
           cont = base + jj + 1;
@@ -304,32 +227,7 @@ __device__ __forceinline__ bool draw_tile(int tile, int H, int W, int gx,
         if (__all_sync(0xffffffffu, done)) break;
       }
     }
-    // every warp is done with this buffer (it may be refilled) and the block
-    // learns whether any pixel still blends
-    const bool more = __syncthreads_or(!done) && !sm.fail && b + 1 < nb;
-    if (!more) {
-      // copies still in flight into the other buffer must land before the
-      // block's shared memory is reused or released
-      if (threadIdx.x == 0) {
-        if (sm.fail) {
-          atomicOr(&g_raster_status, kStatusBulkTimeout);
-          mbar_wait(&sm.full[buf], sm.fills[buf] & 1);
-        }
-        if (b + 1 < nb) mbar_wait(&sm.full[buf ^ 1], sm.fills[buf ^ 1] & 1);
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        sm.fills[buf] += 1;
-        if (b + 1 < nb) sm.fills[buf ^ 1] += 1;
-      }
-      break;
-    }
-    if (threadIdx.x == 0) sm.fills[buf] += 1;  // (read again only after the next barrier)
-    if (b + 2 < nb) fill_slot<V>(gnext, records, sm.rec[buf], nullptr, &sm.full[buf]);
-  }
-  if (nb > 0) {
-    __syncthreads();  // fills counted; fail visible
-    if (sm.fail) return false;
+    if (!__syncthreads_or(!done)) break;
   }
   if (inside) {
     const int64_t pix = (int64_t)py * W + px, hw = (int64_t)H * W;
@@ -338,7 +236,6 @@ __device__ __forceinline__ bool draw_tile(int tile, int H, int W, int gx,
     contrib[pix] = cont;
     final_tau[pix] = n > 0 ? T : tau_init;
   }
-  return true;
 }
 
 template <int K>
@@ -347,10 +244,9 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4)
            const float4* __restrict__ records, float tau_init, float* __restrict__ out,
            int32_t* __restrict__ contrib, float* __restrict__ final_tau) {
   pdl_wait();
-  __shared__ DrawSmem<RecordLayout<K>::kVec4> sm;
-  draw_smem_init(sm);
+  __shared__ float4 srec[RecordLayout<K>::kVec4 * kBatch];
   draw_tile<K>(blockIdx.x, H, W, gx, ranges, gsid, records, tau_init, out, contrib, final_tau,
-               sm);
+               srec);
 }
 
 // ------------------------------------------------- batched (persistent) draw
@@ -384,9 +280,8 @@ struct DrawQueue {
 template <int K>
 __global__ void __launch_bounds__(kDrawFwdThreads, 4) k_draw_queue(DrawQueue* __restrict__ q) {
   pdl_wait();
-  __shared__ DrawSmem<RecordLayout<K>::kVec4> sm;
+  __shared__ float4 srec[RecordLayout<K>::kVec4 * kBatch];
   __shared__ int s_item, s_job;
-  draw_smem_init(sm);
   const int total = (int)q->total, njobs = (int)q->njobs;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -400,9 +295,8 @@ __global__ void __launch_bounds__(kDrawFwdThreads, 4) k_draw_queue(DrawQueue* __
     const int item = s_item;
     if (item >= total) break;
     const DrawJob& jb = q->jobs[s_job];
-    if (!draw_tile<K>(item - jb.item0, jb.H, jb.W, jb.gx, jb.ranges, jb.gsid, jb.records,
-                      jb.tau_init, jb.out, jb.contrib, jb.final_tau, sm))
-      break;  // (uniform: draw_tile's result follows a block barrier)
+    draw_tile<K>(item - jb.item0, jb.H, jb.W, jb.gx, jb.ranges, jb.gsid, jb.records, jb.tau_init,
+                 jb.out, jb.contrib, jb.final_tau, srec);
     __syncthreads();  // s_item / s_job are rewritten by the next claim
   }
 }
@@ -505,8 +399,8 @@ struct BwdPixel {
 // pixel's gradient terms into x (x[0..K) features, then alpha, u, conic).
 template <int K, bool GEOM, bool DTAU>
 __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, float4 v0,
-                                              float4 v1, float dx, float dy, const float4* rec,
-                                              float* x) {
+                                              float4 v1, float dx, float dy, const float4* srec,
+                                              int jj, float* x) {
   if (!(idx < p.cont) || m > v1.y) return false;
   const float g = expf(-0.5f * m);
   const float ap = fminf(kAlphaMax, v1.z * g);
@@ -518,7 +412,7 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
   for (int k = 0; k < K; ++k) x[k] += p.dl[k] * wgt;
   if (GEOM) {
     float f[K];
-    load_feats<K>(rec, v1.w, f);
+    load_feats<K>(srec, jj, v1.w, f);
     float dap = 0.f;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -544,13 +438,13 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
 // exchange at offset 16 leaves ja's partial sums on lanes 0-15 and jb's on
 // lanes 16-31, then each half-warp transposes its K values (5 + 8 shuffles
 // for K = 5, against 2 x 9 for two single reductions).
-template <int K, int S>
+template <int K>
 __device__ __forceinline__ void adjoint_weights_pair(BwdPixel<K> (&p)[2], int base, int ja, int jb,
-                                                     const float4* rs, const int32_t* sgid,
+                                                     const float4* srec, const int32_t* sgid,
                                                      float fx, float fy0, float fy1, int lane,
                                                      float* __restrict__ dfeat) {
-  const float4 a0 = rs[ja * S], a1 = rs[ja * S + 1];
-  const float4 b0 = rs[jb * S], b1 = rs[jb * S + 1];
+  const float4 a0 = srec[ja], a1 = srec[kBatch + ja];
+  const float4 b0 = srec[jb], b1 = srec[kBatch + jb];
   const float fy[2] = {fy0, fy1};
   float apa[2], apb[2];
   bool ua[2], ub[2];
@@ -641,9 +535,9 @@ __device__ __forceinline__ float* grad_slot(int v, int64_t g, float* dfeat, floa
 // together: one exchange at lane offset 16 leaves ja's partial sums on lanes
 // 0-15 and jb's on lanes 16-31, then each half-warp transposes its values
 // (K + 6 + 15 shuffles for the pair instead of 2 x 16 for K = 3..8).
-template <int K, bool DTAU, int S>
+template <int K, bool DTAU>
 __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base, int ja, int jb,
-                                                  const float4* rs, const int32_t* sgid,
+                                                  const float4* srec, const int32_t* sgid,
                                                   float fx, float fy0, float fy1, int lane,
                                                   float* __restrict__ dfeat,
                                                   float* __restrict__ dalpha,
@@ -652,8 +546,8 @@ __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base,
   constexpr int NREAL = K + 6;
   constexpr int NV = Pow2<NREAL>::value;
   static_assert(NV <= 16, "half-warp transposition holds at most 16 values");
-  const float4 a0 = rs[ja * S], a1 = rs[ja * S + 1];
-  const float4 b0 = rs[jb * S], b1 = rs[jb * S + 1];
+  const float4 a0 = srec[ja], a1 = srec[kBatch + ja];
+  const float4 b0 = srec[jb], b1 = srec[kBatch + jb];
   float xa[NV], xb[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) xa[v] = xb[v] = 0.f;
@@ -663,12 +557,10 @@ __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base,
   const float ma1 = fmaxf(0.f, maha_sq(a0.z, a0.w, a1.x, dxa, dya1));
   const float mb0 = fmaxf(0.f, maha_sq(b0.z, b0.w, b1.x, dxb, dyb0));
   const float mb1 = fmaxf(0.f, maha_sq(b0.z, b0.w, b1.x, dxb, dyb1));
-  const float4* ra = rs + ja * S;
-  const float4* rb = rs + jb * S;
-  bool ha = adjoint_pixel<K, true, DTAU>(p[0], base + ja, ma0, a0, a1, dxa, dya0, ra, xa);
-  bool hb = adjoint_pixel<K, true, DTAU>(p[0], base + jb, mb0, b0, b1, dxb, dyb0, rb, xb);
-  ha |= adjoint_pixel<K, true, DTAU>(p[1], base + ja, ma1, a0, a1, dxa, dya1, ra, xa);
-  hb |= adjoint_pixel<K, true, DTAU>(p[1], base + jb, mb1, b0, b1, dxb, dyb1, rb, xb);
+  bool ha = adjoint_pixel<K, true, DTAU>(p[0], base + ja, ma0, a0, a1, dxa, dya0, srec, ja, xa);
+  bool hb = adjoint_pixel<K, true, DTAU>(p[0], base + jb, mb0, b0, b1, dxb, dyb0, srec, jb, xb);
+  ha |= adjoint_pixel<K, true, DTAU>(p[1], base + ja, ma1, a0, a1, dxa, dya1, srec, ja, xa);
+  hb |= adjoint_pixel<K, true, DTAU>(p[1], base + jb, mb1, b0, b1, dxb, dyb1, srec, jb, xb);
   const unsigned ca = __ballot_sync(0xffffffffu, ha), cb = __ballot_sync(0xffffffffu, hb);
   if (!(ca | cb)) return;
   if (__popc(ca) <= 1 && __popc(cb) <= 1) {
@@ -717,7 +609,7 @@ __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base,
 // (vanilla_3dgs/gsplatcu/kernel.cu:912-919).  As in the reference, the 0.99
 // clamp and max(0, .) are not differentiated.
 template <int K, bool GEOM, bool DTAU>
-__global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 8)
+__global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
     k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
                     const int32_t* __restrict__ gsid, const float4* __restrict__ records,
                     const int32_t* __restrict__ contrib, const float* __restrict__ final_tau,
@@ -725,14 +617,12 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 8)
                     float* __restrict__ dfeat, float* __restrict__ dalpha,
                     float* __restrict__ du, float* __restrict__ dconic) {
   pdl_wait();
-  constexpr int V = RecordLayout<K>::kVec4, S = Ring<V>::S;
+  constexpr int V = RecordLayout<K>::kVec4;
   constexpr int NREAL = GEOM ? K + 6 : K;
   constexpr int NV = Pow2<NREAL>::value;
-  __shared__ __align__(16) float4 srec[2][kBatchB * S];
-  __shared__ int32_t sgid[2][kBatchB];
-  __shared__ __align__(8) uint64_t full[2];
+  __shared__ float4 srec[V * kBatch];
+  __shared__ int32_t sgid[kBatch];
   __shared__ unsigned s_maxc;
-  __shared__ int s_fail;
   const PixelPair pp = pixels_of(blockIdx.x, gx);
   const int lane = threadIdx.x & 31;
   const int2 rg = ranges[blockIdx.x];
@@ -755,137 +645,91 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 8)
     p[q].cont = in ? contrib[pix] : 0;
   }
   const int wmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(p[0].cont, p[1].cont));
-  if (threadIdx.x == 0) {
-    s_maxc = 0u;
-    s_fail = 0;
-    mbar_init(&full[0], blockDim.x);  // one arrival per thread per fill
-    mbar_init(&full[1], blockDim.x);
-  }
+  if (threadIdx.x == 0) s_maxc = 0u;
   __syncthreads();
   if (lane == 0) atomicMax(&s_maxc, (unsigned)wmax);
   __syncthreads();
   // contributor indices never exceed the tile's list (clamped for safety
-  // against mismatched inputs); batches are walked from the last contributor
-  // down: batch b covers list positions [top_b - cnt_b, top_b)
+  // against mismatched inputs)
   const int maxc = min((int)s_maxc, rg.y - rg.x);
-  const int nb = (maxc + kBatchB - 1) / kBatchB;
-  const auto lo_of = [&](int b) { return max(0, maxc - (b + 1) * kBatchB); };
-  const auto cnt_of = [&](int b) { return maxc - b * kBatchB - lo_of(b); };
-  static_assert(kBatchB == kDrawThreads, "one record per thread per batch");
-  if (nb > 0) {
-    const int g0 = fetch_id(gsid, rg.x + lo_of(0), cnt_of(0));
-    const int g1 = nb > 1 ? fetch_id(gsid, rg.x + lo_of(1), cnt_of(1)) : -1;
-    fill_slot<V>(g0, records, srec[0], sgid[0], &full[0]);
-    if (nb > 1) fill_slot<V>(g1, records, srec[1], sgid[1], &full[1]);
-  }
   const float fx = (float)pp.px, fy0 = (float)pp.py0, fy1 = (float)pp.py1;
-  for (int b = 0; b < nb; ++b) {
-    const int buf = b & 1, base = lo_of(b), cnt = cnt_of(b);
-    const float4* rs = srec[buf];
-    const int32_t* sg = sgid[buf];
-    const int gnext = b + 2 < nb ? fetch_id(gsid, rg.x + lo_of(b + 2), cnt_of(b + 2)) : -1;
-    const bool landed = mbar_wait(&full[buf], (b >> 1) & 1);
-    if (!landed) s_fail = 1;
-    const int hi = min(cnt, wmax - base);
-    if (__all_sync(0xffffffffu, landed)) {
-      for (int s_hi = hi; s_hi > 0; s_hi -= 32) {
-        const int s_lo = max(0, s_hi - 32);
-        const int j = s_lo + lane;
-        bool ov = j < s_hi && box_meets_block(rs[j * S], rs[j * S + 2], pp.wx, pp.wy, 7, 7);
-        if (ov)
-          ov = ellipse_meets_block(rs[j * S], rs[j * S + 1], rs[j * S + 2], (float)pp.wx,
-                                   (float)pp.wy, (float)(pp.wx + 7), (float)(pp.wy + 7));
-        unsigned mask = __ballot_sync(0xffffffffu, ov);
-        while (mask) {
-          const int msb = 31 - __clz(mask);
-          mask &= ~(1u << msb);
-          if (mask) {
-            const int msb2 = 31 - __clz(mask);
-            mask &= ~(1u << msb2);
-            if constexpr (GEOM)
-              adjoint_geom_pair<K, DTAU, S>(p, base, s_lo + msb, s_lo + msb2, rs, sg, fx, fy0,
-                                            fy1, lane, dfeat, dalpha, du, dconic);
-            else
-              adjoint_weights_pair<K, S>(p, base, s_lo + msb, s_lo + msb2, rs, sg, fx, fy0, fy1,
-                                         lane, dfeat);
-            continue;
-          }
-          const int jj = s_lo + msb;
-          const int idx = base + jj;
-          float x[NV];
-#pragma unroll
-          for (int v = 0; v < NV; ++v) x[v] = 0.f;
-          const float4* r = rs + jj * S;
-          const float4 v0 = r[0];
-          const float4 v1 = r[1];
-          const float dx = v0.x - fx, dy0 = v0.y - fy0, dy1 = v0.y - fy1;
-          const float m0 = fmaxf(0.f, maha_sq(v0.z, v0.w, v1.x, dx, dy0));
-          const float m1 = fmaxf(0.f, maha_sq(v0.z, v0.w, v1.x, dx, dy1));
-          bool hit = adjoint_pixel<K, GEOM, DTAU>(p[0], idx, m0, v0, v1, dx, dy0, r, x);
-          hit |= adjoint_pixel<K, GEOM, DTAU>(p[1], idx, m1, v0, v1, dx, dy1, r, x);
-          const unsigned cm = __ballot_sync(0xffffffffu, hit);
-          if (!cm) continue;
-          const int64_t g = sg[jj];
-          if (__popc(cm) == 1) {
-            if (hit) {
-#pragma unroll
-              for (int k = 0; k < K; ++k) atomicAdd(dfeat + g * K + k, x[k]);
-              if (GEOM) {
-                atomicAdd(dalpha + g, x[K]);
-                atomicAdd(du + 2 * g, x[K + 1]);
-                atomicAdd(du + 2 * g + 1, x[K + 2]);
-                atomicAdd(dconic + 3 * g, x[K + 3]);
-                atomicAdd(dconic + 3 * g + 1, x[K + 4]);
-                atomicAdd(dconic + 3 * g + 2, x[K + 5]);
-              }
-            }
-            continue;
-          }
-          int vidx;
-          bool owner;
-          const float tot = warp_transpose_sum<NV>(x, lane, &vidx, &owner);
-          if (owner && vidx < NREAL) atomicAdd(grad_slot<K>(vidx, g, dfeat, dalpha, du, dconic), tot);
-        }
-      }
-    }
-    // every warp is done with this buffer (it may be refilled)
+  for (int top = maxc; top > 0; top -= kBatch) {
+    const int base = max(0, top - kBatch);
+    const int cnt = top - base;
     __syncthreads();
-    if (s_fail || b + 1 >= nb) {
-      if (threadIdx.x == 0) {
-        if (s_fail) {
-          atomicOr(&g_raster_status, kStatusBulkTimeout);
-          mbar_wait(&full[buf], (b >> 1) & 1);
+    stage_batch<V, kDrawThreads>(gsid, rg.x + base, cnt, records, srec, sgid);
+    __syncthreads();
+    const int hi = min(cnt, wmax - base);
+    for (int s_hi = hi; s_hi > 0; s_hi -= 32) {
+      const int s_lo = max(0, s_hi - 32);
+      const int j = s_lo + lane;
+      bool ov = j < s_hi && box_meets_block(srec[j], srec[2 * kBatch + j], pp.wx, pp.wy, 7, 7);
+      if (ov)
+        ov = ellipse_meets_block(srec[j], srec[kBatch + j], srec[2 * kBatch + j], (float)pp.wx,
+                                 (float)pp.wy, (float)(pp.wx + 7), (float)(pp.wy + 7));
+      unsigned mask = __ballot_sync(0xffffffffu, ov);
+      while (mask) {
+        const int msb = 31 - __clz(mask);
+        mask &= ~(1u << msb);
+        if (mask) {
+          const int msb2 = 31 - __clz(mask);
+          mask &= ~(1u << msb2);
+          if constexpr (GEOM)
+            adjoint_geom_pair<K, DTAU>(p, base, s_lo + msb, s_lo + msb2, srec, sgid, fx, fy0, fy1,
+                                       lane, dfeat, dalpha, du, dconic);
+          else
+            adjoint_weights_pair<K>(p, base, s_lo + msb, s_lo + msb2, srec, sgid, fx, fy0, fy1,
+                                    lane, dfeat);
+          continue;
         }
-        if (b + 1 < nb) mbar_wait(&full[buf ^ 1], ((b + 1) >> 1) & 1);
+        const int jj = s_lo + msb;
+        const int idx = base + jj;
+        float x[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) x[v] = 0.f;
+        const float4 v0 = srec[jj];
+        const float4 v1 = srec[kBatch + jj];
+        const float dx = v0.x - fx, dy0 = v0.y - fy0, dy1 = v0.y - fy1;
+        const float m0 = fmaxf(0.f, maha_sq(v0.z, v0.w, v1.x, dx, dy0));
+        const float m1 = fmaxf(0.f, maha_sq(v0.z, v0.w, v1.x, dx, dy1));
+        bool hit = adjoint_pixel<K, GEOM, DTAU>(p[0], idx, m0, v0, v1, dx, dy0, srec, jj, x);
+        hit |= adjoint_pixel<K, GEOM, DTAU>(p[1], idx, m1, v0, v1, dx, dy1, srec, jj, x);
+        const unsigned cm = __ballot_sync(0xffffffffu, hit);
+        if (!cm) continue;
+        const int64_t g = sgid[jj];
+        if (__popc(cm) == 1) {
+          if (hit) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) atomicAdd(dfeat + g * K + k, x[k]);
+            if (GEOM) {
+              atomicAdd(dalpha + g, x[K]);
+              atomicAdd(du + 2 * g, x[K + 1]);
+              atomicAdd(du + 2 * g + 1, x[K + 2]);
+              atomicAdd(dconic + 3 * g, x[K + 3]);
+              atomicAdd(dconic + 3 * g + 1, x[K + 4]);
+              atomicAdd(dconic + 3 * g + 2, x[K + 5]);
+            }
+          }
+          continue;
+        }
+        int vidx;
+        bool owner;
+        const float tot = warp_transpose_sum<NV>(x, lane, &vidx, &owner);
+        if (owner && vidx < NREAL) {
+          float* dst;
+          if (vidx < K)
+            dst = dfeat + g * K + vidx;
+          else if (vidx == K)
+            dst = dalpha + g;
+          else if (vidx < K + 3)
+            dst = du + 2 * g + (vidx - K - 1);
+          else
+            dst = dconic + 3 * g + (vidx - K - 3);
+          atomicAdd(dst, tot);
+        }
       }
-      break;
     }
-    if (b + 2 < nb) fill_slot<V>(gnext, records, srec[buf], sgid[buf], &full[buf]);
   }
-}
-
-// ------------------------------------------------------------ status
-const uint32_t* raster_status_word() {
-  void* p = nullptr;
-  if (cudaGetSymbolAddress(&p, g_raster_status) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return nullptr;
-  }
-  return (const uint32_t*)p;
-}
-
-int raster_status(uint32_t* out, bool clear, cudaStream_t st) {
-  if (cudaMemcpyFromSymbolAsync(out, g_raster_status, sizeof(uint32_t), 0,
-                                cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    return check_launch("device_status", 0);
-  if (clear) {
-    const uint32_t zero = 0;
-    if (cudaMemcpyToSymbolAsync(g_raster_status, &zero, sizeof(uint32_t), 0,
-                                cudaMemcpyHostToDevice, st) != cudaSuccess)
-      return check_launch("device_status", 0);
-  }
-  if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("device_status", 0);
-  return GSB_OK;
 }
 
 // ------------------------------------------------------------ launchers

@@ -306,7 +306,6 @@ def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_
              ptr(ranges), None, st)  # (status read above)
         call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(full), ptr(state),
              float(tau_init), ptr(out), ptr(contrib), ptr(final_tau), st)
-        _lib.fetch_device_status(dev, st)  # (read at the next check)
         counted.synchronize()
         _lib.raise_if_timed_out(dev, op)
         if int(host[0]) == 0:
@@ -322,7 +321,6 @@ def _sort_and_draw(op, n, H, W, C_, state, ranges, out, contrib, final_tau, tau_
          st)
     call(op, "gsb_splat_draw", n, H, W, C_, ptr(ranges), ptr(gsid), ptr(state), float(tau_init),
          ptr(out), ptr(contrib), ptr(final_tau), st)
-    _lib.fetch_device_status(dev, st)  # (read at the next check)
     _CAPACITY[key] = (int(M * 1.25) + 4096, (1 << int(plan.max_depth_key).bit_length()) - 1)
     return gsid
 
@@ -434,14 +432,12 @@ def _splat_backward(op, H, W, C_, us, cinv2ds, alphas, feats, contrib, final_tau
             call(op, "gsb_splat_backward_packed", n, H, W, C_, ptr(ranges), ptr(gsid),
                  ptr(contrib), ptr(final_tau), ptr(dloss), ptr(dtau), ptr(packed), ptr(dfeat),
                  ptr(dalpha), ptr(du), ptr(dq), stream_of(us))
-            _lib.fetch_device_status(dev, stream_of(us))
             return dfeat, dalpha, du, dq
         state = torch.empty(int(_lib.lib().gsb_splat_state_bytes(n, C_, H, W)),
                             dtype=torch.uint8, device=dev)
         call(op, "gsb_splat_backward", n, H, W, C_, ptr(us), ptr(cinv), ptr(alphas), ptr(feats),
              _sh_dtype(feats), ptr(ranges), ptr(gsid), ptr(contrib), ptr(final_tau), ptr(dloss),
              ptr(dtau), ptr(state), ptr(dfeat), ptr(dalpha), ptr(du), ptr(dq), stream_of(us))
-        _lib.fetch_device_status(dev, stream_of(us))
     return dfeat, dalpha, du, dq
 
 
