@@ -261,14 +261,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(kernel_tag):
-    """Per-launch DRAM traffic of a kernel from a committed ncu summary
-    (profiles/<kernel_tag>.md, line 'traffic_bytes_per_launch: N')."""
+def profile_figure(kernel_tag, key):
+    """A per-launch figure of a kernel from its committed ncu summary
+    (profiles/<kernel_tag>.md, a line '<key>: N'): traffic_bytes_per_launch
+    (dram__bytes_read.sum + dram__bytes_write.sum), warp_inst_per_launch
+    (smsp__inst_executed.sum), inst_per_blended_pair."""
     p = os.path.join(ROOT, "profiles", kernel_tag + ".md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
@@ -827,8 +829,14 @@ def run_b200(a):
     achieved = dom_bytes / (stages[dom] / 1000.0) / 1e9
     tag = {"draw": "k_draw_1M_1080p", "draw_backward": "k_draw_backward_1M_1080p"}[dom]
     roof = dict(bound="hbm", kernel=f"k_{dom}", achieved=round(achieved, 1), peak=peak,
-                unit="GB/s", frac=round(achieved / peak, 4), traffic=profile_traffic(tag),
+                unit="GB/s", frac=round(achieved / peak, 4),
+                traffic=profile_figure(tag, "traffic_bytes_per_launch"),
                 algorithmic_bytes=int(dom_bytes), launch_ms=round(stages[dom], 4),
+                warp_inst_per_launch=profile_figure(tag, "warp_inst_per_launch"),
+                inst_per_blended_pair=profile_figure(tag, "inst_per_blended_pair"),
+                bound_note="issue-bound: the HBM fraction is low by construction; "
+                           "warp instructions per blended (pixel, Gaussian) pair is the figure "
+                           "the kernel design moves",
                 peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s")
 

@@ -437,7 +437,12 @@ __device__ __forceinline__ bool adjoint_pixel(BwdPixel<K>& p, int idx, float m, 
 // of adjoint_pixel.  The two gradient vectors are summed together: one
 // exchange at offset 16 leaves ja's partial sums on lanes 0-15 and jb's on
 // lanes 16-31, then each half-warp transposes its K values (5 + 8 shuffles
-// for K = 5, against 2 x 9 for two single reductions).
+// for K = 5, against 2 x 9 for two single reductions).  When at most
+// kDirectLanes lanes hit each record, those lanes add their own sums
+// directly (at most 2 x kDirectLanes x K atomics instead of about 60
+// reduction instructions; a quarter of the records a warp visits have so few
+// hits at 1M Gaussians, 1080p).
+constexpr int kDirectLanes = 4;
 template <int K>
 __device__ __forceinline__ void adjoint_weights_pair(BwdPixel<K> (&p)[2], int base, int ja, int jb,
                                                      const float4* srec, const int32_t* sgid,
@@ -483,7 +488,7 @@ __device__ __forceinline__ void adjoint_weights_pair(BwdPixel<K> (&p)[2], int ba
   const bool ha = ua[0] || ua[1], hb = ub[0] || ub[1];
   const unsigned ca = __ballot_sync(0xffffffffu, ha), cb = __ballot_sync(0xffffffffu, hb);
   if (!(ca | cb)) return;
-  if (__popc(ca) <= 1 && __popc(cb) <= 1) {
+  if (__popc(ca) <= kDirectLanes && __popc(cb) <= kDirectLanes) {
     if (ha) {
       const int64_t g = sgid[ja];
 #pragma unroll

@@ -251,8 +251,7 @@ class _Batch:
             raise _lib.GsplatError(f"serve: table copy failed ({err})")
         _lib.call("serve", "gsb_draw_batch", _lib.ptr(self.dev), 3, st)
         # the library's device status bits (a bounded wait of the members'
-        # preprocess or of the compositing ran out), fetched into a word
-        # cleared first
+        # preprocess ran out), fetched into a word cleared first
         self.status.zero_()
         _lib.call("serve", "gsb_device_status_fetch", _lib.ptr(self.status), st)
         err, = _rt.cudaMemcpyAsync(self.status_host.data_ptr(), self.status.data_ptr(), 4,
