@@ -161,103 +161,162 @@ __global__ void __launch_bounds__(kThreads)
 // sh2Weight / sh2Color -- gsplatcu/kernel.cu:670-870, 1040-1169.  Both are the
 // same map feat_k = sum_l Y_l(dir) c[l*K + k] (band-major); colours are K = 3.
 // All Gaussians are evaluated (no depth test), as in the reference.
-// A Gaussian's coefficient row is nb*K values (up to 128); read one row per
+// A Gaussian's coefficient row is NB*K values (up to 128); read one row per
 // thread straight from global memory, a warp's loads would be strided by the
 // row length and thrash L1.  The block's rows, one contiguous span, are
-// therefore copied first (coalesced, kShCopy loads in flight per thread) into
-// shared memory at an odd row stride, where each thread reads its own row
-// without bank conflicts.
+// therefore copied first into shared memory at an odd row stride, where each
+// thread reads its own row without bank conflicts: one 4-byte asynchronous
+// copy (cp.async) per element (FP32) or element pair (BF16), so the whole
+// span is in flight at once without holding registers.  The band count NB is
+// a template parameter, so the basis, its gradient and the Jacobian sums stay
+// in registers.  The outputs (K weights, and with the Jacobians NB basis
+// values and 3K direction derivatives per Gaussian) are gathered in shared
+// memory at odd row strides and written back as contiguous spans of the
+// block's rows.
 constexpr int kShThreads = 64;  // 64 rows of at most 129 floats: 33 KB of shared memory
-constexpr int kShCopy = 8;
 
-template <int K, typename T>
+template <int K, int NB>
+struct ShOut {
+  static constexpr int SK = K | 1, SNB = NB | 1, S3K = (3 * K) | 1;
+  static constexpr int kFloats = kShThreads * (SK + SNB + S3K);  // with the Jacobians
+};
+
+// Copies `rows` rows of `w` floats from shared memory (row stride `ws`) to
+// the contiguous global span `dst`, one float per thread per step.
+template <int w, int ws>
+__device__ __forceinline__ void rows_out(const float* src, int rows, float* __restrict__ dst) {
+  for (int e = threadIdx.x; e < rows * w; e += kShThreads) {
+    const int r = e / w;
+    dst[e] = src[r * ws + (e - r * w)];
+  }
+}
+
+template <int K, int NB, typename T>
 __global__ void __launch_bounds__(kShThreads)
-    k_sh2feat(int64_t n, const T* __restrict__ shs, int nb, bool staged,
+    k_sh2feat(int64_t n, const T* __restrict__ shs, bool staged,
               const float* __restrict__ pws, const float* __restrict__ twc,
               float* __restrict__ feat, float* __restrict__ dshs, float* __restrict__ dpws) {
   extern __shared__ float srows[];
-  const int rl = nb * K, stride = rl | 1;
+  constexpr int rl = NB * K, stride = rl | 1;
+  // staged BF16 rows: 32-bit words per row and the row stride in words
+  // (odd BF16 rows are never staged)
+  constexpr int kBfWords = rl / 2 > 0 ? rl / 2 : 1, kBfStride = kBfWords | 1;
+  using O = ShOut<K, NB>;
   const int64_t row0 = (int64_t)blockIdx.x * kShThreads;
   const int rows = (int)min((int64_t)kShThreads, n - row0);
-  // FP32 rows are copied element by element; BF16 rows of even length from a
-  // 4-byte aligned base as element pairs, one 32-bit load each (2-byte
-  // element loads cost more than the strided reads they replace); other BF16
-  // rows are read in place.  The host makes that decision (`staged`) and
+  // FP32 rows are copied element by element, BF16 rows of even length from a
+  // 4-byte aligned base as element pairs (2-byte copies cost more than the
+  // strided reads they replace); other BF16 rows are read in place.  The host makes that decision (`staged`) and
   // sizes the shared memory by it.
   constexpr bool kF32 = sizeof(T) == 4;
-  if (staged) {
-    // G elements per load; (row, column) of load e advanced by kShThreads
-    // loads per step
-    const int G = kF32 ? 1 : 2;
-    const int rlg = rl / G, total = rows * rlg;
-    int r = threadIdx.x / rlg, q = threadIdx.x - r * rlg;
-    const int dr = kShThreads / rlg, dq = kShThreads - dr * rlg;
-    for (int e0 = threadIdx.x; e0 < total; e0 += kShCopy * kShThreads) {
-      float2 v[kShCopy];
-      int at[kShCopy];
-#pragma unroll
-      for (int u = 0; u < kShCopy; ++u) {
-        const int e = e0 + u * kShThreads;
-        if constexpr (kF32) {
-          v[u].x = e < total ? ld(shs + row0 * rl, e) : 0.f;
-        } else {
-          const __nv_bfloat162* src = reinterpret_cast<const __nv_bfloat162*>(shs + row0 * rl);
-          v[u] = e < total ? __bfloat1622float2(src[e]) : make_float2(0.f, 0.f);
-        }
-        at[u] = r * stride + q * G;
-        q += dq;
-        r += dr;
-        if (q >= rlg) {
-          q -= rlg;
-          ++r;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kShCopy; ++u) {
-        if (e0 + u * kShThreads < total) {
-          srows[at[u]] = v[u].x;
-          if constexpr (!kF32) srows[at[u] + 1] = v[u].y;
-        }
+  if (kF32 && staged) {
+    // FP32: every element of the block's span is one 4-byte asynchronous
+    // copy (cp.async), so the whole span is in flight at once without
+    // holding registers; (row, column) of element e advanced by kShThreads
+    // elements per step
+    const float* src = reinterpret_cast<const float*>(shs) + row0 * rl;
+    const int total = rows * rl;
+    int r = threadIdx.x / rl, q = threadIdx.x - r * rl;
+    constexpr int dr = kShThreads / rl, dq = kShThreads - dr * rl;
+    for (int e = threadIdx.x; e < total; e += kShThreads) {
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(srows + r * stride + q)),
+                   "l"(src + e)
+                   : "memory");
+      q += dq;
+      r += dr;
+      if (q >= rl) {
+        q -= rl;
+        ++r;
       }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (staged) {
+    // BF16 rows of even length from a 4-byte aligned base: each element pair
+    // is one 4-byte asynchronous copy, kept raw at an odd row stride of
+    // 32-bit words and converted when read
+    uint32_t* dst = reinterpret_cast<uint32_t*>(srows);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(shs + row0 * rl);
+    const int total = rows * kBfWords;
+    int r = threadIdx.x / kBfWords, q = threadIdx.x - r * kBfWords;
+    constexpr int dr = kShThreads / kBfWords, dq = kShThreads - dr * kBfWords;
+    for (int e = threadIdx.x; e < total; e += kShThreads) {
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(dst + r * kBfStride + q)),
+                   "l"(src + e)
+                   : "memory");
+      q += dq;
+      r += dr;
+      if (q >= kBfWords) {
+        q -= kBfWords;
+        ++r;
+      }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
   }
   __syncthreads();
   const int64_t i = row0 + threadIdx.x;
-  if (i >= n) return;
-  const float* srow = srows + threadIdx.x * stride;
-  const T* grow = shs + i * (int64_t)rl;
-  const auto c = [&](int idx) { return staged ? srow[idx] : ld(grow, idx); };
-  float dir[3] = {0.f, 0.f, 0.f}, nd[3] = {0.f, 0.f, 0.f}, ninv = 0.f;
-  float Y[16];
-  if (nb > 1) {
-    const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
-    const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
-    view_direction(pw, cam, dir, nd, &ninv);
-  }
-  sh_basis(dir, nb, Y);
-  float acc[K];
-  sh_weights_full<K>(c, nb, Y, acc);
-#pragma unroll
-  for (int k = 0; k < K; ++k) feat[i * K + k] = acc[k];
-  if (dshs) {
-    for (int l = 0; l < nb; ++l) dshs[i * nb + l] = Y[l];
-    float G[48], J[9];
-    sh_basis_grad(dir, nb, /*ref_quirk=*/true, G);
-    if (nb > 1) dir_jacobian(nd, ninv, J);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      float dd[3] = {0.f, 0.f, 0.f};
-      for (int l = 1; l < nb; ++l) {
-        const float cv = c(l * K + k);
-        dd[0] += G[3 * l] * cv;
-        dd[1] += G[3 * l + 1] * cv;
-        dd[2] += G[3 * l + 2] * cv;
-      }
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-        dpws[(i * K + k) * 3 + j] =
-            nb > 1 ? dd[0] * J[j] + dd[1] * J[3 + j] + dd[2] * J[6 + j] : 0.f;
+  const bool live = i < n;
+  const bool jac = dshs != nullptr;
+  float acc[K], Y[16], dp[3 * K];
+  if (live) {
+    const float* srow = srows + threadIdx.x * stride;
+    const __nv_bfloat16* sraw = reinterpret_cast<const __nv_bfloat16*>(
+        reinterpret_cast<const uint32_t*>(srows) + threadIdx.x * kBfStride);
+    const T* grow = shs + i * (int64_t)rl;
+    const auto c = [&](int idx) {
+      if constexpr (kF32)
+        return staged ? srow[idx] : ld(grow, idx);
+      else
+        return staged ? __bfloat162float(sraw[idx]) : ld(grow, idx);
+    };
+    float dir[3] = {0.f, 0.f, 0.f}, nd[3] = {0.f, 0.f, 0.f}, ninv = 0.f;
+    if (NB > 1) {
+      const float3 pw = make_float3(pws[3 * i], pws[3 * i + 1], pws[3 * i + 2]);
+      const float3 cam = make_float3(__ldg(twc), __ldg(twc + 1), __ldg(twc + 2));
+      view_direction(pw, cam, dir, nd, &ninv);
     }
+    sh_basis(dir, NB, Y);
+    sh_weights_full<K>(c, NB, Y, acc);
+    if (jac) {
+      float Gd[48], J[9];
+      sh_basis_grad(dir, NB, /*ref_quirk=*/true, Gd);
+      if (NB > 1) dir_jacobian(nd, ninv, J);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        float dd[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int l = 1; l < NB; ++l) {
+          const float cv = c(l * K + k);
+          dd[0] += Gd[3 * l] * cv;
+          dd[1] += Gd[3 * l + 1] * cv;
+          dd[2] += Gd[3 * l + 2] * cv;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          dp[3 * k + j] = NB > 1 ? dd[0] * J[j] + dd[1] * J[3 + j] + dd[2] * J[6 + j] : 0.f;
+      }
+    }
+  }
+  __syncthreads();  // the staged rows are no longer read
+  float* s_feat = srows;
+  float* s_y = s_feat + kShThreads * O::SK;
+  float* s_dp = s_y + kShThreads * O::SNB;
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) s_feat[threadIdx.x * O::SK + k] = acc[k];
+    if (jac) {
+#pragma unroll
+      for (int l = 0; l < NB; ++l) s_y[threadIdx.x * O::SNB + l] = Y[l];
+#pragma unroll
+      for (int m = 0; m < 3 * K; ++m) s_dp[threadIdx.x * O::S3K + m] = dp[m];
+    }
+  }
+  __syncthreads();
+  rows_out<K, O::SK>(s_feat, rows, feat + row0 * K);
+  if (jac) {
+    rows_out<NB, O::SNB>(s_y, rows, dshs + row0 * NB);
+    rows_out<3 * K, O::S3K>(s_dp, rows, dpws + row0 * 3 * K);
   }
 }
 
@@ -294,6 +353,20 @@ int launch_inverse_cov2d(int64_t n, const float* cov2ds, float* depths, float* c
   return check_launch("inverseCov2D");
 }
 
+template <int K, typename T>
+static int sh2feat_kn(int64_t n, const T* s, int nb, bool staged, size_t smem, int g,
+                      const float* pws, const float* twc, float* feat, float* dshs, float* dpws,
+                      cudaStream_t st) {
+  switch (nb) {
+    case 1: k_sh2feat<K, 1, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
+    case 4: k_sh2feat<K, 4, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
+    case 9: k_sh2feat<K, 9, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
+    case 16: k_sh2feat<K, 16, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
+    default: return GSB_ERR_INVALID_ARGUMENT;
+  }
+  return GSB_OK;
+}
+
 template <typename T>
 static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws, const float* twc,
                      float* feat, float* dshs, float* dpws, cudaStream_t st) {
@@ -303,16 +376,26 @@ static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws
   // from a 4-byte aligned base
   const bool staged = sizeof(T) == 4 ||
                       ((nb * K) % 2 == 0 && (reinterpret_cast<uintptr_t>(shs) & 3) == 0);
-  const size_t smem = staged ? (size_t)kShThreads * ((nb * K) | 1) * sizeof(float) : 0;
+  const size_t row_words = sizeof(T) == 4 ? (size_t)((nb * K) | 1)
+                                           : (size_t)(((nb * K) / 2) | 1);  // raw BF16 pairs
+  const size_t stage_bytes = staged ? (size_t)kShThreads * row_words * 4 : 0;
+  // output gathering: K weights, NB basis values and 3K derivatives per row
+  // at odd strides (the NB + 3K part only with the Jacobians, but always
+  // reserved: it is small)
+  const size_t out_bytes =
+      (size_t)kShThreads * ((K | 1) + (nb | 1) + ((3 * K) | 1)) * sizeof(float);
+  const size_t smem = stage_bytes > out_bytes ? stage_bytes : out_bytes;
+  int rc;
   switch (K) {
-#define GSB_K(KK)                                                                              \
-  case KK:                                                                                     \
-    k_sh2feat<KK, T><<<g, kShThreads, smem, st>>>(n, s, nb, staged, pws, twc, feat, dshs, dpws); \
+#define GSB_K(KK)                                                                          \
+  case KK:                                                                                 \
+    rc = sh2feat_kn<KK, T>(n, s, nb, staged, smem, g, pws, twc, feat, dshs, dpws, st);     \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K
     default: return GSB_ERR_INVALID_ARGUMENT;
   }
+  if (rc) return rc;
   return check_launch("sh2Weight");
 }
 
