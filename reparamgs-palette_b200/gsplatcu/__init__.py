@@ -29,7 +29,7 @@ import threading
 import torch
 
 from . import _lib
-from ._lib import GsplatError, call, ptr, stream_of
+from ._lib import GsplatError, call, on_device, ptr, stream_of
 
 __all__ = [
     "project", "computeCov3D", "computeCov2D", "inverseCov2D", "sh2Weight", "sh2Weight_fast",
@@ -86,7 +86,7 @@ def project(pws, Rcw, tcw, focal_x, focal_y, center_x, center_y, calc_J):
     n = _n(pws)
     us, pcs, depths = _empty((n, 2), pws), _empty((n, 3), pws), _empty((n,), pws)
     du = _empty((n, 2, 3), pws) if calc_J else None
-    with torch.cuda.device(pws.device):
+    with on_device(pws.device):
         call(op, "gsb_project", n, ptr(pws), ptr(Rcw), ptr(tcw), float(focal_x), float(focal_y),
              float(center_x), float(center_y), ptr(us), ptr(pcs), ptr(depths), ptr(du),
              stream_of(pws))
@@ -102,7 +102,7 @@ def computeCov3D(rots, scales, depths, calc_J):
     cov = _empty((n, 6), rots)
     dq = _empty((n, 6, 4), rots) if calc_J else None
     ds = _empty((n, 6, 3), rots) if calc_J else None
-    with torch.cuda.device(rots.device):
+    with on_device(rots.device):
         call(op, "gsb_compute_cov3d", n, ptr(rots), ptr(scales), ptr(depths), ptr(cov), ptr(dq),
              ptr(ds), stream_of(rots))
     return [cov, dq, ds] if calc_J else [cov]
@@ -117,7 +117,7 @@ def computeCov2D(cov3ds, pcs, Rcw, depths, focal_x, focal_y, width, height, calc
     out = _empty((n, 3), pcs)
     d3 = _empty((n, 3, 6), pcs) if calc_J else None
     dp = _empty((n, 3, 3), pcs) if calc_J else None
-    with torch.cuda.device(pcs.device):
+    with on_device(pcs.device):
         call(op, "gsb_compute_cov2d", n, ptr(cov3ds), ptr(pcs), ptr(Rcw), ptr(depths),
              float(focal_x), float(focal_y), float(width), float(height), ptr(out), ptr(d3),
              ptr(dp), stream_of(pcs))
@@ -134,7 +134,7 @@ def inverseCov2D(cov2ds, depths, calc_J):
     cinv = _empty((n, 3), cov2ds)
     areas = _empty((n, 2), cov2ds, torch.int32)
     dc = _empty((n, 3, 3), cov2ds) if calc_J else None
-    with torch.cuda.device(cov2ds.device):
+    with on_device(cov2ds.device):
         call(op, "gsb_inverse_cov2d", n, ptr(cov2ds), ptr(depths), ptr(cinv), ptr(areas), ptr(dc),
              stream_of(cov2ds))
     return [cinv, areas, dc] if calc_J else [cinv, areas]
@@ -158,7 +158,7 @@ def sh2Weight(shs, pws, twc, calc_J, num_palette):
     w = _empty((n, K), pws)
     dshs = _empty((n, 1, nb), pws) if calc_J else None
     dpws = _empty((n, K, 3), pws) if calc_J else None
-    with torch.cuda.device(pws.device):
+    with on_device(pws.device):
         call(op, "gsb_sh2weight", n, ptr(shs), _sh_dtype(shs), nb, K, ptr(pws), ptr(twc), ptr(w),
              ptr(dshs), ptr(dpws), stream_of(pws))
     return [w, dshs, dpws] if calc_J else [w]
@@ -174,7 +174,7 @@ def sh2Color(shs, pws, twc, calc_J):
     col = _empty((n, 3), pws)
     dshs = _empty((n, 1, nb), pws) if calc_J else None
     dpws = _empty((n, 3, 3), pws) if calc_J else None
-    with torch.cuda.device(pws.device):
+    with on_device(pws.device):
         call(op, "gsb_sh2color", n, ptr(shs), _sh_dtype(shs), nb, ptr(pws), ptr(twc), ptr(col),
              ptr(dshs), ptr(dpws), stream_of(pws))
     return [col, dshs, dpws] if calc_J else [col]
@@ -210,7 +210,7 @@ def sh2Weight_fast(shs_dc, shs_A, shs_B, pws, twc, calc_J, num_palette, Q):
     w = _empty((n, K), pws)
     ddc = _empty((n, K), pws) if calc_J else None
     ylm = _empty((n, L), pws) if calc_J else None
-    with torch.cuda.device(pws.device):
+    with on_device(pws.device):
         st = stream_of(pws)
         call(op, "gsb_sh2weight_fast", n, ptr(dc), ptr(A), ptr(B), _sh_dtype(A), K, P, Q, rank,
              ptr(pws), ptr(twc), ptr(w), ptr(ddc), ptr(ylm), st)
@@ -230,7 +230,7 @@ def sh2Weight_fast_B(shs_A, shs_B, Ylm_stored, dloss_dw, num_palette, Q):
     if int(ylm.shape[1]) * K != P * Q:
         raise ValueError(f"gsplatcu.{op}: Ylm has {int(ylm.shape[1])} bands but P*Q/K = {P * Q // K}")
     dA, dB = _empty(tuple(A.shape), A), _empty(tuple(B.shape), A)
-    with torch.cuda.device(A.device):
+    with on_device(A.device):
         st = stream_of(A)
         call(op, "gsb_sh2weight_fast_backward", n, ptr(A), ptr(B), _sh_dtype(A), ptr(ylm), ptr(dw),
              K, P, Q, rank, ptr(dA), ptr(dB), st)
@@ -335,7 +335,7 @@ def _splat_forward(op, H, W, C_, us, cinv2ds, alphas, depths, feats, areas, tau_
     gx, gy = _grid(H, W)
     dev = us.device
     L = _lib.lib()
-    with torch.cuda.device(dev):
+    with on_device(dev):
         st = stream_of(us)
         state = torch.empty(int(L.gsb_splat_state_bytes(n, C_, H, W)), dtype=torch.uint8,
                             device=dev)
@@ -426,7 +426,7 @@ def _splat_backward(op, H, W, C_, us, cinv2ds, alphas, feats, contrib, final_tau
     dalpha = torch.zeros((n, 1, 1), dtype=_F32, device=dev) if geom else None
     du = torch.zeros((n, 1, 2), dtype=_F32, device=dev) if geom else None
     dq = torch.zeros((n, 1, 3), dtype=_F32, device=dev) if geom else None
-    with torch.cuda.device(dev):
+    with on_device(dev):
         packed = _take_packed(gsid, H, W, C_, us, cinv, alphas, feats)
         if packed is not None:  # the forward's records, inputs unchanged since
             call(op, "gsb_splat_backward_packed", n, H, W, C_, ptr(ranges), ptr(gsid),
@@ -499,6 +499,6 @@ def lab2rgb(lab_image):
     lab = _cuda(op, "lab_image", lab_image)
     H, W = int(lab.shape[1]), int(lab.shape[2])
     rgb = torch.empty((3, H, W), dtype=_F32, device=lab.device)
-    with torch.cuda.device(lab.device):
+    with on_device(lab.device):
         call(op, "gsb_lab2rgb", H, W, ptr(lab), ptr(rgb), stream_of(lab))
     return rgb

@@ -4,6 +4,7 @@ The library is loaded from this directory.  There is no fallback: if it is
 missing or CUDA is unavailable, every operator raises instead of computing
 anything another way.
 """
+import contextlib
 import ctypes as C
 import os
 import threading
@@ -143,9 +144,15 @@ def exported_symbols():
     return sorted(_SIGS)
 
 
+_FN = {}
+
+
 def call(op, name, *args):
     """Invoke C entry `name`; raise with the library's message on failure."""
-    rc = getattr(lib(), name)(*args)
+    f = _FN.get(name)
+    if f is None:
+        f = _FN[name] = getattr(lib(), name)
+    rc = f(*args)
     if rc != GSB_OK:
         msg = (lib().gsb_last_error() or b"").decode(errors="replace")
         if rc == GSB_ERR_INVALID_ARGUMENT:
@@ -154,11 +161,29 @@ def call(op, name, *args):
 
 
 def ptr(t):
-    return None if t is None else C.c_void_p(t.data_ptr())
+    """Device address of `t` as an int (ctypes passes it as void*), or None."""
+    return None if t is None else t.data_ptr()
+
+
+# torch's raw current-stream query returns the cudaStream_t as an int without
+# building a Stream object (a few microseconds per operator call otherwise)
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
 
 
 def stream_of(t):
-    return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+    """The current CUDA stream of `t`'s device, as an int handle."""
+    if _RAW_STREAM is not None:
+        return _RAW_STREAM(t.device.index)
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+_CUR_DEV = getattr(torch._C, "_cuda_getDevice", None) or torch.cuda.current_device
+
+
+def on_device(dev):
+    """``torch.cuda.device(dev)`` when `dev` is not already the current device;
+    a no-op context otherwise (the switch costs a few microseconds per call)."""
+    return contextlib.nullcontext() if dev.index == _CUR_DEV() else torch.cuda.device(dev)
 
 
 def mapped_address(host):
@@ -198,14 +223,15 @@ def _timeout_word(dev):
 
 
 def fetch_device_status(dev, stream):
-    """Enqueue, on `stream` (a c_void_p), the copy of the device status bits
-    into this thread's host word for `dev`."""
+    """Enqueue, on `stream` (an int handle or a c_void_p), the copy of the
+    device status bits into this thread's host word for `dev`."""
     host, addr, dword = _timeout_word(dev)
     if addr is not None:
-        call("device_status_fetch", "gsb_device_status_fetch", C.c_void_p(addr), stream)
+        call("device_status_fetch", "gsb_device_status_fetch", addr, stream)
     else:
         call("device_status_fetch", "gsb_device_status_fetch", ptr(dword), stream)
-        with torch.cuda.stream(torch.cuda.ExternalStream(stream.value, device=dev)):
+        handle = stream.value if isinstance(stream, C.c_void_p) else stream
+        with torch.cuda.stream(torch.cuda.ExternalStream(handle or 0, device=dev)):
             host.copy_(dword, non_blocking=True)
 
 

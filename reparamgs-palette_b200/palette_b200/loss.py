@@ -42,7 +42,7 @@ class PaletteL1Loss(torch.autograd.Function):
         loss = torch.empty((), dtype=torch.float32, device=layer.device)
         dlayer = torch.empty_like(layer)
         dpal = torch.empty((K, 3), dtype=torch.float32, device=layer.device)
-        with torch.cuda.device(layer.device):
+        with _lib.on_device(layer.device):
             _lib.call("palette_l1_loss", "gsb_palette_l1", K, H, W, _lib.ptr(layer),
                       _lib.ptr(palette), _lib.ptr(target), None, _lib.ptr(loss), _lib.ptr(dlayer),
                       _lib.ptr(dpal), _lib.stream_of(layer))
@@ -67,7 +67,7 @@ def palette_image(layer, palette):
     image = torch.empty((3, H, W), dtype=torch.float32, device=layer.device)
     loss = torch.empty((), dtype=torch.float32, device=layer.device)
     zero = torch.zeros((3, H, W), dtype=torch.float32, device=layer.device)
-    with torch.cuda.device(layer.device):
+    with _lib.on_device(layer.device):
         _lib.call("palette_image", "gsb_palette_l1", K, H, W, _lib.ptr(layer), _lib.ptr(palette),
                   _lib.ptr(zero), _lib.ptr(image), _lib.ptr(loss), None, None,
                   _lib.stream_of(layer))
@@ -91,7 +91,7 @@ class PaletteGeoLoss(torch.autograd.Function):
         dlayer = torch.empty_like(layer)
         dchroma = torch.empty((Kc, 3), dtype=torch.float32, device=layer.device)
         code = {"mse": _lib.LOSS_MSE, "l1": _lib.LOSS_L1}[kind]
-        with torch.cuda.device(layer.device):
+        with _lib.on_device(layer.device):
             _lib.call("palette_geo_loss", "gsb_palette_geo_loss", Kc, H, W, _lib.ptr(layer),
                       _lib.ptr(target), _lib.ptr(chroma), int(bool(clamp)), code,
                       float(lambda_pos), None, _lib.ptr(loss), _lib.ptr(dlayer),
@@ -121,7 +121,7 @@ def barycentric_target(target, chroma, clamp=False):
     out = torch.empty((Kc + 2, H, W), dtype=torch.float32, device=target.device)
     zero = torch.zeros_like(out)
     loss = torch.empty((3,), dtype=torch.float32, device=target.device)
-    with torch.cuda.device(target.device):
+    with _lib.on_device(target.device):
         _lib.call("barycentric_target", "gsb_palette_geo_loss", Kc, H, W, _lib.ptr(zero),
                   _lib.ptr(target), _lib.ptr(chroma), int(bool(clamp)), _lib.LOSS_MSE, 0.0,
                   _lib.ptr(out), _lib.ptr(loss), None, None, _lib.stream_of(target))
@@ -135,7 +135,7 @@ def _l1_ssim(name, K, H, W, layer, palette, target, lambda_ssim, lambda_pos, dat
     dlayer = torch.empty_like(layer) if need_grad else None
     dpal = torch.empty((K, 3), dtype=torch.float32, device=dev) if (
         need_grad and palette is not None) else None
-    with torch.cuda.device(dev):
+    with _lib.on_device(dev):
         _lib.call(name, "gsb_palette_l1_ssim", K, H, W, _lib.ptr(layer),
                   None if palette is None else _lib.ptr(palette), _lib.ptr(target),
                   float(lambda_ssim), float(lambda_pos), float(data_range), None, _lib.ptr(loss),

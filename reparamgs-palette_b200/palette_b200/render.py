@@ -24,7 +24,6 @@ its backward sums the views' gradients in FP32 inside the kernels (the first
 view overwrites the FP32 gradient buffers, the others add to them) and casts
 once, so BF16 parameters are not accumulated in BF16.
 """
-import contextlib
 import ctypes as C
 import weakref
 
@@ -114,8 +113,7 @@ def _render_one(pws, rots, scales, alphas, w0, A, B, cam, mode, K, P, Q, rank):
     L = _lib.lib()
     camst, keep = camera_struct(cam)
     params = _params(mode, K, P, Q, rank, w0, A, B)
-    on_dev = dev.index == torch.cuda.current_device()
-    with contextlib.nullcontext() if on_dev else torch.cuda.device(dev):
+    with _lib.on_device(dev):
         st = _lib.stream_of(pws)
         state = torch.empty(_state_bytes(n, K, H, W), dtype=torch.uint8, device=dev)
         depths = torch.empty((n,), dtype=_F32, device=dev)
@@ -163,7 +161,7 @@ class _RenderPalette(torch.autograd.Function):
         geom = any(ctx.needs_input_grad[:4])
         e = (lambda *shape: torch.empty(shape, dtype=_F32, device=dev)) if geom else \
             (lambda *shape: None)
-        with torch.cuda.device(dev):
+        with _lib.on_device(dev):
             scratch = torch.empty(int(L.gsb_render_backward_bytes(n, K)), dtype=torch.uint8,
                                   device=dev)
             dpws, drots, dscales, dalphas = e(n, 3), e(n, 4), e(n, 3), e(n)
@@ -256,7 +254,7 @@ class _RenderPaletteViews(torch.autograd.Function):
             (lambda *shape: None)
         L = _lib.lib()
         params = _params(mode, K, P, Q, rank, w0, A, B)
-        with torch.cuda.device(dev):
+        with _lib.on_device(dev):
             st = _lib.stream_of(pws)
             scratch = torch.empty(int(L.gsb_render_backward_bytes(n, K)), dtype=torch.uint8,
                                   device=dev)

@@ -71,7 +71,7 @@ class _OperatorSplat(torch.autograd.Function):
         dw0 = torch.empty(tuple(w0.shape), dtype=_F32, device=dev)
         dA = torch.empty(tuple(A.shape), dtype=_F32, device=dev) if A is not None else None
         dB = torch.empty(tuple(B.shape), dtype=_F32, device=dev) if B is not None else None
-        with torch.cuda.device(dev):
+        with _lib.on_device(dev):
             st = _lib.stream_of(pws)
             _lib.call("splat_palette_weights.backward", "gsb_palette_weights_backward", n,
                       C.byref(camst), _lib.ptr(pws), C.byref(params), _lib.ptr(dW),

@@ -291,6 +291,39 @@ def test_bf16_full_weights_match_rounded_oracle(cuda_ok):
     np.testing.assert_allclose(np_of(w), o_w, rtol=1e-5, atol=2e-7)
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+@pytest.mark.parametrize("nb,K", [(1, 3), (1, 8), (4, 3), (4, 5), (9, 5), (9, 8), (16, 3), (16, 5),
+                                  (16, 8)])
+def test_sh_every_band_count_with_jacobians(cuda_ok, nb, K, dtype):
+    """The SH kernel is instantiated per band count (1, 4, 9, 16): weights
+    (or colours for K = 3) and both Jacobian outputs for each, FP32 rows and
+    BF16 rows (staged as raw element pairs when nb*K is even, read in place
+    when it is odd), against the oracle on the same stored values: weights
+    and basis within 1e-5 relative, direction derivatives within 1e-4
+    (norm-wise)."""
+    n = 3000
+    g = torch.Generator().manual_seed(200 + nb * 10 + K)
+    vals = (torch.randn((n, nb * K), generator=g) * 0.2).to(dtype)
+    shs = vals.cuda()
+    sc, st = _scene(n, seed=43)
+    cam = _cam(64, 64, (0.5, -7.0, 1.0))
+    twc = orc.camera_arrays(cam, np.float32)[2]
+    if K == 3:
+        f, dsh, dpw = gsc.sh2Color(shs, st["pws"], cam.twc, True)
+        f0, = gsc.sh2Color(shs, st["pws"], cam.twc, False)
+    else:
+        f, dsh, dpw = gsc.sh2Weight(shs, st["pws"], cam.twc, True, K)
+        f0, = gsc.sh2Weight(shs, st["pws"], cam.twc, False, K)
+    assert torch.equal(f, f0)  # the Jacobian outputs leave the weights unchanged
+    o_f, o_dsh, o_dpw = orc.sh2feat(vals.float().numpy(), sc["pws"], twc, K, True)
+    np.testing.assert_allclose(np_of(f), o_f, rtol=1e-5, atol=2e-7)
+    np.testing.assert_allclose(np_of(dsh), o_dsh, rtol=1e-5, atol=2e-7)
+    if nb > 1:
+        assert rel_err(dpw, o_dpw) < 1e-4
+    else:
+        assert float(dpw.abs().max()) == 0.0
+
+
 @pytest.mark.parametrize("nb,K,offset", [(9, 5, 0), (9, 3, 0), (16, 5, 1), (16, 3, 1), (4, 5, 1),
                                          (9, 5, 1)])
 def test_bf16_sh_rows_odd_length_or_misaligned(cuda_ok, nb, K, offset):
