@@ -593,42 +593,58 @@ __global__ void __launch_bounds__(kFuseThreads)
         float cov3[6], M3[9], Rq[9], cov2[3], M2[6], xy[2];
         covariance_3d(q, sc, cov3, M3, Rq);
         covariance_2d(cov3, p.x, p.y, p.z, cr.R, cam.fx, cam.fy, cam.tanx, cam.tany, cov2, M2, xy);
-        const float a = cov2[0], b = cov2[1], c = cov2[2];
-        const float det_inv = 1.f / (a * c - b * b);
-        if (!isnan(det_inv)) {
-          const float d2 = det_inv * det_inv;
-          const float Ji[9] = {-c * c * d2,           2 * b * c * d2,            -a * c * d2 + det_inv,
-                               b * c * d2,            -2 * b * b * d2 - det_inv, a * b * d2,
-                               -a * c * d2 + det_inv, 2 * a * b * d2,            -a * a * d2};
-          float dc2[3];
+        // the chain in FP64 (one per Gaussian: cheap), from the FP32 forward
+        // values; d conic / d cov2d with the b^2 / det^2 entries written as
+        // such rather than as 1/det - ac/det^2, which cancels
+        const double a = cov2[0], b = cov2[1], c = cov2[2];
+        const double det = a * c - b * b;
+        if (det != 0.0 && !isnan(det)) {
+          const double det_inv = 1.0 / det, d2 = det_inv * det_inv;
+          const double Ji[9] = {-c * c * d2, 2 * b * c * d2, -b * b * d2,
+                                b * c * d2,  -2 * b * b * d2 - det_inv, a * b * d2,
+                                -b * b * d2, 2 * a * b * d2, -a * a * d2};
+          double dc2[3];
 #pragma unroll
           for (int j = 0; j < 3; ++j) dc2[j] = gq[0] * Ji[j] + gq[1] * Ji[3 + j] + gq[2] * Ji[6 + j];
-          float d3[18], dpc_m[9];
-          cov2d_jacobians(cov3, M2, cr.R, xy[0], xy[1], p.z, cam.fx, cam.fy, d3, dpc_m);
-          float dS[6];
+          double c3d[6], M2d[6], Rd[9];
+#pragma unroll
+          for (int u = 0; u < 6; ++u) { c3d[u] = cov3[u]; M2d[u] = M2[u]; }
+#pragma unroll
+          for (int u = 0; u < 9; ++u) Rd[u] = cr.R[u];
+          double d3[18], dpc_m[9];
+          cov2d_jacobians<double>(c3d, M2d, Rd, xy[0], xy[1], p.z, cam.fx, cam.fy, d3, dpc_m);
+          double dS[6];
 #pragma unroll
           for (int u = 0; u < 6; ++u)
             dS[u] = dc2[0] * d3[u] + dc2[1] * d3[6 + u] + dc2[2] * d3[12 + u];
-          float dpc[3];
+          double dpc[3];
 #pragma unroll
           for (int j = 0; j < 3; ++j)
             dpc[j] = dc2[0] * dpc_m[j] + dc2[1] * dpc_m[3 + j] + dc2[2] * dpc_m[6 + j];
-          const float zi = 1.f / p.z, zi2 = zi * zi;
+          const double zi = 1.0 / p.z, zi2 = zi * zi;
           dpc[0] += gu[0] * (cam.fx * zi);
           dpc[1] += gu[1] * (cam.fy * zi);
-          dpc[2] += gu[0] * (-(p.x * cam.fx) * zi2) + gu[1] * (-(p.y * cam.fy) * zi2);
+          dpc[2] += gu[0] * (-(p.x * (double)cam.fx) * zi2) + gu[1] * (-(p.y * (double)cam.fy) * zi2);
 #pragma unroll
           for (int j = 0; j < 3; ++j)
-            dpw[j] += cr.R[j] * dpc[0] + cr.R[3 + j] * dpc[1] + cr.R[6 + j] * dpc[2];
-          float jq[24], js[18];
-          cov3d_jacobians(q, sc, M3, Rq, jq, js);
+            dpw[j] += (float)(Rd[j] * dpc[0] + Rd[3 + j] * dpc[1] + Rd[6 + j] * dpc[2]);
+          double M3d[9], Rqd[9];
+#pragma unroll
+          for (int u = 0; u < 9; ++u) { M3d[u] = M3[u]; Rqd[u] = Rq[u]; }
+          double jq[24], js[18];
+          cov3d_jacobians<double>(q, sc, M3d, Rqd, jq, js);
+          double dqd[4] = {0.0, 0.0, 0.0, 0.0}, dsd[3] = {0.0, 0.0, 0.0};
 #pragma unroll
           for (int u = 0; u < 6; ++u) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) dq[j] += dS[u] * jq[4 * u + j];
+            for (int j = 0; j < 4; ++j) dqd[j] += dS[u] * jq[4 * u + j];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) ds[j] += dS[u] * js[3 * u + j];
+            for (int j = 0; j < 3; ++j) dsd[j] += dS[u] * js[3 * u + j];
           }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dq[j] += (float)dqd[j];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) ds[j] += (float)dsd[j];
         }
       }
       sh_basis_grad(dir, L + 1, /*ref_quirk=*/false, G);

@@ -339,29 +339,32 @@ __device__ __forceinline__ void lowrank_weights(const S* dc, const S* a, const S
 }
 
 // ------------------------------------------------------------ Jacobians
+// Computed in the scalar type T: float for the operators' Jacobian outputs,
+// double in the adjoint's geometry chain (in FP32 that chain's rotation and
+// scale gradients lost up to 3e-4 relative to rounding).
 // d Sigma_(rc) / d q_j and / d s_j for Sigma = M M^T, M = R(q) diag(s).
-__device__ __forceinline__ void cov3d_jacobians(float4 q, float3 s, const float* M,
-                                                const float* R, float* dq /*6x4*/,
-                                                float* ds /*6x3*/) {
-  const float w = q.x, x = q.y, y = q.z, z = q.w;
+template <typename T>
+__device__ __forceinline__ void cov3d_jacobians(float4 q, float3 s, const T* M, const T* R,
+                                                T* dq /*6x4*/, T* ds /*6x3*/) {
+  const T w = q.x, x = q.y, y = q.z, z = q.w;
   // dR_ab / dq_j (rows a*3+b)
-  const float dR[9][4] = {{0.f, 0.f, -4.f * y, -4.f * z},
-                          {-2.f * z, 2.f * y, 2.f * x, -2.f * w},
-                          {2.f * y, 2.f * z, 2.f * w, 2.f * x},
-                          {2.f * z, 2.f * y, 2.f * x, 2.f * w},
-                          {0.f, -4.f * x, 0.f, -4.f * z},
-                          {-2.f * x, -2.f * w, 2.f * z, 2.f * y},
-                          {-2.f * y, 2.f * z, -2.f * w, 2.f * x},
-                          {2.f * x, 2.f * w, 2.f * z, 2.f * y},
-                          {0.f, -4.f * x, -4.f * y, 0.f}};
-  const float sv[3] = {s.x, s.y, s.z};
+  const T dR[9][4] = {{T(0), T(0), -T(4) * y, -T(4) * z},
+                      {-T(2) * z, T(2) * y, T(2) * x, -T(2) * w},
+                      {T(2) * y, T(2) * z, T(2) * w, T(2) * x},
+                      {T(2) * z, T(2) * y, T(2) * x, T(2) * w},
+                      {T(0), -T(4) * x, T(0), -T(4) * z},
+                      {-T(2) * x, -T(2) * w, T(2) * z, T(2) * y},
+                      {-T(2) * y, T(2) * z, -T(2) * w, T(2) * x},
+                      {T(2) * x, T(2) * w, T(2) * z, T(2) * y},
+                      {T(0), -T(4) * x, -T(4) * y, T(0)}};
+  const T sv[3] = {s.x, s.y, s.z};
   const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
 #pragma unroll
   for (int u = 0; u < 6; ++u) {
     const int r = sym[u][0], c = sym[u][1];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      float acc = 0.f;
+      T acc = T(0);
 #pragma unroll
       for (int b = 0; b < 3; ++b)
         acc += (M[3 * c + b] * dR[3 * r + b][j] + M[3 * r + b] * dR[3 * c + b][j]) * sv[b];
@@ -375,9 +378,10 @@ __device__ __forceinline__ void cov3d_jacobians(float4 q, float3 s, const float*
 // Jacobians of cov2d = (Sigma'_00 + .3, Sigma'_01, Sigma'_11 + .3) w.r.t. the 6
 // unique entries of Sigma and the camera-space centre (clamp not
 // differentiated, as in the reference).  M = J Rcw.
-__device__ __forceinline__ void cov2d_jacobians(const float* cov3, const float* M, const float* Rcw,
-                                                float x, float y, float z, float fx, float fy,
-                                                float* d3 /*3x6*/, float* dp /*3x3*/) {
+template <typename T>
+__device__ __forceinline__ void cov2d_jacobians(const T* cov3, const T* M, const T* Rcw, T x, T y,
+                                                T z, T fx, T fy, T* d3 /*3x6*/,
+                                                T* dp /*3x3*/) {
   const int sym[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
   const int out[3][2] = {{0, 0}, {0, 1}, {1, 1}};
 #pragma unroll
@@ -385,39 +389,39 @@ __device__ __forceinline__ void cov2d_jacobians(const float* cov3, const float* 
 #pragma unroll
     for (int u = 0; u < 6; ++u) {
       const int a = out[o][0], b = out[o][1], k = sym[u][0], l = sym[u][1];
-      float v = M[3 * a + k] * M[3 * b + l];
+      T v = M[3 * a + k] * M[3 * b + l];
       if (k != l) v += M[3 * a + l] * M[3 * b + k];
       d3[6 * o + u] = v;
     }
-  const float S[9] = {cov3[0], cov3[1], cov3[2], cov3[1], cov3[3], cov3[4], cov3[2], cov3[4], cov3[5]};
-  float dm[3][6];
+  const T S[9] = {cov3[0], cov3[1], cov3[2], cov3[1], cov3[3], cov3[4], cov3[2], cov3[4], cov3[5]};
+  T dm[3][6];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float sm0 = S[3 * c] * M[0] + S[3 * c + 1] * M[1] + S[3 * c + 2] * M[2];
-    const float sm1 = S[3 * c] * M[3] + S[3 * c + 1] * M[4] + S[3 * c + 2] * M[5];
-    dm[0][c] = 2.f * sm0;
-    dm[0][3 + c] = 0.f;
+    const T sm0 = S[3 * c] * M[0] + S[3 * c + 1] * M[1] + S[3 * c + 2] * M[2];
+    const T sm1 = S[3 * c] * M[3] + S[3 * c + 1] * M[4] + S[3 * c + 2] * M[5];
+    dm[0][c] = T(2) * sm0;
+    dm[0][3 + c] = T(0);
     dm[1][c] = sm1;
     dm[1][3 + c] = sm0;
-    dm[2][c] = 0.f;
-    dm[2][3 + c] = 2.f * sm1;
+    dm[2][c] = T(0);
+    dm[2][3 + c] = T(2) * sm1;
   }
-  const float zi2 = 1.f / (z * z), zi3 = zi2 / z;
-  float dmp[6][3];
+  const T zi2 = T(1) / (z * z), zi3 = zi2 / z;
+  T dmp[6][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     dmp[c][0] = -fx * Rcw[6 + c] * zi2;
-    dmp[c][1] = 0.f;
-    dmp[c][2] = -fx * Rcw[c] * zi2 + 2.f * fx * Rcw[6 + c] * x * zi3;
-    dmp[3 + c][0] = 0.f;
+    dmp[c][1] = T(0);
+    dmp[c][2] = -fx * Rcw[c] * zi2 + T(2) * fx * Rcw[6 + c] * x * zi3;
+    dmp[3 + c][0] = T(0);
     dmp[3 + c][1] = -fy * Rcw[6 + c] * zi2;
-    dmp[3 + c][2] = -fy * Rcw[3 + c] * zi2 + 2.f * fy * Rcw[6 + c] * y * zi3;
+    dmp[3 + c][2] = -fy * Rcw[3 + c] * zi2 + T(2) * fy * Rcw[6 + c] * y * zi3;
   }
 #pragma unroll
   for (int o = 0; o < 3; ++o)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      float acc = 0.f;
+      T acc = T(0);
 #pragma unroll
       for (int m = 0; m < 6; ++m) acc += dm[o][m] * dmp[m][j];
       dp[3 * o + j] = acc;
