@@ -32,10 +32,6 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // Global -> shared bulk copy; `bytes` a multiple of 16, both addresses 16-byte
 // aligned.  Completion is signalled on `bar` as transaction bytes.
 __device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes,
