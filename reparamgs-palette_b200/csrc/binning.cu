@@ -366,10 +366,17 @@ __global__ void __launch_bounds__(kSortThreads)
   for (int k = threadIdx.x; k < 8 * kRadixBins; k += kSortThreads) (&h[0][0])[k] = 0u;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortTile;
-#pragma unroll 4
+  // all of the thread's keys in flight before the histogram updates
+  KT k[kSortItems];
+#pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
     const int64_t idx = base + r * kSortThreads + threadIdx.x;
-    if (idx < M) atomicAdd(&h[w][(uint32_t)(keys[idx] >> shift) & mask], 1u);
+    k[r] = idx < M ? keys[idx] : (KT)0;
+  }
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int64_t idx = base + r * kSortThreads + threadIdx.x;
+    if (idx < M) atomicAdd(&h[w][(uint32_t)(k[r] >> shift) & mask], 1u);
   }
   __syncthreads();
   for (uint32_t d = threadIdx.x; d <= mask; d += kSortThreads) {
@@ -387,12 +394,22 @@ __global__ void __launch_bounds__(256)
   __shared__ uint32_t warp_tot[8];
   uint32_t* row = hist + (int64_t)blockIdx.x * nblocks;
   uint32_t carry = 0;
-  for (int64_t base = 0; base < nblocks; base += 256) {
-    const int64_t j = base + threadIdx.x;
-    const uint32_t v = (j < nblocks) ? row[j] : 0u;
+  constexpr int kItems = 8;  // consecutive counts per thread: one block scan per 2048
+  for (int64_t base = 0; base < nblocks; base += 256 * kItems) {
+    const int64_t j0 = base + (int64_t)threadIdx.x * kItems;
+    uint32_t v[kItems], s = 0;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+      v[i] = j0 + i < nblocks ? row[j0 + i] : 0u;
+      s += v[i];
+    }
     uint32_t tot;
-    const uint32_t ex = block_excl_scan256(v, warp_tot, &tot);
-    if (j < nblocks) row[j] = carry + ex;
+    uint32_t run = carry + block_excl_scan256(s, warp_tot, &tot);
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+      if (j0 + i < nblocks) row[j0 + i] = run;
+      run += v[i];
+    }
     carry += tot;
   }
   if (threadIdx.x == 0) digit_tot[blockIdx.x] = carry;
@@ -491,23 +508,34 @@ __global__ void __launch_bounds__(kSortThreads)
 // getRanges (gsplatcu/kernel.cu:165-187) on the sorted keys, with the same
 // writes -- including that the end of the only tile is left unset when
 // M == 1.  `ranges` is cleared beforehand.
+constexpr int kRangeItems = 8;  // keys per thread in k_ranges
+
 template <typename KT>
 __global__ void k_ranges(const KT* __restrict__ keys, int64_t M, int dkey_bits,
                          int2* __restrict__ ranges, const uint32_t* __restrict__ mdev) {
   pdl_wait();
   if (capacity_overflow(M, mdev, dkey_bits)) return;
   M = device_patches(M, mdev);
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= M) return;
-  const uint32_t cur = key_tile(keys[p], dkey_bits);
-  const uint32_t prv = key_tile(keys[p == 0 ? 0 : p - 1], dkey_bits);
-  if (p == 0)
-    ranges[cur].x = 0;
-  else if (p == M - 1)
-    ranges[cur].y = (int)M;
-  if (prv != cur) {
-    ranges[prv].y = (int)p;
-    ranges[cur].x = (int)p;
+  const int64_t b0 = (int64_t)blockIdx.x * (256 * kRangeItems) + threadIdx.x;
+  uint32_t cur[kRangeItems], prv[kRangeItems];
+#pragma unroll
+  for (int r = 0; r < kRangeItems; ++r) {
+    const int64_t p = b0 + r * 256;
+    cur[r] = p < M ? key_tile(keys[p], dkey_bits) : 0u;
+    prv[r] = p < M ? key_tile(keys[p == 0 ? 0 : p - 1], dkey_bits) : 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < kRangeItems; ++r) {
+    const int64_t p = b0 + r * 256;
+    if (p >= M) continue;
+    if (p == 0)
+      ranges[cur[r]].x = 0;
+    else if (p == M - 1)
+      ranges[cur[r]].y = (int)M;
+    if (prv[r] != cur[r]) {
+      ranges[prv[r]].y = (int)p;
+      ranges[cur[r]].x = (int)p;
+    }
   }
 }
 
@@ -646,7 +674,8 @@ static int sort_t(const SortPlan& p, int64_t n, int W, const SplatState& s, void
     vs = vd;
     vd = vt;
   }
-  launch_pdl(k_ranges<KT>, dim3((unsigned)div_up(p.M, 256)), dim3(256), 0, st, (const KT*)ks, p.M,
+  launch_pdl(k_ranges<KT>, dim3((unsigned)div_up(p.M, 256 * kRangeItems)), dim3(256), 0, st,
+             (const KT*)ks, p.M,
              p.dkey_bits, (int2*)ranges_out, mdev);
   return check_launch("splat_sort (ranges)");
 }
