@@ -750,8 +750,11 @@ def run_b200(a):
     ms_per_step = ms / a.steps
     value = world * a.steps / (ms / 1000.0)
 
-    # forward only
+    # forward only (its own warm-up: the first forward-only steps after the
+    # training steps reallocate)
     with torch.no_grad():
+        for _ in range(max(3, a.warmup)):
+            step(wl, backward=False)
         fms = timed(lambda: step(wl, backward=False), a.steps, stream) / a.steps
     fms = allreduce_max(fms, world, device)
 
