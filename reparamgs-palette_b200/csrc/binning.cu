@@ -33,22 +33,21 @@ static void state_layout(int64_t n, int channels, int H, int W, size_t* offs) {
   offs[2] = b; b += align256((size_t)n * 4);                          // counts
   offs[3] = b; b += align256((size_t)(nb > 0 ? nb : 1) * 4);          // block sums
   offs[4] = b; b += align256(16 * 4);                                 // stats
-  offs[5] = b; b += align256((size_t)n * record_vec4(channels) * 16); // records
+  offs[5] = b; b += align256((size_t)(gx * gy > 0 ? gx * gy : 1) * 4); // tile launch order
+  offs[6] = b; b += align256((size_t)n * record_vec4(channels) * 16); // records
   const int64_t np = (n + kPartBlock - 1) / kPartBlock;
-  offs[6] = b; b += 2 * align256((size_t)(np > 0 ? np : 1) * 4);      // part sums, part max
-  offs[7] = b;
-  (void)gx;
-  (void)gy;
+  offs[7] = b; b += 2 * align256((size_t)(np > 0 ? np : 1) * 4);      // part sums, part max
+  offs[8] = b;
 }
 
 size_t splat_state_bytes(int64_t n, int channels, int H, int W) {
-  size_t offs[8];
+  size_t offs[9];
   state_layout(n, channels, H, W, offs);
-  return offs[7];
+  return offs[8];
 }
 
 SplatState carve_state(void* base, int64_t n, int channels, int H, int W) {
-  size_t o[8];
+  size_t o[9];
   state_layout(n, channels, H, W, o);
   char* p = (char*)base;
   SplatState s;
@@ -61,9 +60,10 @@ SplatState carve_state(void* base, int64_t n, int channels, int H, int W) {
   s.counts = (uint32_t*)(p + o[2]);
   s.block_sums = (uint32_t*)(p + o[3]);
   s.stats = (uint32_t*)(p + o[4]);
-  s.records = (float4*)(p + o[5]);
+  s.tile_order = (int32_t*)(p + o[5]);
+  s.records = (float4*)(p + o[6]);
   s.n_parts = (n + kPartBlock - 1) / kPartBlock;
-  s.part_sums = (uint32_t*)(p + o[6]);
+  s.part_sums = (uint32_t*)(p + o[7]);
   s.part_max = s.part_sums + align256((size_t)(s.n_parts > 0 ? s.n_parts : 1) * 4) / 4;
   return s;
 }

@@ -65,6 +65,7 @@ struct SplatState {
   uint32_t* counts;      // [n] patches per Gaussian
   uint32_t* block_sums;  // [n_blocks] -> exclusive block offsets after the scan
   uint32_t* stats;       // [16]: 0/3 = M low/high, 1 = max depth key
+  int32_t* tile_order;   // [gx * gy] launch order of the compositing tiles
   uint32_t* part_sums;   // [n_parts] patches per kPartBlock Gaussians (fused preprocess)
   uint32_t* part_max;    // [n_parts] their largest depth key
   int rec_vec4;          // float4 vectors per record

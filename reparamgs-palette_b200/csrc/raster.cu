@@ -132,6 +132,64 @@ __device__ __forceinline__ void load_feats(const float4* srec, int j, float v2w,
   }
 }
 
+// ------------------------------------------------------ tile launch order
+// Blocks are launched in blockIdx order, a wave at a time.  Compositing a
+// tile costs roughly its list length, which varies by orders of magnitude
+// across an image, so launching tiles in raster order leaves the last waves
+// waiting on a few long tiles.  The compositing kernels instead take their
+// tile from a launch order, longest list first (a largest-first schedule):
+// lengths binned at a quarter octave, descending; order within a bin is
+// arbitrary.  Measured at 1M Gaussians, 1080p: forward 0.309 -> 0.280 ms,
+// adjoint 0.436 -> 0.372 ms (0.220 -> 0.164 and 0.317 -> 0.273 ms for a
+// distant view).  The results do not depend on the order.
+constexpr int kOrderThreads = 1024, kOrderBins = 128;
+
+__device__ __forceinline__ int order_bin(int2 rg) {
+  const uint32_t x = (uint32_t)max(0, rg.y - rg.x) + 1u;   // >= 1
+  const int msb = 31 - __clz(x);
+  const int frac = msb >= 2 ? (int)((x >> (msb - 2)) & 3u) : (int)((x << (2 - msb)) & 3u);
+  return kOrderBins - 1 - min(kOrderBins - 1, 4 * msb + frac);  // longest first
+}
+
+__global__ void __launch_bounds__(kOrderThreads)
+    k_tile_order(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order) {
+  pdl_wait();
+  __shared__ int cnt[kOrderBins];
+  if (threadIdx.x < kOrderBins) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < tiles; t += kOrderThreads) atomicAdd(&cnt[order_bin(ranges[t])], 1);
+  __syncthreads();
+  if (threadIdx.x < 32) {  // exclusive scan of the bins, 4 per lane
+    const int lane = threadIdx.x;
+    int v[kOrderBins / 32], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kOrderBins / 32; ++k) {
+      v[k] = cnt[lane * (kOrderBins / 32) + k];
+      sum += v[k];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    int run = incl - sum;
+#pragma unroll
+    for (int k = 0; k < kOrderBins / 32; ++k) {
+      cnt[lane * (kOrderBins / 32) + k] = run;
+      run += v[k];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < tiles; t += kOrderThreads)
+    order[atomicAdd(&cnt[order_bin(ranges[t])], 1)] = t;
+}
+
+static int launch_tile_order(const int2* ranges, int tiles, int32_t* order, cudaStream_t st) {
+  launch_pdl(k_tile_order, dim3(1), dim3(kOrderThreads), 0, st, ranges, tiles, order);
+  return check_launch("tile order");
+}
+
 // ------------------------------------------------------------- forward
 // Composites one 16x16 tile of one image (draw_weight / draw_color,
 // gsplatcu/kernel.cu:283-372): ranges/gsid/records of that image's tile
@@ -241,12 +299,13 @@ __device__ __forceinline__ void draw_tile(int tile, int H, int W, int gx,
 template <int K>
 __global__ void __launch_bounds__(kDrawFwdThreads, 4)
     k_draw(int H, int W, int gx, const int2* __restrict__ ranges, const int32_t* __restrict__ gsid,
-           const float4* __restrict__ records, float tau_init, float* __restrict__ out,
-           int32_t* __restrict__ contrib, float* __restrict__ final_tau) {
+           const float4* __restrict__ records, const int32_t* __restrict__ order,
+           float tau_init, float* __restrict__ out, int32_t* __restrict__ contrib,
+           float* __restrict__ final_tau) {
   pdl_wait();
   __shared__ float4 srec[RecordLayout<K>::kVec4 * kBatch];
-  draw_tile<K>(blockIdx.x, H, W, gx, ranges, gsid, records, tau_init, out, contrib, final_tau,
-               srec);
+  draw_tile<K>(order[blockIdx.x], H, W, gx, ranges, gsid, records, tau_init, out, contrib,
+               final_tau, srec);
 }
 
 // ------------------------------------------------- batched (persistent) draw
@@ -617,6 +676,7 @@ template <int K, bool GEOM, bool DTAU>
 __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
     k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
                     const int32_t* __restrict__ gsid, const float4* __restrict__ records,
+                    const int32_t* __restrict__ order,
                     const int32_t* __restrict__ contrib, const float* __restrict__ final_tau,
                     const float* __restrict__ dout, const float* __restrict__ dtau,
                     float* __restrict__ dfeat, float* __restrict__ dalpha,
@@ -628,9 +688,10 @@ __global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 7)
   __shared__ float4 srec[V * kBatch];
   __shared__ int32_t sgid[kBatch];
   __shared__ unsigned s_maxc;
-  const PixelPair pp = pixels_of(blockIdx.x, gx);
+  const int tile = order[blockIdx.x];
+  const PixelPair pp = pixels_of(tile, gx);
   const int lane = threadIdx.x & 31;
-  const int2 rg = ranges[blockIdx.x];
+  const int2 rg = ranges[tile];
   if (rg.y - rg.x == 0) return;  // uniform per block
   const int64_t hw = (int64_t)H * W;
   BwdPixel<K> p[2];
@@ -746,11 +807,15 @@ int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, co
   const int tiles = gx * gy;
   if (tiles == 0) return GSB_OK;
   const int2* rg = (const int2*)ranges;
+  if (channels < 1 || channels > 8) return GSB_ERR_INVALID_ARGUMENT;
+  const int rc = launch_tile_order(rg, tiles, s.tile_order, st);
+  if (rc) return rc;
   switch (channels) {
 #define GSB_K(KK)                                                                           \
   case KK:                                                                                  \
     launch_pdl(k_draw<KK>, dim3(tiles), dim3(kDrawFwdThreads), 0, st, H, W, gx, rg, gsid,       \
-               (const float4*)s.records, tau_init, out, contrib, final_tau);                   \
+               (const float4*)s.records, (const int32_t*)s.tile_order, tau_init, out, contrib,   \
+               final_tau);                                                                      \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K
@@ -761,15 +826,15 @@ int launch_draw(int64_t n, int H, int W, int channels, const int32_t* ranges, co
 
 template <int K>
 static void draw_bwd_k(int tiles, int H, int W, int gx, const int2* rg, const int32_t* gsid,
-                       const float4* rec, const int32_t* contrib, const float* ft, const float* dout,
-                       const float* dtau, float* dfeat, float* dalpha, float* du, float* dq,
-                       cudaStream_t st) {
+                       const float4* rec, const int32_t* order, const int32_t* contrib,
+                       const float* ft, const float* dout, const float* dtau, float* dfeat,
+                       float* dalpha, float* du, float* dq, cudaStream_t st) {
   const bool geom = dalpha != nullptr;
   auto kern = (geom && dtau) ? k_draw_backward<K, true, true>
               : geom         ? k_draw_backward<K, true, false>
                              : k_draw_backward<K, false, false>;
-  launch_pdl(kern, dim3(tiles), dim3(kDrawThreads), 0, st, H, W, gx, rg, gsid, rec, contrib, ft,
-             dout, dtau, dfeat, dalpha, du, dq);
+  launch_pdl(kern, dim3(tiles), dim3(kDrawThreads), 0, st, H, W, gx, rg, gsid, rec, order, contrib,
+             ft, dout, dtau, dfeat, dalpha, du, dq);
 }
 
 int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* ranges,
@@ -781,11 +846,14 @@ int launch_draw_backward(int64_t n, int H, int W, int channels, const int32_t* r
   const int tiles = gx * gy;
   if (tiles == 0) return GSB_OK;
   const int2* rg = (const int2*)ranges;
+  if (channels < 1 || channels > 8) return GSB_ERR_INVALID_ARGUMENT;
+  const int rc = launch_tile_order(rg, tiles, s.tile_order, st);
+  if (rc) return rc;
   switch (channels) {
 #define GSB_K(KK)                                                                              \
   case KK:                                                                                     \
-    draw_bwd_k<KK>(tiles, H, W, gx, rg, gsid, s.records, contrib, final_tau, dout, dtau, dfeat, \
-                   dalpha, du, dconic, st);                                                    \
+    draw_bwd_k<KK>(tiles, H, W, gx, rg, gsid, s.records, s.tile_order, contrib, final_tau,      \
+                   dout, dtau, dfeat, dalpha, du, dconic, st);                                 \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K

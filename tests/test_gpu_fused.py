@@ -59,9 +59,11 @@ def _render(st, cam, mode, requires_grad=False, grad_names=None):
 def _state_sections(n, K, H, W):
     al = lambda x: (x + 255) & ~255
     nb = (n + 255) // 256
+    tiles = ((W + 15) // 16) * ((H + 15) // 16)
     o = [0]
-    for size in (n * 8, n * 4, n * 4, nb * 4, 64):
+    for size in (n * 8, n * 4, n * 4, nb * 4, 64, tiles * 4):
         o.append(o[-1] + al(size))
+    del o[5]  # (the tile launch order, written by the compositing launches)
     return o  # rects, dkeys, counts, block sums, stats, records
 
 
