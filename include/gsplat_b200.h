@@ -155,6 +155,10 @@ int gsb_lab2rgb(int height, int width, const float* lab, float* rgb, void* strea
  *                             `sort_ws` of gsb_splat_sort_bytes(plan) bytes.
  *   4. gsb_splat_draw      -- front-to-back compositing (draw_weight /
  *                             draw_color, gsplatcu/kernel.cu:194-372).
+ *                             It (and the adjoint) first writes a launch
+ *                             order of the tiles, longest list first, into
+ *                             `state`; so a state buffer serves one draw or
+ *                             adjoint at a time.
  *
  * Tile lists and ranges are bit-identical to the reference's given identical
  * us/areas/depths: keys (tile << b | uint32(depth*1000)) are emitted in
