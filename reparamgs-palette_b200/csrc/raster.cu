@@ -599,7 +599,11 @@ __device__ __forceinline__ float* grad_slot(int v, int64_t g, float* dfeat, floa
 // each pixel).  The two gradient vectors (K + 6 values each) are summed
 // together: one exchange at lane offset 16 leaves ja's partial sums on lanes
 // 0-15 and jb's on lanes 16-31, then each half-warp transposes its values
-// (K + 6 + 15 shuffles for the pair instead of 2 x 16 for K = 3..8).
+// (K + 6 + 15 shuffles for the pair instead of 2 x 16 for K = 3..8).  When
+// at most kDirectLanesGeom lanes hit each record, those lanes add their own
+// K + 6 sums directly: at 1M / 1080p 0.776 -> 0.755 ms near, 0.462 -> 0.439
+// ms far, against direct atomics for single hits only.
+constexpr int kDirectLanesGeom = 8;
 template <int K, bool DTAU>
 __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base, int ja, int jb,
                                                   const float4* srec, const int32_t* sgid,
@@ -628,7 +632,7 @@ __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base,
   hb |= adjoint_pixel<K, true, DTAU>(p[1], base + jb, mb1, b0, b1, dxb, dyb1, srec, jb, xb);
   const unsigned ca = __ballot_sync(0xffffffffu, ha), cb = __ballot_sync(0xffffffffu, hb);
   if (!(ca | cb)) return;
-  if (__popc(ca) <= 1 && __popc(cb) <= 1) {
+  if (__popc(ca) <= kDirectLanesGeom && __popc(cb) <= kDirectLanesGeom) {
     if (ha) {
       const int64_t g = sgid[ja];
 #pragma unroll
