@@ -177,8 +177,7 @@ constexpr int kShThreads = 64;  // 64 rows of at most 129 floats: 33 KB of share
 
 template <int K, int NB>
 struct ShOut {
-  static constexpr int SK = K | 1, SNB = NB | 1, S3K = (3 * K) | 1;
-  static constexpr int kFloats = kShThreads * (SK + SNB + S3K);  // with the Jacobians
+  static constexpr int SK = K | 1, SNB = NB | 1, S3K = (3 * K) | 1;  // odd row strides
 };
 
 // Copies `rows` rows of `w` floats from shared memory (row stride `ws`) to
