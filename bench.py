@@ -843,7 +843,9 @@ def run_b200(a):
                 peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s")
 
-    serving = serve_bench(a, device) if a.serve_seconds > 0 else None
+    # the serving loop is per GPU (replicas): measured on one GPU, not repeated
+    # on every rank of a scaling run
+    serving = serve_bench(a, device) if a.serve_seconds > 0 and world == 1 else None
 
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
