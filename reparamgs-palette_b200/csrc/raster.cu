@@ -678,9 +678,10 @@ __device__ __forceinline__ void adjoint_geom_pair(BwdPixel<K> (&p)[2], int base,
 // (vanilla_3dgs/gsplatcu/kernel.cu:912-919).  As in the reference, the 0.99
 // clamp and max(0, .) are not differentiated.  Weights-only, 8 blocks per SM
 // (64 registers, a 12-byte spill): 0.377 -> 0.365 ms at 1M / 1080p against 7
-// blocks (72 registers).
+// blocks (72 registers); the full adjoint 6 blocks per SM (80 registers):
+// 0.755 -> 0.722 ms near, 1.146 -> 1.112 ms close, 0.437 -> 0.450 ms far.
 template <int K, bool GEOM, bool DTAU>
-__global__ void __launch_bounds__(kDrawThreads, GEOM ? 5 : 8)
+__global__ void __launch_bounds__(kDrawThreads, GEOM ? 6 : 8)
     k_draw_backward(int H, int W, int gx, const int2* __restrict__ ranges,
                     const int32_t* __restrict__ gsid, const float4* __restrict__ records,
                     const int32_t* __restrict__ order,
