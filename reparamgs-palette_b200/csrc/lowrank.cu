@@ -30,7 +30,9 @@ static __device__ uint32_t g_lowrank_status;
 
 // Shared-memory layout of the fixed-shape kernels: one region per array, the
 // rows of the block's Gaussians back to back (row stride = row length), so a
-// full block's span of every array moves as one 1-D bulk copy.
+// full block's span of every array moves as one 1-D bulk copy.  BF16 factors
+// stay raw (their spans are multiples of 256 bytes), packed at the start of
+// the factor regions they replace, and are widened when read.
 template <int K, int P, int Q, int R>
 struct LrSmem {
   static constexpr int L = P * Q / K;
@@ -40,6 +42,31 @@ struct LrSmem {
   // backward: A, B, ylm, dw in; dA, dB out
   static constexpr int bwd_floats = P * R + R * Q + LL + K + P * R + R * Q;
 };
+
+// The block's rows of a BF16 array, copied raw (no bulk copy: the last block
+// or an unaligned base); 8 loads in flight per thread.
+template <int ROWLEN>
+__device__ __forceinline__ void stage_raw_plain(const __nv_bfloat16* __restrict__ g, int64_t row0,
+                                                int64_t nrows_total, __nv_bfloat16* s) {
+  constexpr int U = 8;
+  const int64_t rows = min((int64_t)blockDim.x, nrows_total - row0);
+  const int total = rows > 0 ? (int)rows * ROWLEN : 0;
+  const __nv_bfloat16* base = g + row0 * ROWLEN;
+  const int nt = blockDim.x;
+  for (int j0 = threadIdx.x; j0 < total; j0 += nt * U) {
+    __nv_bfloat16 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = j0 + u * nt;
+      v[u] = j < total ? base[j] : __nv_bfloat16();
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = j0 + u * nt;
+      if (j < total) s[j] = v[u];
+    }
+  }
+}
 
 template <int K, int P, int Q, int R, typename T>
 __global__ void __launch_bounds__(kLrThreads)
@@ -58,18 +85,35 @@ __global__ void __launch_bounds__(kLrThreads)
   float* s_p = s_b + nt * RQ;
   float* s_w = s_p + nt * 3;
   float* s_y = s_w + nt * K;
+  constexpr bool kBf = sizeof(T) == 2;
+  T* r_dc = reinterpret_cast<T*>(sm);  // BF16: raw rows inside the dc, A, B regions
+  T* r_a = r_dc + nt * K;
+  T* r_b = r_a + nt * PR;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
   const bool full = row0 + nt <= n;
-  const bool bulk = full && sizeof(T) == 4 && aligned16(dc + row0 * K) &&
-                    aligned16(A + row0 * PR) && aligned16(B + row0 * RQ) &&
-                    aligned16(pws + row0 * 3);
+  const bool bulk = full && aligned16(dc + row0 * K) && aligned16(A + row0 * PR) &&
+                    aligned16(B + row0 * RQ) && aligned16(pws + row0 * 3);
   if (bulk && threadIdx.x == 0) {
     mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, (uint32_t)(nt * (K + PR + RQ + 3) * 4));
+    mbar_arrive_expect_tx(&bar, (uint32_t)(nt * ((K + PR + RQ) * sizeof(T) + 3 * 4)));
   }
-  stage_rows<K>(dc, row0, n, s_dc, bulk, &bar);
-  stage_rows<PR>(A, row0, n, s_a, bulk, &bar);
-  stage_rows<RQ>(B, row0, n, s_b, bulk, &bar);
+  if constexpr (kBf) {
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        bulk_load(r_dc, dc + row0 * K, (uint32_t)(nt * K * 2), &bar);
+        bulk_load(r_a, A + row0 * PR, (uint32_t)(nt * PR * 2), &bar);
+        bulk_load(r_b, B + row0 * RQ, (uint32_t)(nt * RQ * 2), &bar);
+      }
+    } else {
+      stage_raw_plain<K>(dc, row0, n, r_dc);
+      stage_raw_plain<PR>(A, row0, n, r_a);
+      stage_raw_plain<RQ>(B, row0, n, r_b);
+    }
+  } else {
+    stage_rows<K>(dc, row0, n, s_dc, bulk, &bar);
+    stage_rows<PR>(A, row0, n, s_a, bulk, &bar);
+    stage_rows<RQ>(B, row0, n, s_b, bulk, &bar);
+  }
   stage_rows<3>(pws, row0, n, s_p, bulk, &bar);
   __syncthreads();
   if (bulk && !mbar_wait(&bar, 0)) {
@@ -90,7 +134,10 @@ __global__ void __launch_bounds__(kLrThreads)
 #pragma unroll
       for (int l = 0; l < L; ++l) s_y[t * S::LL + l] = Y[l + 1];
     }
-    lowrank_weights<K, P, Q, R>(s_dc + t * K, s_a + t * PR, s_b + t * RQ, Y, wk);
+    if constexpr (kBf)
+      lowrank_weights<K, P, Q, R>(r_dc + t * K, r_a + t * PR, r_b + t * RQ, Y, wk);
+    else
+      lowrank_weights<K, P, Q, R>(s_dc + t * K, s_a + t * PR, s_b + t * RQ, Y, wk);
 #pragma unroll
     for (int k = 0; k < K; ++k) s_w[t * K + k] = wk[k];
   }
@@ -176,17 +223,31 @@ __global__ void __launch_bounds__(kLrThreads)
   float* s_g = s_y + nt * LL;
   float* s_da = s_g + nt * K;
   float* s_db = s_da + nt * PR;
+  constexpr bool kBf = sizeof(T) == 2;
+  T* r_a = reinterpret_cast<T*>(sm);  // BF16: raw rows inside the A, B regions
+  T* r_b = r_a + nt * PR;
   const int64_t row0 = (int64_t)blockIdx.x * nt;
   const bool full = row0 + nt <= n;
-  const bool bulk = full && sizeof(T) == 4 && L > 0 && aligned16(A + row0 * PR) &&
-                    aligned16(B + row0 * RQ) && aligned16(ylm + row0 * L) &&
-                    aligned16(dw + row0 * K);
+  const bool bulk = full && L > 0 && aligned16(A + row0 * PR) && aligned16(B + row0 * RQ) &&
+                    aligned16(ylm + row0 * L) && aligned16(dw + row0 * K);
   if (bulk && threadIdx.x == 0) {
     mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, (uint32_t)(nt * (PR + RQ + L + K) * 4));
+    mbar_arrive_expect_tx(&bar, (uint32_t)(nt * ((PR + RQ) * sizeof(T) + (L + K) * 4)));
   }
-  stage_rows<PR>(A, row0, n, s_a, bulk, &bar);
-  stage_rows<RQ>(B, row0, n, s_b, bulk, &bar);
+  if constexpr (kBf) {
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        bulk_load(r_a, A + row0 * PR, (uint32_t)(nt * PR * 2), &bar);
+        bulk_load(r_b, B + row0 * RQ, (uint32_t)(nt * RQ * 2), &bar);
+      }
+    } else {
+      stage_raw_plain<PR>(A, row0, n, r_a);
+      stage_raw_plain<RQ>(B, row0, n, r_b);
+    }
+  } else {
+    stage_rows<PR>(A, row0, n, s_a, bulk, &bar);
+    stage_rows<RQ>(B, row0, n, s_b, bulk, &bar);
+  }
   if (L > 0) stage_rows<LL>(ylm, row0, n, s_y, bulk, &bar);
   stage_rows<K>(dw, row0, n, s_g, bulk, &bar);
   __syncthreads();
@@ -196,6 +257,15 @@ __global__ void __launch_bounds__(kLrThreads)
     return;
   }
   const int t = threadIdx.x;
+  // this thread's factor rows, FP32 or raw BF16 widened on read
+  const auto fa = [&](int j) -> float {
+    if constexpr (kBf) return __bfloat162float(r_a[t * PR + j]);
+    else return s_a[t * PR + j];
+  };
+  const auto fb = [&](int j) -> float {
+    if constexpr (kBf) return __bfloat162float(r_b[t * RQ + j]);
+    else return s_b[t * RQ + j];
+  };
   if (row0 + t < n) {
     float y[LL], g0[K];
 #pragma unroll
@@ -206,12 +276,12 @@ __global__ void __launch_bounds__(kLrThreads)
       float a[P], b[Q], da[P], db[Q];
 #pragma unroll
       for (int j = 0; j < P; ++j) {
-        a[j] = s_a[t * P + j];
+        a[j] = fa(j);
         da[j] = 0.f;
       }
 #pragma unroll
       for (int j = 0; j < Q; ++j) {
-        b[j] = s_b[t * Q + j];
+        b[j] = fb(j);
         db[j] = 0.f;
       }
 #pragma unroll
@@ -237,7 +307,7 @@ __global__ void __launch_bounds__(kLrThreads)
           const int g = p * Q + q;
           const float c = g0[g % K] * y[g / K];
 #pragma unroll
-          for (int r = 0; r < R; ++r) acc[r] += c * s_b[t * RQ + r * Q + q];
+          for (int r = 0; r < R; ++r) acc[r] += c * fb(r * Q + q);
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) s_da[t * PR + p * R + r] = acc[r];
@@ -252,7 +322,7 @@ __global__ void __launch_bounds__(kLrThreads)
           const int g = p * Q + q;
           const float c = g0[g % K] * y[g / K];
 #pragma unroll
-          for (int r = 0; r < R; ++r) acc[r] += c * s_a[t * PR + p * R + r];
+          for (int r = 0; r < R; ++r) acc[r] += c * fa(p * R + r);
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) s_db[t * RQ + r * Q + q] = acc[r];

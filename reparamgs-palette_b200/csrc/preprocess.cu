@@ -164,16 +164,28 @@ __global__ void __launch_bounds__(kThreads)
 // A Gaussian's coefficient row is NB*K values (up to 128); read one row per
 // thread straight from global memory, a warp's loads would be strided by the
 // row length and thrash L1.  The block's rows, one contiguous span, are
-// therefore copied first into shared memory at an odd row stride, where each
-// thread reads its own row without bank conflicts: one 4-byte asynchronous
-// copy (cp.async) per element (FP32) or element pair (BF16), so the whole
-// span is in flight at once without holding registers.  The band count NB is
-// a template parameter, so the basis, its gradient and the Jacobian sums stay
-// in registers.  The outputs (K weights, and with the Jacobians NB basis
+// therefore copied first into shared memory, where each thread reads its own
+// row without bank conflicts, by asynchronous copies (cp.async), so the whole
+// span is in flight at once without holding registers.  The staging mode is a
+// template parameter (kShInPlace, kShStage4, kShStage16; see below), so the
+// coefficient reads carry no runtime choice.  The band count NB is a template
+// parameter too, so the basis, its gradient and the Jacobian sums stay in
+// registers.  The outputs (K weights, and with the Jacobians NB basis
 // values and 3K direction derivatives per Gaussian) are gathered in shared
 // memory at odd row strides and written back as contiguous spans of the
 // block's rows.
 constexpr int kShThreads = 64;  // 64 rows of at most 129 floats: 33 KB of shared memory
+
+// Staging modes of k_sh2feat:
+// - kShInPlace: rows read from global memory (BF16 rows of odd length or from
+//   a base that is not 4-byte aligned);
+// - kShStage4: one 4-byte copy per FP32 element or BF16 element pair, rows at
+//   an odd stride of 32-bit words;
+// - kShStage16: FP32 rows whose length is a multiple of 4, from a 16-byte
+//   aligned base: one 16-byte copy per 4 elements, rows at an odd stride of
+//   16-byte words, read as float4 (a quarter-warp's 8 lanes hit 8 distinct
+//   4-bank groups).
+constexpr int kShInPlace = 0, kShStage4 = 1, kShStage16 = 2;
 
 template <int K, int NB>
 struct ShOut {
@@ -190,25 +202,46 @@ __device__ __forceinline__ void rows_out(const float* src, int rows, float* __re
   }
 }
 
-template <int K, int NB, typename T>
+template <int K, int NB, typename T, int MODE>
 __global__ void __launch_bounds__(kShThreads)
-    k_sh2feat(int64_t n, const T* __restrict__ shs, bool staged,
-              const float* __restrict__ pws, const float* __restrict__ twc,
-              float* __restrict__ feat, float* __restrict__ dshs, float* __restrict__ dpws) {
-  extern __shared__ float srows[];
+    k_sh2feat(int64_t n, const T* __restrict__ shs, const float* __restrict__ pws,
+              const float* __restrict__ twc, float* __restrict__ feat,
+              float* __restrict__ dshs, float* __restrict__ dpws) {
+  extern __shared__ __align__(16) float srows[];
   constexpr int rl = NB * K, stride = rl | 1;
+  // kShStage16: 16-byte words per row and the row stride in floats
+  constexpr int kV4 = rl / 4 > 0 ? rl / 4 : 1, kV4Stride = 4 * (kV4 | 1);
+  static_assert(MODE != kShStage16 || (sizeof(T) == 4 && rl % 4 == 0), "16-byte staging");
   // staged BF16 rows: 32-bit words per row and the row stride in words
   // (odd BF16 rows are never staged)
   constexpr int kBfWords = rl / 2 > 0 ? rl / 2 : 1, kBfStride = kBfWords | 1;
   using O = ShOut<K, NB>;
   const int64_t row0 = (int64_t)blockIdx.x * kShThreads;
   const int rows = (int)min((int64_t)kShThreads, n - row0);
-  // FP32 rows are copied element by element, BF16 rows of even length from a
-  // 4-byte aligned base as element pairs (2-byte copies cost more than the
-  // strided reads they replace); other BF16 rows are read in place.  The host makes that decision (`staged`) and
-  // sizes the shared memory by it.
+  // BF16 rows of even length from a 4-byte aligned base are copied as element
+  // pairs (2-byte copies cost more than the strided reads they replace); other
+  // BF16 rows are read in place.  The host picks the mode and sizes the
+  // shared memory by it.
   constexpr bool kF32 = sizeof(T) == 4;
-  if (kF32 && staged) {
+  if constexpr (MODE == kShStage16) {
+    const float4* src = reinterpret_cast<const float4*>(shs + row0 * rl);
+    const int total = rows * kV4;
+    int r = threadIdx.x / kV4, q = threadIdx.x - r * kV4;
+    constexpr int dr = kShThreads / kV4, dq = kShThreads - dr * kV4;
+    for (int e = threadIdx.x; e < total; e += kShThreads) {
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(srows + r * kV4Stride + 4 * q)),
+                   "l"(src + e)
+                   : "memory");
+      q += dq;
+      r += dr;
+      if (q >= kV4) {
+        q -= kV4;
+        ++r;
+      }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if constexpr (MODE == kShStage4 && kF32) {
     // FP32: every element of the block's span is one 4-byte asynchronous
     // copy (cp.async), so the whole span is in flight at once without
     // holding registers; (row, column) of element e advanced by kShThreads
@@ -230,7 +263,7 @@ __global__ void __launch_bounds__(kShThreads)
       }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-  } else if (staged) {
+  } else if constexpr (MODE == kShStage4) {
     // BF16 rows of even length from a 4-byte aligned base: each element pair
     // is one 4-byte asynchronous copy, kept raw at an odd row stride of
     // 32-bit words and converted when read
@@ -260,14 +293,22 @@ __global__ void __launch_bounds__(kShThreads)
   float acc[K], Y[16], dp[3 * K];
   if (live) {
     const float* srow = srows + threadIdx.x * stride;
+    const float4* srow4 = reinterpret_cast<const float4*>(srows + threadIdx.x * kV4Stride);
     const __nv_bfloat16* sraw = reinterpret_cast<const __nv_bfloat16*>(
         reinterpret_cast<const uint32_t*>(srows) + threadIdx.x * kBfStride);
     const T* grow = shs + i * (int64_t)rl;
-    const auto c = [&](int idx) {
-      if constexpr (kF32)
-        return staged ? srow[idx] : ld(grow, idx);
-      else
-        return staged ? __bfloat162float(sraw[idx]) : ld(grow, idx);
+    const auto c = [&](int idx) -> float {
+      if constexpr (MODE == kShStage16) {
+        const float4 v = srow4[idx >> 2];
+        return (idx & 3) == 0 ? v.x : (idx & 3) == 1 ? v.y : (idx & 3) == 2 ? v.z : v.w;
+      } else if constexpr (MODE == kShStage4) {
+        if constexpr (kF32)
+          return srow[idx];
+        else
+          return __bfloat162float(sraw[idx]);
+      } else {
+        return ld(grow, idx);
+      }
     };
     float dir[3] = {0.f, 0.f, 0.f}, nd[3] = {0.f, 0.f, 0.f}, ninv = 0.f;
     if (NB > 1) {
@@ -352,15 +393,33 @@ int launch_inverse_cov2d(int64_t n, const float* cov2ds, float* depths, float* c
   return check_launch("inverseCov2D");
 }
 
+template <int K, int NB, typename T>
+static void sh2feat_launch(int64_t n, const T* s, int mode, size_t smem, int g, const float* pws,
+                           const float* twc, float* feat, float* dshs, float* dpws,
+                           cudaStream_t st) {
+  if constexpr (sizeof(T) == 4 && (NB * K) % 4 == 0) {
+    if (mode == kShStage16) {
+      k_sh2feat<K, NB, T, kShStage16><<<g, kShThreads, smem, st>>>(n, s, pws, twc, feat, dshs,
+                                                                   dpws);
+      return;
+    }
+  }
+  if (mode == kShStage4)
+    k_sh2feat<K, NB, T, kShStage4><<<g, kShThreads, smem, st>>>(n, s, pws, twc, feat, dshs, dpws);
+  else
+    k_sh2feat<K, NB, T, kShInPlace><<<g, kShThreads, smem, st>>>(n, s, pws, twc, feat, dshs,
+                                                                 dpws);
+}
+
 template <int K, typename T>
-static int sh2feat_kn(int64_t n, const T* s, int nb, bool staged, size_t smem, int g,
+static int sh2feat_kn(int64_t n, const T* s, int nb, int mode, size_t smem, int g,
                       const float* pws, const float* twc, float* feat, float* dshs, float* dpws,
                       cudaStream_t st) {
   switch (nb) {
-    case 1: k_sh2feat<K, 1, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
-    case 4: k_sh2feat<K, 4, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
-    case 9: k_sh2feat<K, 9, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
-    case 16: k_sh2feat<K, 16, T><<<g, kShThreads, smem, st>>>(n, s, staged, pws, twc, feat, dshs, dpws); break;
+    case 1: sh2feat_launch<K, 1, T>(n, s, mode, smem, g, pws, twc, feat, dshs, dpws, st); break;
+    case 4: sh2feat_launch<K, 4, T>(n, s, mode, smem, g, pws, twc, feat, dshs, dpws, st); break;
+    case 9: sh2feat_launch<K, 9, T>(n, s, mode, smem, g, pws, twc, feat, dshs, dpws, st); break;
+    case 16: sh2feat_launch<K, 16, T>(n, s, mode, smem, g, pws, twc, feat, dshs, dpws, st); break;
     default: return GSB_ERR_INVALID_ARGUMENT;
   }
   return GSB_OK;
@@ -371,13 +430,17 @@ static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws
                      float* feat, float* dshs, float* dpws, cudaStream_t st) {
   const T* s = (const T*)shs;
   const int g = div_up(n > 0 ? n : 1, kShThreads);
-  // BF16 rows are staged as 32-bit element pairs: only rows of even length
-  // from a 4-byte aligned base
-  const bool staged = sizeof(T) == 4 ||
-                      ((nb * K) % 2 == 0 && (reinterpret_cast<uintptr_t>(shs) & 3) == 0);
-  const size_t row_words = sizeof(T) == 4 ? (size_t)((nb * K) | 1)
-                                           : (size_t)(((nb * K) / 2) | 1);  // raw BF16 pairs
-  const size_t stage_bytes = staged ? (size_t)kShThreads * row_words * 4 : 0;
+  // FP32 rows by 16-byte copies when their length is a multiple of 4 and the
+  // base 16-byte aligned, else by 4-byte copies; BF16 rows as 32-bit element
+  // pairs when of even length from a 4-byte aligned base, else in place
+  const int rl = nb * K;
+  const uintptr_t base = reinterpret_cast<uintptr_t>(shs);
+  const int mode = sizeof(T) == 4 ? (rl % 4 == 0 && (base & 15) == 0 ? kShStage16 : kShStage4)
+                                  : (rl % 2 == 0 && (base & 3) == 0 ? kShStage4 : kShInPlace);
+  const size_t row_words = mode == kShStage16 ? (size_t)(4 * ((rl / 4) | 1))
+                           : sizeof(T) == 4   ? (size_t)(rl | 1)
+                                              : (size_t)((rl / 2) | 1);  // raw BF16 pairs
+  const size_t stage_bytes = mode != kShInPlace ? (size_t)kShThreads * row_words * 4 : 0;
   // output gathering: K weights, NB basis values and 3K derivatives per row
   // at odd strides (the NB + 3K part only with the Jacobians, but always
   // reserved: it is small)
@@ -388,7 +451,7 @@ static int sh2feat_t(int64_t n, const void* shs, int nb, int K, const float* pws
   switch (K) {
 #define GSB_K(KK)                                                                          \
   case KK:                                                                                 \
-    rc = sh2feat_kn<KK, T>(n, s, nb, staged, smem, g, pws, twc, feat, dshs, dpws, st);     \
+    rc = sh2feat_kn<KK, T>(n, s, nb, mode, smem, g, pws, twc, feat, dshs, dpws, st);       \
     break;
     GSB_K(1) GSB_K(2) GSB_K(3) GSB_K(4) GSB_K(5) GSB_K(6) GSB_K(7) GSB_K(8)
 #undef GSB_K

@@ -355,6 +355,74 @@ def test_bf16_sh_rows_odd_length_or_misaligned(cuda_ok, nb, K, offset):
     assert rel_err(dpw, o_dpw) < 1e-4
 
 
+@pytest.mark.parametrize("nb,K,offset", [(16, 5, 1), (16, 5, 2), (4, 5, 3), (16, 8, 1),
+                                         (9, 5, 0), (16, 3, 0)])
+def test_fp32_sh_staging_modes_agree(cuda_ok, nb, K, offset):
+    """FP32 coefficient rows are staged by 16-byte copies when the row length
+    is a multiple of 4 and the base 16-byte aligned, else by 4-byte copies.
+    A contiguous view at a storage offset of 1-3 floats takes the 4-byte
+    path; rows of 45 or 48 floats (9 x 5, 16 x 3) take it as well (or the
+    16-byte one, 48). Every output equals that of the aligned call bit for
+    bit, and matches the oracle."""
+    n = 3000  # 46 full blocks of 64 rows and a last one of 56
+    g = torch.Generator().manual_seed(300 + nb * 10 + K + offset)
+    vals = torch.randn((n, nb * K), generator=g) * 0.2
+    ref_shs = vals.cuda()
+    assert ref_shs.data_ptr() % 16 == 0
+    if offset:
+        buf = torch.empty((n * nb * K + offset,), device="cuda")
+        buf[offset:] = ref_shs.reshape(-1)
+        shs = buf[offset:].view(n, nb * K)
+        assert shs.is_contiguous() and shs.data_ptr() % 16 == 4 * offset
+    else:
+        shs = ref_shs
+    sc, st = _scene(n, seed=44)
+    cam = _cam(64, 64, (0.5, -7.5, 0.8))
+    call = (lambda s, j: gsc.sh2Color(s, st["pws"], cam.twc, j)) if K == 3 else \
+        (lambda s, j: gsc.sh2Weight(s, st["pws"], cam.twc, j, K))
+    for jac in (False, True):
+        got, want = call(shs, jac), call(ref_shs, jac)
+        for x, y in zip(got, want):
+            assert torch.equal(x, y)
+    twc = orc.camera_arrays(cam, np.float32)[2]
+    f, dsh, dpw = call(shs, True)
+    o_f, o_dsh, o_dpw = orc.sh2feat(vals.numpy(), sc["pws"], twc, K, True)
+    np.testing.assert_allclose(np_of(f), o_f, rtol=1e-5, atol=2e-7)
+    np.testing.assert_allclose(np_of(dsh), o_dsh, rtol=1e-5, atol=2e-7)
+    assert rel_err(dpw, o_dpw) < 1e-4
+
+
+@pytest.mark.parametrize("rank", [1, 3])
+def test_bf16_lowrank_unaligned_factors_agree(cuda_ok, rank):
+    """BF16 low-rank factors are bulk-copied raw when a block's spans start on
+    16-byte boundaries, else copied raw element by element. Factors in views
+    at an odd storage offset (every block on the element path) give the same
+    weights, basis and factor gradients bit for bit as aligned ones."""
+    n = 4000
+    sc, st = _scene(n, seed=50 + rank, mode="lowrank", rank=rank, dtype=torch.bfloat16)
+    cam = _cam(64, 64, (0.8, -7.0, 0.4))
+    A, B = st["A"], st["B"]
+    if rank == 1:
+        A, B = A[:, :, 0].contiguous(), B[:, 0, :].contiguous()
+
+    def shifted(t):
+        buf = torch.empty((t.numel() + 1,), dtype=t.dtype, device="cuda")
+        buf[1:] = t.reshape(-1)
+        v = buf[1:].view(t.shape)
+        assert v.is_contiguous() and v.data_ptr() % 4 == 2
+        return v
+
+    dc_s, A_s, B_s = shifted(st["dc"]), shifted(A), shifted(B)
+    got = gsc.sh2Weight_fast(dc_s, A_s, B_s, st["pws"], cam.twc, True, 5, 15)
+    want = gsc.sh2Weight_fast(st["dc"], A, B, st["pws"], cam.twc, True, 5, 15)
+    for x, y in zip(got, want):
+        assert torch.equal(x, y)
+    dw = torch.randn((n, 5), device="cuda", generator=torch.Generator("cuda").manual_seed(9))
+    gA, gB = gsc.sh2Weight_fast_B(A_s, B_s, want[2], dw, 5, 15)
+    wA, wB = gsc.sh2Weight_fast_B(A, B, want[2], dw, 5, 15)
+    assert torch.equal(gA, wA) and torch.equal(gB, wB)
+
+
 def test_lab2rgb_matches_oracle(cuda_ok):
     g = torch.Generator().manual_seed(0)
     lab = torch.stack([torch.rand(40, 50, generator=g), torch.rand(40, 50, generator=g) * 160 - 80,
