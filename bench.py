@@ -321,16 +321,15 @@ def stage_breakdown(wl, reps=5):
                             device=us.device)
         import ctypes as C
         sp = _lib.stream_of(us)
-        d0, a0 = d.clone(), areas.clone()
-
         def pack():
-            d.copy_(d0)
-            areas.copy_(a0)
             _lib.call("bench", "gsb_splat_pack", n, H, W, K, _lib.ptr(us), _lib.ptr(cinv),
                       _lib.ptr(wl["alphas"]), _lib.ptr(w), 0, _lib.ptr(d), _lib.ptr(areas),
                       _lib.ptr(state), sp)
-        out["bin_pack_scan"] = timed(pack, reps, st) / reps
+        # the pack's in-place updates (depth and extent of Gaussians with an
+        # empty tile rectangle) are idempotent: after this first call every
+        # timed call sees the same inputs and writes the same outputs
         pack()
+        out["bin_pack_scan"] = timed(pack, reps, st) / reps
         plan = _lib.SplatPlan()
         _lib.call("bench", "gsb_splat_counts", n, H, W, _lib.ptr(state), C.byref(plan), sp)
         M = int(plan.patches)
