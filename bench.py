@@ -758,26 +758,29 @@ def run_b200(a):
     fms = allreduce_max(fms, world, device)
 
     # end to end: every step copies its inputs (camera, target image) from pinned
-    # host memory and reads its loss back into pinned host memory.  The target
-    # of step i+1 is copied on a side stream while step i computes (an input
-    # pipeline that prefetches one step ahead, into the buffer step i-1 used);
-    # the camera (R, t and centre: 60 bytes in one pinned buffer) is copied in
-    # line, issued before the next target's prefetch so that it does not queue
-    # behind that 25 MB copy on the host-to-device copy engine.  All copies
-    # fall inside the timed region.
+    # host memory and reads its loss back into pinned host memory.  The inputs
+    # of step i+1 -- the camera (R, t and centre: 60 bytes in one pinned buffer)
+    # and the target -- are copied on a side stream while step i computes (an
+    # input pipeline that prefetches one step ahead, into the buffers step i-1
+    # used), and each step's loss is read back on a third stream once the step
+    # is done, so that no copy sits between two steps' kernels on the compute
+    # stream.  All copies fall inside the timed region.
     cam = wl["cam"]
     cam_h = torch.cat([cam.Rcw.reshape(-1), cam.tcw.reshape(-1), cam.twc.reshape(-1)]).cpu()
     cam_h = cam_h.pin_memory()
     loss_h = torch.empty((), dtype=torch.float32).pin_memory()
     tgt_d = [torch.empty_like(wl["target"]) for _ in range(2)]
+    cam_d = [torch.empty(cam_h.shape, dtype=cam_h.dtype, device=device) for _ in range(2)]
     copy_stream = torch.cuda.Stream(device)
+    read_stream = torch.cuda.Stream(device)
     copied = [torch.cuda.Event() for _ in range(2)]
     used = [torch.cuda.Event() for _ in range(2)]
     from palette_b200.scene import Camera
 
     def prefetch(slot):
         with torch.cuda.stream(copy_stream):
-            copy_stream.wait_event(used[slot])  # the step that last read this buffer
+            copy_stream.wait_event(used[slot])  # the step that last read these buffers
+            cam_d[slot].copy_(cam_h, non_blocking=True)
             tgt_d[slot].copy_(wl["target_host"], non_blocking=True)
             copied[slot].record(copy_stream)
 
@@ -787,15 +790,20 @@ def run_b200(a):
         prefetch(0)
         for i in range(k):
             slot = i % 2
-            cam_d = cam_h.to(device, non_blocking=True)
             if i + 1 < k:
                 prefetch((i + 1) % 2)
             stream.wait_event(copied[slot])
+            cd = cam_d[slot]
             c = Camera(0, cam.width, cam.height, cam.fx, cam.fy, cam.cx, cam.cy,
-                       cam_d[:9].view(3, 3), cam_d[9:12], twc=cam_d[12:15])
+                       cd[:9].view(3, 3), cd[9:12], twc=cd[12:15])
             loss = step(wl, cam=c, target=tgt_d[slot])
             used[slot].record(stream)
-            loss_h.copy_(loss.detach(), non_blocking=True)
+            with torch.cuda.stream(read_stream):
+                read_stream.wait_event(used[slot])
+                loss = loss.detach()
+                loss.record_stream(read_stream)  # not recycled before the copy ran
+                loss_h.copy_(loss, non_blocking=True)
+        stream.wait_stream(read_stream)  # the last read-back inside the timed region
     for _ in range(2):
         e2e_run(2)
     torch.cuda.synchronize()
@@ -862,7 +870,9 @@ def run_b200(a):
                     frames_per_s=round(world * 1000.0 / fms, 2), forward_ms=round(fms, 4),
                     e2e=dict(value=round(world * a.steps / (ems / 1000.0), 3), unit="iters/s",
                              h2d_bytes_per_step=h2d, d2h_bytes_per_step=4,
-                             input_pipeline="next step's target copied while this step computes"),
+                             input_pipeline="next step's camera and target copied on a side "
+                                            "stream while this step computes; each loss read "
+                                            "back on a third stream"),
                     gpu_launches=launches, clocks=clk, roofline=roof, cpu_baseline=cb,
                     fused_path=dict(iters_per_s=round(world * 1000.0 / fu_ms, 3),
                                     ms_per_step=round(fu_ms, 4), forward_ms=round(fu_fms, 4),
